@@ -1,0 +1,189 @@
+// k_flux_stag.cu -- fused explicit-flux kernel of the staggered schemes (HW2, VV4).
+//
+// One CTA owns a 32 x 8 (x, y) tile and marches a chunk of z-planes.  The velocity
+// planes z-H .. z+H (H = 3 for VV4, 1 for HW2) of the tile plus an H-wide periodic
+// halo live in a shared-memory ring of 2H+2 slots; the next plane is fetched with
+// LDGSTS (cp.async) while the current one is computed, so every v_n value crosses
+// HBM once and the halo re-reads hit L2.  The epilogue fuses the SBDF3 history
+// combination (staggered/func_global.h:910-932) and the weighted sum of RHS_x
+// used by the constant-flow-rate forcing, so the kernel reads v_n, v_{n-1},
+// v_{n-2}, F_{n-1}, F_{n-2} and writes F_n and the RHS exactly once.
+// Arithmetic: stencil_stag.cuh (staggered/func_global.h:345-625).
+#include <algorithm>
+
+#include "kernels.cuh"
+#include "stencil_stag.cuh"
+
+namespace tc {
+
+constexpr int STX = 32, STY = 8;
+
+template <typename T, int H>
+struct RingAcc {
+    static constexpr int PW = STX + 2 * H, PH = STY + 2 * H, PL = PW * PH, RS = 2 * H + 2;
+    const T* ring;
+    int zs, tx, ty;
+    __device__ __forceinline__ T operator()(int c, int dx, int dy, int dz) const {
+        const int slot = (zs + dz) & (RS - 1);
+        return ring[((slot * 3 + c) * PH + ty + H + dy) * PW + tx + H + dx];
+    }
+};
+
+template <typename T, int SCHEME, int VISC, bool LES, int ORDER>
+__global__ void __launch_bounds__(STX* STY, 2) k_flux_stag(FluxArgs<T> a, int tz) {
+    constexpr int H = SCHEME == TC_SCHEME_VV4 ? 3 : 1;
+    using ACC = RingAcc<T, H>;
+    constexpr int PW = ACC::PW, PL = ACC::PL, RS = ACC::RS;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    T* ring = reinterpret_cast<T*>(smraw);
+    __shared__ double sbuf[32];
+
+    const Geom& g = a.g;
+    const int NX = g.NX, NY = g.NY, NZ = g.NZ;
+    const size_t NXY = (size_t)NX * NY;
+    const int tx = threadIdx.x % STX, ty = threadIdx.x / STX;
+    const int x0 = blockIdx.x * STX, y0 = blockIdx.y * STY;
+    const int zb = blockIdx.z * tz, ze = min(NZ, zb + tz);
+    const int ix = x0 + tx, iy = y0 + ty;
+    const bool active = ix < NX && iy < NY;
+
+    auto load_plane = [&](int z) {
+        T* dst = ring + (z & (RS - 1)) * 3 * PL;
+        for (int e = threadIdx.x; e < 3 * PL; e += blockDim.x) {
+            const int c = e / PL, r = e - c * PL, py = r / PW, px = r - py * PW;
+            const int gx = wrapi(x0 - H + px, NX), gy = wrapi(y0 - H + py, NY);
+            cp_async<sizeof(T)>(dst + e, a.vel.c[c] + (size_t)z * NXY + (size_t)gy * NX + gx);
+        }
+    };
+    for (int z = max(0, zb - H); z <= min(NZ - 1, zb + H); z++) load_plane(z);
+    cp_async_commit();
+
+    StagZ<T> mz;
+    mz.NZ = NZ;
+    mz.DZ = a.m.DZ;
+    mz.DZW = a.m.DZW;
+    mz.hx = (T)g.hx;
+    mz.hy = (T)g.hy;
+    mz.ihx = (T)g.inv_hx;
+    mz.ihy = (T)g.inv_hy;
+    mz.visc = (T)g.visc;
+    const int xm = wrapi(ix - 1, NX), xp = wrapi(ix + 1, NX);
+    const int ym = wrapi(iy - 1, NY), yp = wrapi(iy + 1, NY);
+    const T inv_tau = a.inv_tau;
+    double ub = 0.0;
+
+    for (int z = zb; z < ze; z++) {
+        if (z + 1 < ze && z + H + 1 < NZ) load_plane(z + H + 1);
+        cp_async_commit();
+        cp_async_wait<1>();
+        __syncthreads();
+        if (active) {
+            mz.iz = z;
+            const ACC A{ring, z & (RS - 1), tx, ty};
+            T cf[3], vf[3];
+            if (SCHEME == TC_SCHEME_VV4) conv_vv4(A, mz, a.m.GCZ[z], cf);
+            else conv_hw2(A, mz, cf);
+            if (VISC == TC_VISC_CROSS) {
+                visc_cross(A, mz, vf);
+            } else {
+                const T* nt = a.nu_t;
+                auto MU = [&](int dx, int dy, int dz) -> T {
+                    if (!LES) return (T)g.visc;
+                    const int xx = dx < 0 ? xm : (dx > 0 ? xp : ix);
+                    const int yy = dy < 0 ? ym : (dy > 0 ? yp : iy);
+                    return (T)g.visc + __ldg(nt + (size_t)(z + dz) * NXY + (size_t)yy * NX + xx);
+                };
+                visc_naive(A, MU, mz, vf);
+            }
+            T f[3];
+            f[0] = ((T)g.sour_dpdx + cf[0]) + vf[0];
+            f[1] = (T(0) + cf[1]) + vf[1];
+            f[2] = (T(0) + cf[2]) + vf[2];
+            if (z == 0) f[2] = 0;
+            const size_t id = (size_t)z * NXY + (size_t)iy * NX + ix;
+#pragma unroll
+            for (int c = 0; c < 3; c++) a.fout.c[c][id] = f[c];
+            if (ORDER > 0) {
+                T r[3];
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    const T vn = A(c, 0, 0, 0);
+                    if (ORDER == 1) {
+                        r[c] = f[c] + inv_tau * vn;
+                    } else if (ORDER == 2) {
+                        r[c] = (T(2.) * f[c] - a.fp.c[c][id]) + inv_tau * (2 * vn - T(0.5) * a.velp.c[c][id]);
+                    } else {
+                        r[c] = ((3 * f[c] - 3 * a.fp.c[c][id]) + a.fq.c[c][id]) +
+                               inv_tau * ((3 * vn - T(1.5) * a.velp.c[c][id]) +
+                                          T(0.33333333333333333333) * a.velq.c[c][id]);
+                    }
+                    a.rhs.c[c][id] = r[c];
+                }
+                ub += (double)r[0] * (double)a.m.DZ[z];
+            }
+        }
+        __syncthreads();
+    }
+    if (ORDER > 0 && a.ub_out) {
+        const double s = block_sum(ub, sbuf);
+        grid_sum_finish(s, a.ub_partial, a.ticket, a.ub_out, sbuf);
+    }
+}
+
+static void flux_stag_shape(const Geom& g, dim3& grid, int& tz) {
+    const int tiles = ((g.NX + STX - 1) / STX) * ((g.NY + STY - 1) / STY);
+    int nch = std::max(1, (148 * 8 + tiles - 1) / tiles);
+    tz = std::max(4, (g.NZ + nch - 1) / nch);
+    grid = dim3((g.NX + STX - 1) / STX, (g.NY + STY - 1) / STY, (g.NZ + tz - 1) / tz);
+}
+
+int flux_grid_blocks(const Geom& g) {
+    dim3 gr;
+    int tz;
+    flux_stag_shape(g, gr, tz);
+    return (int)(gr.x * gr.y * gr.z);
+}
+
+template <typename T, int SCHEME, int VISC, bool LES, int ORDER>
+static void run(const FluxArgs<T>& a, cudaStream_t s) {
+    constexpr int H = SCHEME == TC_SCHEME_VV4 ? 3 : 1;
+    constexpr size_t smem = sizeof(T) * (2 * H + 2) * 3 * (STX + 2 * H) * (STY + 2 * H);
+    static bool attr = false;
+    auto kern = k_flux_stag<T, SCHEME, VISC, LES, ORDER>;
+    if (!attr) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr = true;
+    }
+    dim3 grid;
+    int tz;
+    flux_stag_shape(a.g, grid, tz);
+    kern<<<grid, STX * STY, smem, s>>>(a, tz);
+}
+
+template <typename T, int SCHEME, int VISC, bool LES>
+static void run_order(const FluxArgs<T>& a, cudaStream_t s) {
+    switch (a.order) {
+        case 0: run<T, SCHEME, VISC, LES, 0>(a, s); break;
+        case 1: run<T, SCHEME, VISC, LES, 1>(a, s); break;
+        case 2: run<T, SCHEME, VISC, LES, 2>(a, s); break;
+        default: run<T, SCHEME, VISC, LES, 3>(a, s); break;
+    }
+}
+
+template <typename T, int SCHEME>
+static void run_visc(const FluxArgs<T>& a, cudaStream_t s) {
+    if (a.g.visc_type == TC_VISC_CROSS) run_order<T, SCHEME, TC_VISC_CROSS, false>(a, s);
+    else if (a.nu_t) run_order<T, SCHEME, TC_VISC_NAIVE, true>(a, s);
+    else run_order<T, SCHEME, TC_VISC_NAIVE, false>(a, s);
+}
+
+template <typename T>
+void launch_flux_stag(const FluxArgs<T>& a, cudaStream_t s) {
+    if (a.g.scheme == TC_SCHEME_VV4) run_visc<T, TC_SCHEME_VV4>(a, s);
+    else run_visc<T, TC_SCHEME_HW2>(a, s);
+}
+
+template void launch_flux_stag<double>(const FluxArgs<double>&, cudaStream_t);
+template void launch_flux_stag<float>(const FluxArgs<float>&, cudaStream_t);
+
+}  // namespace tc

@@ -1,0 +1,349 @@
+// k_misc.cu -- velocity correction, Smagorinsky viscosity, stand-alone operators,
+// fused per-plane diagnostics and the host-boundary layout conversions.
+#include <algorithm>
+
+#include "kernels.cuh"
+#include "stencil_div.cuh"
+#include "stencil_stag.cuh"
+
+namespace tc {
+
+constexpr int KX = 32, KY = 8;
+
+// ---------------------------------------------------------------------------
+// Gradient + correction.  ApplyGradient: HW2 staggered/func_global.h:297-303,
+// VV4 :316-322, collocated collocated_AB3/func_global.h:298-303; correction
+// staggered/func_global.h:939-941, collocated_AB3/func_global.h:430-448.
+// Each thread marches a column of z; x/y neighbours of p come through L1.
+// ---------------------------------------------------------------------------
+template <typename T, int SCHEME, bool STAB1, bool GRADONLY>
+__global__ void __launch_bounds__(KX* KY) k_correct(CorrArgs<T> a, int tz) {
+    const Geom& g = a.g;
+    const int NX = g.NX, NY = g.NY, NZ = g.NZ;
+    const size_t NXY = (size_t)NX * NY;
+    const int ix = blockIdx.x * KX + threadIdx.x % KX, iy = blockIdx.y * KY + threadIdx.x / KX;
+    if (ix >= NX || iy >= NY) return;
+    const int zb = blockIdx.z * tz, ze = min(NZ, zb + tz);
+    const int xm = wrapi(ix - 1, NX), xmm = wrapi(ix - 2, NX), xp = wrapi(ix + 1, NX);
+    const int ym = wrapi(iy - 1, NY), ymm = wrapi(iy - 2, NY), yp = wrapi(iy + 1, NY);
+    const T* p = a.p;
+    const T ihx = (T)g.inv_hx, ihy = (T)g.inv_hy;
+    T du = 0;
+    if (!GRADONLY && a.cfr) {
+        const double ub = (*a.ub_sum) * a.cfr_scale * (double)a.tob;
+        const double d = (a.cfr_target - ub) * a.cfr_volfac;
+        du = (T)d;
+        if (blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0) *a.du_out = d;
+    }
+    for (int z = zb; z < ze; z++) {
+        const size_t pl = (size_t)z * NXY, id = pl + (size_t)iy * NX + ix;
+        const T p0 = __ldg(p + id);
+        T gp[3];
+        if (SCHEME == TC_SCHEME_HW2) {
+            gp[0] = ihx * (p0 - __ldg(p + pl + (size_t)iy * NX + xm));
+            gp[1] = ihy * (p0 - __ldg(p + pl + (size_t)ym * NX + ix));
+            gp[2] = z == 0 ? T(0) : (p0 - __ldg(p + id - NXY)) * (2 / (a.m.DZ[z] + a.m.DZ[z - 1]));
+        } else if (SCHEME == TC_SCHEME_VV4) {
+            const T g1 = a.m.GC1[z], g2 = a.m.GC2[z];
+            gp[0] = ihx * (g1 * (p0 - __ldg(p + pl + (size_t)iy * NX + xm)) +
+                           g2 * (__ldg(p + pl + (size_t)iy * NX + xp) - __ldg(p + pl + (size_t)iy * NX + xmm)));
+            gp[1] = ihy * (g1 * (p0 - __ldg(p + pl + (size_t)ym * NX + ix)) +
+                           g2 * (__ldg(p + pl + (size_t)yp * NX + ix) - __ldg(p + pl + (size_t)ymm * NX + ix)));
+            if (z == 0) {
+                gp[2] = 0;
+            } else {
+                const T pl1 = __ldg(p + id - NXY);
+                const T pr = z == NZ - 1 ? -p0 : __ldg(p + id + NXY);
+                const T pll = z == 1 ? -pl1 : __ldg(p + id - 2 * NXY);
+                gp[2] = ((p0 - pl1) - T(0.03703703703703703703) * (pr - pll)) * a.m.GCZ[z];
+            }
+        } else {
+            if (z == 0 || z == NZ - 1) {
+                gp[0] = gp[1] = gp[2] = 0;
+            } else {
+                gp[0] = T(0.5) * ihx * (__ldg(p + pl + (size_t)iy * NX + xp) - __ldg(p + pl + (size_t)iy * NX + xm));
+                gp[1] = T(0.5) * ihy * (__ldg(p + pl + (size_t)yp * NX + ix) - __ldg(p + pl + (size_t)ym * NX + ix));
+                gp[2] = T(0.5) * (__ldg(p + id + NXY) - __ldg(p + id - NXY)) / a.m.cellh[z];
+            }
+        }
+        if (GRADONLY) {
+#pragma unroll
+            for (int c = 0; c < 3; c++) a.vout.c[c][id] = gp[c];
+        } else {
+#pragma unroll
+            for (int c = 0; c < 3; c++) a.vout.c[c][id] = (a.rhs.c[c][id] - gp[c]) * a.tob;
+            if (a.cfr && !(SCHEME == TC_SCHEME_COLLOC && (z == 0 || z == NZ - 1))) a.vout.c[0][id] += du;
+            if (STAB1) a.pnext[id] = p0 + a.pcur[id];
+        }
+    }
+}
+
+static void column_shape(const Geom& g, dim3& grid, int& tz) {
+    const int tiles = ((g.NX + KX - 1) / KX) * ((g.NY + KY - 1) / KY);
+    const int nch = std::max(1, (148 * 8 + tiles - 1) / tiles);
+    tz = std::max(1, (g.NZ + nch - 1) / nch);
+    grid = dim3((g.NX + KX - 1) / KX, (g.NY + KY - 1) / KY, (g.NZ + tz - 1) / tz);
+}
+
+template <typename T, int SCHEME>
+static void correct_scheme(const CorrArgs<T>& a, cudaStream_t s) {
+    dim3 grid;
+    int tz;
+    column_shape(a.g, grid, tz);
+    if (a.grad_only) k_correct<T, SCHEME, false, true><<<grid, KX * KY, 0, s>>>(a, tz);
+    else if (a.pnext) k_correct<T, SCHEME, true, false><<<grid, KX * KY, 0, s>>>(a, tz);
+    else k_correct<T, SCHEME, false, false><<<grid, KX * KY, 0, s>>>(a, tz);
+}
+
+template <typename T>
+void launch_correct(const CorrArgs<T>& a, cudaStream_t s) {
+    if (a.g.scheme == TC_SCHEME_VV4) correct_scheme<T, TC_SCHEME_VV4>(a, s);
+    else if (a.g.scheme == TC_SCHEME_HW2) correct_scheme<T, TC_SCHEME_HW2>(a, s);
+    else correct_scheme<T, TC_SCHEME_COLLOC>(a, s);
+}
+
+// ---------------------------------------------------------------------------
+// Smagorinsky-van Driest eddy viscosity.  Staggered: per cell,
+// staggered/func_global.h:875-890 with |S| of :823-870.  Collocated: per element
+// (lower-corner node index), collocated_AB3/func_global.h:342-384.
+// ---------------------------------------------------------------------------
+template <typename T>
+struct GAcc {
+    const T* v[3];
+    int ix, iy, iz, NX, NY;
+    size_t NXY;
+    __device__ __forceinline__ T operator()(int c, int dx, int dy, int dz) const {
+        const int x = wrapi(ix + dx, NX), y = wrapi(iy + dy, NY);
+        return __ldg(v[c] + (size_t)(iz + dz) * NXY + (size_t)y * NX + x);
+    }
+};
+
+template <typename T>
+__device__ __forceinline__ T smag_nut(T AbsS, T dist, T vol, T inv_ls) {
+    const T yp = dist * inv_ls;
+    const T C_SMAG = T(0.1), C_exp = T(0.04 * 0.04 * 0.04);
+    const T fvd = 1 - exp(-C_exp * yp * yp * yp);
+    T Dl = C_SMAG * pow(vol, T(0.33333333333333333333));
+    if (Dl > T(0.41) * dist) Dl = T(0.41) * dist;
+    return fvd * Dl * Dl * AbsS;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_turb_stag(TurbArgs<T> a) {
+    const Geom& g = a.g;
+    const long long in = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (in >= g.N) return;
+    const int ix = (int)(in % g.NX), iy = (int)((in / g.NX) % g.NY), iz = (int)(in / g.NXY);
+    GAcc<T> A{{a.v.c[0], a.v.c[1], a.v.c[2]}, ix, iy, iz, g.NX, g.NY, (size_t)g.NXY};
+    StagZ<T> mz{iz, g.NZ, a.m.DZ, a.m.DZW, (T)g.hx, (T)g.hy, (T)g.inv_hx, (T)g.inv_hy, (T)g.visc};
+    const T S = abs_strain(A, mz);
+    const T* ZZ = a.m.ZZ;
+    const T H = T(0.5) * (ZZ[g.NZ] - ZZ[0]);
+    const T Z = T(0.5) * (ZZ[iz] + ZZ[iz + 1]) - ZZ[0];
+    const T d = (Z < H) ? Z : 2 * H - Z;
+    a.nu_t[in] = smag_nut(S, d, (T)g.hx * (T)g.hy * a.m.DZ[iz], (T)g.inv_ls);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_turb_coll(TurbArgs<T> a) {
+    const Geom& g = a.g;
+    const long long ie = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (ie >= g.N) return;
+    const int ix = (int)(ie % g.NX), iy = (int)((ie / g.NX) % g.NY), iz = (int)(ie / g.NXY);
+    if (iz >= g.NZ - 1) return;
+    GAcc<T> A{{a.v.c[0], a.v.c[1], a.v.c[2]}, ix, iy, iz, g.NX, g.NY, (size_t)g.NXY};
+    const T hz = (T)a.m.dDZ[iz];
+    const T ihx = (T)g.inv_hx, ihy = (T)g.inv_hy;
+    T gr[3][3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        const T q = A(c, 0, 0, 0), qx = A(c, 1, 0, 0), qy = A(c, 0, 1, 0), qxy = A(c, 1, 1, 0);
+        const T qz = A(c, 0, 0, 1), qxz = A(c, 1, 0, 1), qyz = A(c, 0, 1, 1), qxyz = A(c, 1, 1, 1);
+        gr[0][c] = ((qx + qxy + qxz + qxyz) - (q + qy + qz + qyz)) * (T(0.25) * ihx);
+        gr[1][c] = ((qy + qxy + qyz + qxyz) - (q + qx + qz + qxz)) * (T(0.25) * ihy);
+        gr[2][c] = ((qz + qxz + qyz + qxyz) - (q + qx + qy + qxy)) / (4 * hz);
+    }
+    gr[0][1] = T(0.5) * (gr[0][1] + gr[1][0]);
+    gr[0][2] = T(0.5) * (gr[0][2] + gr[2][0]);
+    gr[1][2] = T(0.5) * (gr[1][2] + gr[2][1]);
+    T S = gr[0][0] * gr[0][0] + gr[1][1] * gr[1][1] + gr[2][2] * gr[2][2] +
+          2 * (gr[0][1] * gr[0][1] + gr[0][2] * gr[0][2] + gr[1][2] * gr[1][2]);
+    S = sqrt(2 * S);
+    const double* ZZ = a.m.dZZ;
+    const T H = (T)(0.5 * (ZZ[g.NZ - 1] - ZZ[0]));
+    const T Z = (T)(0.5 * (ZZ[iz] + ZZ[iz + 1]));
+    const T d = (Z < H) ? Z : 2 * H - Z;
+    a.nu_t[ie] = smag_nut(S, d, (T)g.hx * (T)g.hy * hz, (T)g.inv_ls);
+}
+
+template <typename T>
+void launch_turb(const TurbArgs<T>& a, cudaStream_t s) {
+    const unsigned nb = (unsigned)((a.g.N + 255) / 256);
+    if (a.g.scheme == TC_SCHEME_COLLOC) k_turb_coll<T><<<nb, 256, 0, s>>>(a);
+    else k_turb_stag<T><<<nb, 256, 0, s>>>(a);
+}
+
+// ---------------------------------------------------------------------------
+// Stand-alone divergence (operator form of ApplyDivergence)
+// ---------------------------------------------------------------------------
+template <typename T, int SCHEME>
+__global__ void __launch_bounds__(256) k_divergence(DivArgs<T> a) {
+    const Geom& g = a.g;
+    const long long in = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (in >= g.N) return;
+    const int ix = (int)(in % g.NX), iy = (int)((in / g.NX) % g.NY), iz = (int)(in / g.NXY);
+    a.dv[in] = div_at<T, SCHEME, false>(g, a.m, a.v, nullptr, ix, iy, iz);
+}
+
+template <typename T>
+void launch_divergence(const DivArgs<T>& a, cudaStream_t s) {
+    const unsigned nb = (unsigned)((a.g.N + 255) / 256);
+    if (a.g.scheme == TC_SCHEME_VV4) k_divergence<T, TC_SCHEME_VV4><<<nb, 256, 0, s>>>(a);
+    else if (a.g.scheme == TC_SCHEME_HW2) k_divergence<T, TC_SCHEME_HW2><<<nb, 256, 0, s>>>(a);
+    else k_divergence<T, TC_SCHEME_COLLOC><<<nb, 256, 0, s>>>(a);
+}
+
+// ---------------------------------------------------------------------------
+// Per-plane diagnostics in double: one CTA per z-plane.
+// planes[z*16 + k]: 0..2 sum u, v, w_c; 3..8 sum uu, vv, w_cw_c, uv, uw_c, vw_c;
+// 9 sum nu_t; 10 sum p; 11 sum pp; 12 sum w (raw); 13 sum w^2 (raw);
+// 14..15 max CFL convective / viscous part; 16.. unused.  (CalcProfiles,
+// CalcIntegral, CalcKineticEnergy, CalcCFL: staggered/func_global.h:678-808.)
+// ---------------------------------------------------------------------------
+constexpr int NDIAG = 16;
+static_assert(NDIAG + 3 == TC_DIAG_STRIDE, "diagnostics layout");
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_diag(DiagArgs<T> a) {
+    const Geom& g = a.g;
+    const int z = blockIdx.x;
+    const int NX = g.NX, NY = g.NY, NZ = g.NZ;
+    const size_t NXY = (size_t)NX * NY;
+    const bool coll = g.scheme == TC_SCHEME_COLLOC;
+    double s[NDIAG];
+#pragma unroll
+    for (int k = 0; k < NDIAG; k++) s[k] = 0;
+    double mconv = 0, mvisc = 0, mboth = 0;
+    const double ihx = g.inv_hx, ihy = g.inv_hy;
+    const double ihz = coll ? 1.0 / (double)a.m.cellh[z] : 1.0 / (double)a.m.DZ[z];
+    const double kv = coll ? (g.visc_type == TC_VISC_GALERKIN ? 2.0 : 1.0) : (g.visc_type != TC_VISC_CROSS ? 2.0 : 1.0);
+    const double lap = ihx * ihx + ihy * ihy + ihz * ihz;
+    for (size_t j = threadIdx.x; j < NXY; j += blockDim.x) {
+        const size_t id = (size_t)z * NXY + j;
+        const double u = a.v.c[0][id], v = a.v.c[1][id], w = a.v.c[2][id];
+        const double wc = coll ? w : 0.5 * (w + (z == NZ - 1 ? 0.0 : (double)a.v.c[2][id + NXY]));
+        s[0] += u; s[1] += v; s[2] += wc;
+        s[3] += u * u; s[4] += v * v; s[5] += wc * wc; s[6] += u * v; s[7] += u * wc; s[8] += v * wc;
+        double nt = 0;
+        if (a.nu_t) {
+            s[9] += a.nu_t[id];
+            if (!coll) nt = a.nu_t[id];
+            else if (z != 0 && z != NZ - 1) {
+                const int ix = (int)(j % NX), iy = (int)(j / NX);
+                const int xm = ix == 0 ? NX - 1 : ix - 1, ym = iy == 0 ? NY - 1 : iy - 1;
+                const T* n = a.nu_t;
+                const size_t p0 = (size_t)z * NXY, p1 = p0 - NXY;
+                nt = 0.125 * ((double)n[p0 + iy * NX + ix] + n[p0 + iy * NX + xm] + n[p0 + ym * NX + ix] + n[p0 + ym * NX + xm] +
+                              n[p1 + iy * NX + ix] + n[p1 + iy * NX + xm] + n[p1 + ym * NX + ix] + n[p1 + ym * NX + xm]);
+            }
+        }
+        const double p = a.p ? (double)a.p[id] : 0.0;
+        s[10] += p; s[11] += p * p; s[12] += w; s[13] += w * w;
+        const double cc = a.tau * (fabs(u) * ihx + fabs(v) * ihy + fabs(w) * ihz);
+        const double cv = 4 * kv * a.tau * ((double)g.visc + nt) * lap;
+        mconv = fmax(mconv, cc);
+        mvisc = fmax(mvisc, cv);
+        mboth = fmax(mboth, cc + cv);
+    }
+    __shared__ double sb[NDIAG + 3][8];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < NDIAG; k++) {
+        const double r = warp_sum(s[k]);
+        if (lane == 0) sb[k][wid] = r;
+    }
+    mconv = warp_max(mconv);
+    mvisc = warp_max(mvisc);
+    mboth = warp_max(mboth);
+    if (lane == 0) {
+        sb[NDIAG][wid] = mconv;
+        sb[NDIAG + 1][wid] = mvisc;
+        sb[NDIAG + 2][wid] = mboth;
+    }
+    __syncthreads();
+    if (threadIdx.x < NDIAG + 3) {
+        const int k = threadIdx.x;
+        double r = sb[k][0];
+        for (int w2 = 1; w2 < (int)(blockDim.x >> 5); w2++) r = k < NDIAG ? r + sb[k][w2] : fmax(r, sb[k][w2]);
+        a.planes[(size_t)z * TC_DIAG_STRIDE + k] = r;
+    }
+}
+
+template <typename T>
+void launch_diag(const DiagArgs<T>& a, cudaStream_t s) {
+    k_diag<T><<<a.g.NZ, 256, 0, s>>>(a);
+}
+
+// ---------------------------------------------------------------------------
+// Layout conversions at the host boundary.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_aos_to_soa(const double* __restrict__ src, V3<T> dst, long long n) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        dst.c[0][i] = (T)src[3 * i];
+        dst.c[1][i] = (T)src[3 * i + 1];
+        dst.c[2][i] = (T)src[3 * i + 2];
+    }
+}
+template <typename T>
+__global__ void k_soa_to_aos(CV3<T> src, double* __restrict__ dst, long long n) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        dst[3 * i] = (double)src.c[0][i];
+        dst[3 * i + 1] = (double)src.c[1][i];
+        dst[3 * i + 2] = (double)src.c[2][i];
+    }
+}
+template <typename T>
+__global__ void k_d2t(const double* __restrict__ src, T* __restrict__ dst, long long n) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        dst[i] = (T)src[i];
+}
+template <typename T>
+__global__ void k_t2d(const T* __restrict__ src, double* __restrict__ dst, long long n) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        dst[i] = (double)src[i];
+}
+
+static unsigned conv_blocks(long long n) { return (unsigned)std::min<long long>((n + 255) / 256, 148 * 32); }
+
+template <typename T>
+void launch_aos_to_soa(const double* src, V3<T> dst, long long n, cudaStream_t s) {
+    k_aos_to_soa<T><<<conv_blocks(n), 256, 0, s>>>(src, dst, n);
+}
+template <typename T>
+void launch_soa_to_aos(CV3<T> src, double* dst, long long n, cudaStream_t s) {
+    k_soa_to_aos<T><<<conv_blocks(n), 256, 0, s>>>(src, dst, n);
+}
+template <typename T>
+void launch_d2t(const double* src, T* dst, long long n, cudaStream_t s) {
+    k_d2t<T><<<conv_blocks(n), 256, 0, s>>>(src, dst, n);
+}
+template <typename T>
+void launch_t2d(const T* src, double* dst, long long n, cudaStream_t s) {
+    k_t2d<T><<<conv_blocks(n), 256, 0, s>>>(src, dst, n);
+}
+
+#define TC_INST(T)                                                                 \
+    template void launch_correct<T>(const CorrArgs<T>&, cudaStream_t);            \
+    template void launch_turb<T>(const TurbArgs<T>&, cudaStream_t);               \
+    template void launch_divergence<T>(const DivArgs<T>&, cudaStream_t);          \
+    template void launch_diag<T>(const DiagArgs<T>&, cudaStream_t);               \
+    template void launch_aos_to_soa<T>(const double*, V3<T>, long long, cudaStream_t); \
+    template void launch_soa_to_aos<T>(CV3<T>, double*, long long, cudaStream_t); \
+    template void launch_d2t<T>(const double*, T*, long long, cudaStream_t);      \
+    template void launch_t2d<T>(const T*, double*, long long, cudaStream_t);
+TC_INST(double)
+TC_INST(float)
+#undef TC_INST
+
+}  // namespace tc

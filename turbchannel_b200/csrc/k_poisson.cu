@@ -1,0 +1,433 @@
+// k_poisson.cu -- pressure Poisson solve of the SBDF3 step on sm_100a.
+//
+// The reference solves L p = div(RHS) with a 2-D FFT over each z-plane (cuFFT
+// D2Z / FFTW), one banded solve per (kx, ky) mode along z, the inverse FFT, a 1/NXY
+// scale and a separate normalisation pass (staggered/func_global.h:214-248,
+// 71-189, 657-675).  Here the same algorithm runs as four kernels over a half
+// spectrum laid out spec[z][kx][ky] (ky fastest, kx = 0..NX/2):
+//   k_div_xfft : divergence of the RHS (HW2 :306-312, VV4 :325-333, collocated
+//                collocated_AB3/func_global.h:310-325) computed straight into shared
+//                memory, two rows packed as one complex FFT along x, unpacked to the
+//                half spectrum;
+//   k_yfft     : complex FFT along y of contiguous lines (forward and inverse);
+//   k_zsolve   : banded elimination per mode (tridiagonal for HW2 and collocated,
+//                7-diagonal for VV4) with the pin of the mean mode; the pressure
+//                normalisation only touches mode (0,0), so it is applied there in
+//                spectral space instead of as a separate pass;
+//   k_ixfft    : inverse real FFT along x (two rows per complex FFT) and the 1/NXY
+//                scale, writing p.
+// In the mixed mode the modes with small |k| (including (0,0)) are solved in
+// double from the float spectrum; all others in float.
+#include <algorithm>
+
+#include "kernels.cuh"
+#include "stencil_div.cuh"
+
+namespace tc {
+
+// ---------------------------------------------------------------------------
+// divergence + forward x-FFT
+// ---------------------------------------------------------------------------
+template <typename T, int SCHEME, bool SCALAR>
+__global__ void __launch_bounds__(256) k_div_xfft(DivFftArgs<T> a, int rows) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const Geom& g = a.g;
+    const int NX = g.NX, NY = g.NY, NXH = g.NXH;
+    const int nl = rows >> 1;
+    cplx<T>* A = reinterpret_cast<cplx<T>*>(smraw);
+    cplx<T>* B = A + nl * NX;
+    const int z = blockIdx.y, y0 = blockIdx.x * rows;
+    T* Ar = reinterpret_cast<T*>(A);
+    for (int e = threadIdx.x; e < rows * NX; e += blockDim.x) {
+        const int r = e / NX, x = e - r * NX;
+        Ar[2 * ((r >> 1) * NX + x) + (r & 1)] = div_at<T, SCHEME, SCALAR>(g, a.m, a.v, a.src_scalar, x, y0 + r, z);
+    }
+    const cplx<T>* R = fft_lines(A, B, nl, NX, a.px, a.twx, -1);
+    for (int e = threadIdx.x; e < NXH * rows; e += blockDim.x) {
+        const int kx = e / rows, r = e - kx * rows, l = r >> 1;
+        const cplx<T> Zk = R[l * NX + kx], Zm = R[l * NX + (kx == 0 ? 0 : NX - kx)];
+        cplx<T> val;
+        if ((r & 1) == 0) val = {T(0.5) * (Zk.x + Zm.x), T(0.5) * (Zk.y - Zm.y)};
+        else val = {T(0.5) * (Zk.y + Zm.y), -T(0.5) * (Zk.x - Zm.x)};
+        a.spec[((size_t)z * NXH + kx) * NY + y0 + r] = val;
+    }
+}
+
+static int pick_rows(int NX, int NY, size_t cbytes) {
+    for (int r : {8, 4, 2})
+        if (NY % r == 0 && (size_t)r * NX * cbytes <= 100 * 1024) return r;
+    return 2;
+}
+
+template <typename T>
+void launch_div_xfft(const DivFftArgs<T>& a, cudaStream_t s) {
+    const int rows = pick_rows(a.g.NX, a.g.NY, sizeof(cplx<T>));
+    const size_t smem = (size_t)rows * a.g.NX * sizeof(cplx<T>);
+    dim3 grid(a.g.NY / rows, a.g.NZ);
+#define TC_LDX(SCH, SC)                                                                                 \
+    {                                                                                                   \
+        auto k = k_div_xfft<T, SCH, SC>;                                                                \
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);               \
+        k<<<grid, 256, smem, s>>>(a, rows);                                                             \
+    }
+    if (a.src_scalar) TC_LDX(TC_SCHEME_HW2, true)
+    else if (a.g.scheme == TC_SCHEME_HW2) TC_LDX(TC_SCHEME_HW2, false)
+    else if (a.g.scheme == TC_SCHEME_VV4) TC_LDX(TC_SCHEME_VV4, false)
+    else TC_LDX(TC_SCHEME_COLLOC, false)
+#undef TC_LDX
+}
+
+// ---------------------------------------------------------------------------
+// y-FFT on contiguous lines
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) k_yfft(YFftArgs<T> a, int lines) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const int NY = a.g.NY;
+    const long long total = (long long)a.g.NZ * a.g.NXH;
+    const long long L0 = (long long)blockIdx.x * lines;
+    const int nl = (int)min((long long)lines, total - L0);
+    cplx<T>* A = reinterpret_cast<cplx<T>*>(smraw);
+    cplx<T>* B = A + lines * NY;
+    cplx<T>* src = a.spec + L0 * NY;
+    for (int e = threadIdx.x; e < nl * NY; e += blockDim.x) A[e] = src[e];
+    const cplx<T>* R = fft_lines(A, B, nl, NY, a.py, a.twy, a.sign);
+    for (int e = threadIdx.x; e < nl * NY; e += blockDim.x) src[e] = R[e];
+}
+
+template <typename T>
+void launch_yfft(const YFftArgs<T>& a, cudaStream_t s) {
+    int lines = std::max(1, std::min(16, 4096 / a.g.NY));
+    while (lines > 1 && (size_t)2 * lines * a.g.NY * sizeof(cplx<T>) > 96 * 1024) lines >>= 1;
+    const size_t smem = (size_t)2 * lines * a.g.NY * sizeof(cplx<T>);
+    const long long total = (long long)a.g.NZ * a.g.NXH;
+    auto k = k_yfft<T>;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k<<<(unsigned)((total + lines - 1) / lines), 256, smem, s>>>(a, lines);
+}
+
+// ---------------------------------------------------------------------------
+// Banded z-solve per mode
+// ---------------------------------------------------------------------------
+template <typename C, typename T>
+__device__ __forceinline__ const C* pickm(const T* t, const double* d) {
+    if constexpr (sizeof(C) == sizeof(double)) return reinterpret_cast<const C*>(d);
+    else return reinterpret_cast<const C*>(t);
+}
+
+template <typename C, typename T>
+__device__ __forceinline__ cplx<C> ldc(const cplx<T>* p) {
+    const cplx<T> v = *p;
+    return {(C)v.x, (C)v.y};
+}
+template <typename C, typename T>
+__device__ __forceinline__ void stc(cplx<T>* p, cplx<C> v) {
+    *p = {(T)v.x, (T)v.y};
+}
+
+// Mean-mode normalisation in spectral space (equivalent to NormalizePressure
+// applied after the inverse FFT): x_iz -= NXY * p_shift * profile_iz.
+template <typename T>
+__device__ void normalize_mean_mode(const ZSolveArgs<T>& a) {
+    const Geom& g = a.g;
+    const size_t zs = (size_t)g.NXH * g.NY;
+    cplx<T>* x = a.spec;
+    double psum = 0;
+    if (g.scheme == TC_SCHEME_VV4) {
+        for (int i = 0; i < g.NZ; i++) psum += (double)x[i * zs].x * a.m.dKERG[i] * a.m.dDZ[i];
+        const double c = psum / a.m.KERG_norm2;
+        for (int i = 0; i < g.NZ; i++) x[i * zs].x = (T)((double)x[i * zs].x - c * a.m.dKERG[i]);
+    } else if (g.scheme == TC_SCHEME_HW2) {
+        for (int i = 0; i < g.NZ; i++) psum += (double)x[i * zs].x * a.m.dDZ[i];
+        const double c = psum / (a.m.dZZ[g.NZ] - a.m.dZZ[0]);
+        for (int i = 0; i < g.NZ; i++) x[i * zs].x = (T)((double)x[i * zs].x - c);
+    } else {
+        // collocated_AB3/func_global.h:163-170 (shift = sum(p vol) hx hy / area)
+        for (int i = 0; i < g.NZ; i++) psum += (double)x[i * zs].x * (a.m.dcellh[i] * g.hx * g.hy);
+        const double c = (double)g.NXY * (psum * g.hx * g.hy / g.area);
+        for (int i = 0; i < g.NZ; i++) x[i * zs].x = (T)((double)x[i * zs].x - c);
+    }
+}
+
+template <typename C, typename T, int SCHEME>
+__device__ void zsolve_mode(const ZSolveArgs<T>& a, int kx, int ky, C* sc) {
+    const Geom& g = a.g;
+    const int NZ = g.NZ;
+    const size_t M = (size_t)g.NXH * g.NY;
+    const size_t m = (size_t)kx * g.NY + ky;
+    cplx<T>* x = a.spec + m;
+    const size_t zs = M;  // spec stride between z-planes
+    const bool pin = (kx == 0 && ky == 0);
+    if (SCHEME == TC_SCHEME_HW2 || SCHEME == TC_SCHEME_COLLOC) {
+        const C* MA = pickm<C>(a.m.MAT_A, a.m.dMAT_A);
+        const C* DZ = SCHEME == TC_SCHEME_HW2 ? pickm<C>(a.m.DZ, a.m.dDZ) : pickm<C>(a.m.DZ, a.m.dDZ);
+        C MM;
+        if (SCHEME == TC_SCHEME_HW2) {
+            MM = 2 * ((1 - (C)a.tabs.cosx[kx]) * (C)g.inv_hx * (C)g.inv_hx + (1 - (C)a.tabs.cosy[ky]) * (C)g.inv_hy * (C)g.inv_hy);
+        } else {
+            MM = (1 - (C)a.tabs.cosx[kx]) * (C)g.hy / (C)g.hx + (1 - (C)a.tabs.cosy[ky]) * (C)g.hx / (C)g.hy;
+        }
+        C b0;
+        if (SCHEME == TC_SCHEME_HW2) b0 = -DZ[0] * MM - MA[1];
+        else {
+            b0 = -MA[1];
+            if (!g.fd_mode) b0 += DZ[0] * MM;
+        }
+        if (pin) b0 *= 2;
+        const C ib0 = 1 / b0;
+        cplx<C> prev = ldc<C>(x);
+        prev.x *= ib0;
+        prev.y *= ib0;
+        stc(x, prev);
+        C pp = MA[1] * ib0;
+        sc[0] = pp;
+        for (int i = 1; i <= NZ - 1; i++) {
+            C d;
+            if (SCHEME == TC_SCHEME_HW2) {
+                d = -MA[i] - DZ[i] * MM;
+                if (i != NZ - 1) d -= MA[i + 1];
+            } else {
+                const C mm = (g.fd_mode && (i == NZ - 1)) ? C(0) : MM;
+                d = 0;
+                d -= MA[i] + DZ[i - 1] * mm;
+                if (i != NZ - 1) d -= MA[i + 1] + DZ[i] * mm;
+            }
+            d -= MA[i] * pp;
+            d = 1 / d;
+            if (i != NZ - 1) {
+                pp = MA[i + 1] * d;
+                sc[(size_t)i * M] = pp;
+            }
+            cplx<C> xi = ldc<C>(x + i * zs);
+            xi.x = (xi.x - MA[i] * prev.x) * d;
+            xi.y = (xi.y - MA[i] * prev.y) * d;
+            stc(x + i * zs, xi);
+            prev = xi;
+        }
+        for (int i = NZ - 2; i >= 0; i--) {
+            cplx<C> xi = ldc<C>(x + i * zs);
+            const C p = sc[(size_t)i * M];
+            xi.x -= prev.x * p;
+            xi.y -= prev.y * p;
+            stc(x + i * zs, xi);
+            prev = xi;
+        }
+    } else {  // VV4, staggered/func_global.h:110-189
+        const C* MA = pickm<C>(a.m.MAT_A, a.m.dMAT_A);
+        const C* DZ = pickm<C>(a.m.DZ, a.m.dDZ);
+        const C* DZW = pickm<C>(a.m.DZW, a.m.dDZW);
+        const C C27 = C(0.03703703703703703703), C9 = C(0.11111111111111111111);
+        const C sx = (C)a.tabs.sinx[kx], sy = (C)a.tabs.siny[ky];
+        const C s3x = 3 * sx - 4 * sx * sx * sx, s3y = 3 * sy - 4 * sy * sy * sy;
+        const C ihx = (C)g.inv_hx, ihy = (C)g.inv_hy;
+        const C tiny = C(1e-30);
+        C b[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};  // b[j][k]: row i-3+j, coefficient of x_{row+k+1}
+        cplx<C> xr[3] = {{0, 0}, {0, 0}, {0, 0}};       // eliminated rhs of rows i-3, i-2, i-1
+        for (int i = 0; i < NZ; i++) {
+            C row[7] = {0, 0, 0, 0, 0, 0, 0};
+            C sum = 0;
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                if (i + k - 3 < 0 || i + k - 3 >= NZ) continue;
+                row[k] = MA[i * 3 + k];
+                sum += MA[i * 3 + k];
+            }
+#pragma unroll
+            for (int k = 1; k <= 3; k++) {
+                if (i + k >= NZ) continue;
+                row[3 + k] = MA[(i + k) * 3 + 3 - k];
+                sum += MA[(i + k) * 3 + 3 - k];
+            }
+            if (i <= 2) row[3] = (C)a.m.MAT_D[i];
+            else if (i >= NZ - 3) row[3] = (C)a.m.MAT_D[i - (NZ - 3) + 3];
+            else row[3] = -sum;
+            if (pin && i == 0) row[3] *= 2;
+            {
+                C ci = DZ[i] * sx - C27 * DZW[i] * s3x;
+                row[3] -= 4 * ihx * ihx * ci * ci / (DZ[i] - C9 * DZW[i]);
+                ci = DZ[i] * sy - C27 * DZW[i] * s3y;
+                row[3] -= 4 * ihy * ihy * ci * ci / (DZ[i] - C9 * DZW[i]);
+            }
+            cplx<C> xi = ldc<C>(x + (size_t)i * zs);
+#pragma unroll
+            for (int j = -3; j < 0; j++) {
+                if (i + j < 0) continue;
+                const C mult = -row[3 + j];
+#pragma unroll
+                for (int k = 1; k <= 3; k++) {
+                    if (i + j + k >= NZ) continue;
+                    row[3 + j + k] += mult * b[3 + j][k - 1];
+                }
+                xi.x += mult * xr[3 + j].x;
+                xi.y += mult * xr[3 + j].y;
+            }
+            if (fabs((double)row[3]) < (double)tiny) {
+                if (a.err_flag) atomicExch(a.err_flag, 1);
+                cplx<T> bad = {(T)(sizeof(T) == 8 ? -1e50 : -1e30), (T)0};
+                x[0] = bad;
+                return;
+            }
+            const C mult = C(1) / row[3];
+            C nb[3];
+#pragma unroll
+            for (int k = 1; k <= 3; k++) nb[k - 1] = (i + k >= NZ) ? C(0) : row[3 + k] * mult;
+            xi.x *= mult;
+            xi.y *= mult;
+            stc(x + (size_t)i * zs, xi);
+#pragma unroll
+            for (int k = 0; k < 3; k++) sc[((size_t)i * 3 + k) * M] = nb[k];
+#pragma unroll
+            for (int j = 0; j < 2; j++) {
+                xr[j] = xr[j + 1];
+#pragma unroll
+                for (int k = 0; k < 3; k++) b[j][k] = b[j + 1][k];
+            }
+            xr[2] = xi;
+#pragma unroll
+            for (int k = 0; k < 3; k++) b[2][k] = nb[k];
+        }
+        cplx<C> xs[3] = {{0, 0}, {0, 0}, {0, 0}};  // x_{i+1}, x_{i+2}, x_{i+3}
+        for (int i = NZ - 1; i >= 0; i--) {
+            cplx<C> xi = ldc<C>(x + (size_t)i * zs);
+#pragma unroll
+            for (int j = 1; j <= 3; j++) {
+                if (i + j >= NZ) continue;
+                const C bb = sc[((size_t)i * 3 + j - 1) * M];
+                xi.x -= bb * xs[j - 1].x;
+                xi.y -= bb * xs[j - 1].y;
+            }
+            stc(x + (size_t)i * zs, xi);
+            xs[2] = xs[1];
+            xs[1] = xs[0];
+            xs[0] = xi;
+        }
+    }
+}
+
+// All modes (FP64) or, in the mixed mode, all modes outside the low set (float).
+template <typename C, typename T, int SCHEME>
+__global__ void __launch_bounds__(128) k_zsolve_all(ZSolveArgs<T> a, int skip_low) {
+    const Geom& g = a.g;
+    const size_t M = (size_t)g.NXH * g.NY;
+    const size_t m = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= M) return;
+    const int kx = (int)(m / g.NY), ky = (int)(m - (size_t)kx * g.NY);
+    const int LM = g.low_modes;
+    if (skip_low && kx < LM && (ky < LM || ky > g.NY - LM)) return;
+    zsolve_mode<C, T, SCHEME>(a, kx, ky, reinterpret_cast<C*>(a.scratch) + m);
+    if (!skip_low && m == 0) normalize_mean_mode(a);
+}
+
+// The low-|k| modes (kx < LM, |ky| < LM) in double; mode (0,0) also normalised.
+template <typename T, int SCHEME>
+__global__ void __launch_bounds__(64) k_zsolve_low(ZSolveArgs<T> a) {
+    const Geom& g = a.g;
+    const int LM = g.low_modes, nky = 2 * LM - 1;
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= LM * nky) return;
+    const int kx = idx / nky, j = idx - kx * nky;
+    const int ky = j < LM ? j : g.NY - (j - LM + 1);
+    if (kx >= g.NXH || ky < 0 || ky >= g.NY) return;
+    const size_t M = (size_t)g.NXH * g.NY;
+    const size_t m = (size_t)kx * g.NY + ky;
+    zsolve_mode<double, T, SCHEME>(a, kx, ky, reinterpret_cast<double*>(a.scratch) + m);
+    if (m == 0) normalize_mean_mode(a);
+    (void)M;
+}
+
+size_t zsolve_scratch_bytes(const Geom& g, int elem_bytes) {
+    (void)elem_bytes;
+    const int nc = g.scheme == TC_SCHEME_VV4 ? 3 : 1;
+    return (size_t)g.NXH * g.NY * g.NZ * nc * sizeof(double);
+}
+
+template <typename T, int SCHEME>
+static void zsolve_scheme(const ZSolveArgs<T>& a, cudaStream_t s) {
+    const size_t M = (size_t)a.g.NXH * a.g.NY;
+    if (sizeof(T) == sizeof(double)) {
+        k_zsolve_all<double, T, SCHEME><<<(unsigned)((M + 127) / 128), 128, 0, s>>>(a, 0);
+    } else {
+        // Modes outside the low set in float first, then the low set in double.  Both
+        // launches share the scratch buffer, which is sized for double entries; the
+        // float kernel indexes it as float (so the low-set double entries are disjoint
+        // only in time: the launches are stream-ordered).
+        k_zsolve_all<float, T, SCHEME><<<(unsigned)((M + 127) / 128), 128, 0, s>>>(a, 1);
+        const int nlow = a.g.low_modes * (2 * a.g.low_modes - 1);
+        k_zsolve_low<T, SCHEME><<<(nlow + 63) / 64, 64, 0, s>>>(a);
+    }
+}
+
+template <typename T>
+void launch_zsolve(const ZSolveArgs<T>& a, cudaStream_t s) {
+    if (a.g.scheme == TC_SCHEME_VV4) zsolve_scheme<T, TC_SCHEME_VV4>(a, s);
+    else if (a.g.scheme == TC_SCHEME_HW2) zsolve_scheme<T, TC_SCHEME_HW2>(a, s);
+    else zsolve_scheme<T, TC_SCHEME_COLLOC>(a, s);
+}
+
+// ---------------------------------------------------------------------------
+// inverse x-FFT (complex-to-real, two rows per complex FFT) and scaling
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) k_ixfft(IxFftArgs<T> a, int rows) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const Geom& g = a.g;
+    const int NX = g.NX, NY = g.NY, NXH = g.NXH;
+    const int nl = rows >> 1;
+    cplx<T>* A = reinterpret_cast<cplx<T>*>(smraw);
+    cplx<T>* B = A + nl * NX;  // also holds the loaded tile (rows x NXH)
+    cplx<T>* tile = B;
+    const int z = blockIdx.y, y0 = blockIdx.x * rows;
+    for (int e = threadIdx.x; e < NXH * rows; e += blockDim.x) {
+        const int kx = e / rows, r = e - kx * rows;
+        tile[r * NXH + kx] = a.spec[((size_t)z * NXH + kx) * NY + y0 + r];
+    }
+    __syncthreads();
+    const int nh = NX / 2;
+    for (int e = threadIdx.x; e < nl * NX; e += blockDim.x) {
+        const int l = e / NX, k = e - l * NX;
+        const int ra = 2 * l, rb = 2 * l + 1;
+        cplx<T> av, bv;
+        if (k <= nh) {
+            av = tile[ra * NXH + k];
+            bv = tile[rb * NXH + k];
+        } else {
+            av = tile[ra * NXH + NX - k];
+            bv = tile[rb * NXH + NX - k];
+            av.y = -av.y;
+            bv.y = -bv.y;
+        }
+        if (k == 0 || k == nh) {
+            av.y = 0;
+            bv.y = 0;
+        }
+        A[l * NX + k] = {av.x - bv.y, av.y + bv.x};
+    }
+    const cplx<T>* R = fft_lines(A, B, nl, NX, a.px, a.twx, +1);
+    const T sc = a.scale;
+    for (int e = threadIdx.x; e < rows * NX; e += blockDim.x) {
+        const int r = e / NX, x = e - r * NX;
+        const cplx<T> zv = R[(r >> 1) * NX + x];
+        a.p[((size_t)z * NY + y0 + r) * NX + x] = ((r & 1) ? zv.y : zv.x) * sc;
+    }
+}
+
+template <typename T>
+void launch_ixfft(const IxFftArgs<T>& a, cudaStream_t s) {
+    const int rows = pick_rows(a.g.NX, a.g.NY, sizeof(cplx<T>));
+    const size_t nl = rows / 2;
+    const size_t smem = (nl * a.g.NX + std::max(nl * a.g.NX, (size_t)rows * a.g.NXH)) * sizeof(cplx<T>);
+    auto k = k_ixfft<T>;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k<<<dim3(a.g.NY / rows, a.g.NZ), 256, smem, s>>>(a, rows);
+}
+
+template void launch_div_xfft<double>(const DivFftArgs<double>&, cudaStream_t);
+template void launch_div_xfft<float>(const DivFftArgs<float>&, cudaStream_t);
+template void launch_yfft<double>(const YFftArgs<double>&, cudaStream_t);
+template void launch_yfft<float>(const YFftArgs<float>&, cudaStream_t);
+template void launch_zsolve<double>(const ZSolveArgs<double>&, cudaStream_t);
+template void launch_zsolve<float>(const ZSolveArgs<float>&, cudaStream_t);
+template void launch_ixfft<double>(const IxFftArgs<double>&, cudaStream_t);
+template void launch_ixfft<float>(const IxFftArgs<float>&, cudaStream_t);
+
+}  // namespace tc

@@ -1,0 +1,156 @@
+// kernels.cuh -- argument blocks and host launchers of the sm_100a kernels.
+// Internal to turbchannel_b200 (tc_api.cu is the only caller).
+#pragma once
+#include "tc_common.cuh"
+
+namespace tc {
+
+template <typename T>
+struct V3 {
+    T* c[3];
+};
+template <typename T>
+struct CV3 {
+    const T* c[3];
+};
+
+// Fused explicit flux + SBDF3 combine (one pass over v_n and the history).
+//   F_n = (sour_dpdx,0,0) + Conv(v_n) + Visc(v_n)          -> fout
+//   RHS = a0 F_n + a1 F_{n-1} + a2 F_{n-2} + inv_tau (b0 v_n + b1 v_{n-1} + b2 v_{n-2})
+//         (staggered/func_global.h:910-932)                 -> rhs
+//   collocated StabType 1 also subtracts grad p_n (collocated_AB3/func_global.h:436-437).
+//   The weighted sum of RHS_x (bulk velocity of the result, up to tau/bd0) is
+//   reduced deterministically into ub_out when ub_out != nullptr.
+template <typename T>
+struct FluxArgs {
+    Geom g;
+    MeshDev<T> m;
+    CV3<T> vel, velp, velq, fp, fq;
+    V3<T> fout, rhs;
+    const T* nu_t;
+    const T* pcur;
+    T inv_tau;
+    int order;  // 0: F_n only (operator form), 1..3: SBDF order
+    double* ub_partial;
+    unsigned* ticket;
+    double* ub_out;
+};
+
+// Divergence of the RHS fused with the forward real FFT along x.  Output: half
+// spectrum spec[z][kx][y] (kx = 0..NX/2, y fastest).  src_scalar != nullptr: the
+// input is a scalar field (already a divergence / a pressure RHS) instead.
+template <typename T>
+struct DivFftArgs {
+    Geom g;
+    MeshDev<T> m;
+    CV3<T> v;
+    const T* src_scalar;
+    cplx<T>* spec;
+    FftPlan px;
+    const cplx<T>* twx;
+};
+
+// In-place complex FFT along y of the lines spec[z][kx][0..NY).
+template <typename T>
+struct YFftArgs {
+    Geom g;
+    cplx<T>* spec;
+    FftPlan py;
+    const cplx<T>* twy;
+    int sign;
+};
+
+// Banded wall-normal solve per (kx, ky) mode, in place on spec; normalisation of
+// the mean mode (staggered/func_global.h:657-675) applied to mode (0, 0).
+template <typename T>
+struct ZSolveArgs {
+    Geom g;
+    MeshDev<T> m;
+    ModeTabs tabs;
+    cplx<T>* spec;
+    void* scratch;  // per-mode elimination coefficients
+    int* err_flag;  // set when a pivot underflows (the reference writes -1e50)
+};
+
+// Inverse real FFT along x: p = scale * C2R(spec) (+ dest layout [z][y][x]).
+template <typename T>
+struct IxFftArgs {
+    Geom g;
+    const cplx<T>* spec;
+    T* p;
+    FftPlan px;
+    const cplx<T>* twx;
+    T scale;
+};
+
+// Velocity correction v_{n+1} = (RHS - G p) tau/bd0 (+ uniform flow-rate shift of u);
+// collocated StabType 1 also p_{n+1} += p_n.
+template <typename T>
+struct CorrArgs {
+    Geom g;
+    MeshDev<T> m;
+    CV3<T> rhs;
+    const T* p;       // pressure (or pressure increment) whose gradient is removed
+    V3<T> vout;
+    const T* pcur;    // StabType 1: p_n
+    T* pnext;         // StabType 1: p_{n+1} = p + p_n
+    T tob;            // tau / bd0
+    int cfr;          // 1: apply the flow-rate shift
+    double cfr_target;
+    double cfr_scale;      // hx hy / area: bulk velocity = ub_sum * cfr_scale * tob
+    double cfr_volfac;     // area / fluid volume receiving the shift
+    const double* ub_sum;  // sum of RHS_x weights from the flux kernel
+    double* du_out;        // shift applied (for tc_last_dpdx)
+    int grad_only;         // operator form: vout = G p
+};
+
+template <typename T>
+struct TurbArgs {
+    Geom g;
+    MeshDev<T> m;
+    CV3<T> v;
+    T* nu_t;
+};
+
+template <typename T>
+struct DivArgs {
+    Geom g;
+    MeshDev<T> m;
+    CV3<T> v;
+    T* dv;
+};
+
+// Per-plane diagnostics (profiles, integral, KE and CFL ingredients), double.
+template <typename T>
+struct DiagArgs {
+    Geom g;
+    MeshDev<T> m;
+    CV3<T> v;
+    const T* p;
+    const T* nu_t;
+    double tau;
+    double* planes;  // NZ x TC_DIAG_STRIDE
+};
+constexpr int TC_DIAG_STRIDE = 19;
+
+template <typename T> void launch_flux_stag(const FluxArgs<T>& a, cudaStream_t s);
+template <typename T> void launch_flux_coll(const FluxArgs<T>& a, cudaStream_t s);
+template <typename T> void launch_div_xfft(const DivFftArgs<T>& a, cudaStream_t s);
+template <typename T> void launch_yfft(const YFftArgs<T>& a, cudaStream_t s);
+template <typename T> void launch_zsolve(const ZSolveArgs<T>& a, cudaStream_t s);
+template <typename T> void launch_ixfft(const IxFftArgs<T>& a, cudaStream_t s);
+template <typename T> void launch_correct(const CorrArgs<T>& a, cudaStream_t s);
+template <typename T> void launch_turb(const TurbArgs<T>& a, cudaStream_t s);
+template <typename T> void launch_divergence(const DivArgs<T>& a, cudaStream_t s);
+template <typename T> void launch_diag(const DiagArgs<T>& a, cudaStream_t s);
+
+// AoS double <-> SoA T conversions (host boundary), and misc.
+template <typename T> void launch_aos_to_soa(const double* src, V3<T> dst, long long n, cudaStream_t s);
+template <typename T> void launch_soa_to_aos(CV3<T> src, double* dst, long long n, cudaStream_t s);
+template <typename T> void launch_d2t(const double* src, T* dst, long long n, cudaStream_t s);
+template <typename T> void launch_t2d(const T* src, double* dst, long long n, cudaStream_t s);
+
+size_t zsolve_scratch_bytes(const Geom& g, int elem_bytes);
+int flux_grid_blocks(const Geom& g);
+
+}  // namespace tc

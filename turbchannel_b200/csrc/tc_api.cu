@@ -1,0 +1,1031 @@
+// tc_api.cu -- host orchestration and the C ABI (include/turbch.h).
+//
+// A tc_handle owns everything the reference's `struct data` owns
+// (staggered/data_global_inc.h:11-76): the 4-level rings vel/flux/pres, nu_t, the
+// spectrum buffer and the mesh-derived arrays, here on one CUDA device and one
+// stream.  Fields are stored structure-of-arrays in the working precision; the
+// boundary converts from/to the reference's AoS double layout.  One step is
+// seven launches (eight with a Smagorinsky model):
+//   flux+combine -> div+xFFT -> yFFT -> zsolve -> inverse yFFT -> inverse xFFT -> correction
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <random>
+#include <string>
+#include <vector>
+
+#include "kernels.cuh"
+
+using namespace tc;
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+static thread_local std::string g_err;
+static int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+#define TC_CUDA(call)                                                                         \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess) return fail(TC_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+extern "C" const char* tc_last_error(void) { return g_err.c_str(); }
+extern "C" const char* tc_version(void) { return "turbchannel_b200 0.1 (sm_100a)"; }
+
+// ---------------------------------------------------------------------------
+// Mesh-derived data on the host (double).  Staggered: staggered/main.cpp:112-156
+// (InitDerivativeMeshData) with FillMatrix (:12-48) and the banded elimination of
+// :74-109 for the null vector of the VV4 gradient.  Collocated:
+// collocated_AB3/main.cpp:238-300.
+// ---------------------------------------------------------------------------
+struct HostMesh {
+    std::vector<double> ZZ, DZ, DZW, GC1, GC2, GCZ, KERG, MAT_A, cellh;
+    double MAT_D[6] = {0, 0, 0, 0, 0, 0};
+    double KERG_norm2 = 0;
+};
+
+static int banded_solve(int N, int NB, std::vector<double>& M, std::vector<double>& x, double tiny) {
+    const int w = NB / 2;
+    for (int i = 0; i < N; i++) {
+        for (int j = -w; j < 0; j++) {
+            if (i + j < 0) continue;
+            const double mult = -M[i * NB + w + j];
+            for (int k = 0; k <= w; k++) {
+                if (i + j + k >= N) continue;
+                M[i * NB + (w + j) + k] += mult * M[(i + j) * NB + w + k];
+            }
+            x[i] += mult * x[i + j];
+        }
+        if (std::fabs(M[i * NB + w]) < tiny) return 2;
+        const double mult = 1.0 / M[i * NB + w];
+        for (int k = 0; k <= w; k++)
+            if (i + k < N) M[i * NB + w + k] *= mult;
+        x[i] *= mult;
+    }
+    for (int i = N - 1; i >= 0; i--)
+        for (int j = 1; j <= w; j++)
+            if (i + j < N) x[i] -= M[i * NB + w + j] * x[i + j];
+    return 0;
+}
+
+// 7-diagonal VV4 z-Laplacian of the xy-constant mode (div o grad with the 4-point
+// stencils; symmetric reflections at the walls).
+static void vv4_matrix(const HostMesh& hm, int NZ, std::vector<double>& M) {
+    const double gc[4] = {1. / 27., -1., 1., -1. / 27.};
+    M.assign((size_t)7 * NZ, 0.0);
+    for (int j = 0; j < NZ; j++)
+        for (int ll = -1; ll <= 2; ll++) {
+            const double c1 = gc[ll + 1];
+            int l = j + ll;
+            if (l == 0 || l == NZ) continue;
+            if (l < 0) l = -l;
+            if (l > NZ) l = 2 * NZ - l;
+            for (int mm = -2; mm <= 1; mm++) {
+                double c2 = gc[mm + 2];
+                int m = l + mm;
+                if (m < 0) { m = -m - 1; c2 = -c2; }
+                if (m >= NZ) { m = 2 * NZ - m - 1; c2 = -c2; }
+                const int pos = m - j + 3;
+                if (pos < 0 || pos >= 7) continue;
+                M[j * 7 + pos] += c1 * c2 * hm.GCZ[l];
+            }
+        }
+}
+
+static int build_mesh(const tc_params& p, const double* zz, HostMesh& hm) {
+    const int NZ = p.NZ;
+    if (p.scheme == TC_SCHEME_COLLOC) {
+        hm.ZZ.assign(zz, zz + NZ);
+        hm.DZ.assign(NZ, 0.0);
+        for (int i = 0; i < NZ - 1; i++) hm.DZ[i] = hm.ZZ[i + 1] - hm.ZZ[i];
+        hm.MAT_A.assign(NZ, 0.0);
+        for (int j = 1; j < NZ; j++) hm.MAT_A[j] = p.hx * p.hy / hm.DZ[j - 1];
+        if (p.fd_mode) {
+            hm.MAT_A[1] *= 0.5;
+            hm.MAT_A[NZ - 1] *= 0.5;
+        }
+        hm.cellh.assign(NZ, 0.0);
+        for (int iz = 0; iz < NZ; iz++)
+            hm.cellh[iz] = iz == 0 ? 0.5 * hm.DZ[0] : iz == NZ - 1 ? 0.5 * hm.DZ[NZ - 2] : 0.5 * (hm.DZ[iz - 1] + hm.DZ[iz]);
+        hm.DZW = hm.GC1 = hm.GC2 = hm.GCZ = hm.KERG = std::vector<double>(NZ, 0.0);
+        return 0;
+    }
+    hm.ZZ.assign(zz, zz + NZ + 1);
+    hm.DZ.assign(NZ, 0.0);
+    for (int i = 0; i < NZ; i++) hm.DZ[i] = hm.ZZ[i + 1] - hm.ZZ[i];
+    hm.cellh = hm.DZ;
+    hm.DZW = hm.GC1 = hm.GC2 = hm.GCZ = hm.KERG = std::vector<double>(NZ, 0.0);
+    if (p.scheme == TC_SCHEME_HW2) {
+        hm.MAT_A.assign(NZ, 0.0);
+        for (int j = 1; j <= NZ - 1; j++) hm.MAT_A[j] = 2. / (hm.DZ[j - 1] + hm.DZ[j]);
+        return 0;
+    }
+    const std::vector<double>& DZ = hm.DZ;
+    for (int iz = 0; iz < NZ; iz++) {
+        hm.DZW[iz] = (DZ[iz] + DZ[iz == 0 ? iz : iz - 1] + DZ[iz == NZ - 1 ? iz : iz + 1]) / 3.;
+        hm.GC1[iz] = DZ[iz] / (DZ[iz] - hm.DZW[iz] / 9.);
+        hm.GC2[iz] = -(1. / 27.) * hm.DZW[iz] / (DZ[iz] - hm.DZW[iz] / 9.);
+        hm.GCZ[iz] = iz == 0 ? 0.0  // no w-DOF on the bottom wall: never used
+                             : 1 / (0.5 * (DZ[iz] + DZ[iz - 1]) -
+                                    (1. / 27.) * (DZ[iz] + DZ[iz - 1] + 0.5 * (DZ[iz == NZ - 1 ? iz : iz + 1] + DZ[iz == 1 ? 0 : iz - 2])));
+    }
+    std::vector<double> M;
+    vv4_matrix(hm, NZ, M);
+    hm.MAT_A.assign((size_t)3 * NZ, 0.0);
+    for (int iz = 0; iz < NZ; iz++)
+        for (int i = 0; i < 3; i++) hm.MAT_A[iz * 3 + i] = (iz + i - 3 >= 0) ? M[iz * 7 + i] : 0.0;
+    hm.MAT_D[0] = M[3];
+    hm.MAT_D[1] = M[7 + 3];
+    hm.MAT_D[2] = M[14 + 3];
+    hm.MAT_D[3] = M[(NZ - 3) * 7 + 3];
+    hm.MAT_D[4] = M[(NZ - 2) * 7 + 3];
+    hm.MAT_D[5] = M[(NZ - 1) * 7 + 3];
+    std::vector<double> T3((size_t)3 * NZ, 0.0), K(NZ, 1.0);
+    const double eps = 1. / 27.;
+    T3[1] = -1;
+    T3[2] = eps;
+    for (int iz = 1; iz < NZ - 1; iz++) {
+        T3[iz * 3 + 0] = T3[iz * 3 + 2] = eps;
+        T3[iz * 3 + 1] = -1 + eps;
+    }
+    T3[(NZ - 1) * 3] = eps;
+    T3[(NZ - 1) * 3 + 1] = -1;
+    if (banded_solve(NZ, 3, T3, K, 1e-10)) return 1;
+    hm.KERG = K;
+    hm.KERG_norm2 = 0;
+    for (int iz = 0; iz < NZ; iz++) hm.KERG_norm2 += K[iz] * K[iz] * DZ[iz];
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// The handle
+// ---------------------------------------------------------------------------
+static int plan_fft(int n, FftPlan& P) {
+    P.n = n;
+    P.nf = 0;
+    int m = n;
+    while (m % 4 == 0 && P.nf < FFT_MAXF) { P.fac[P.nf++] = 4; m /= 4; }
+    while (m % 2 == 0 && P.nf < FFT_MAXF) { P.fac[P.nf++] = 2; m /= 2; }
+    while (m % 3 == 0 && P.nf < FFT_MAXF) { P.fac[P.nf++] = 3; m /= 3; }
+    return m == 1 ? 0 : 1;
+}
+
+struct tc_handle {
+    tc_params prm;
+    Geom g;
+    HostMesh hm;
+    cudaStream_t st = nullptr;
+    bool fp64 = true;
+    size_t esz = 8;
+    void* vel[4] = {};
+    void* flux[4] = {};
+    void* pres[4] = {};
+    void* nu_t = nullptr;
+    void* ptmp = nullptr;
+    void* spec = nullptr;
+    void* zscr = nullptr;
+    void* mesh_t = nullptr;     // mesh arrays in T
+    double* mesh_d = nullptr;   // mesh arrays in double
+    double* tabs = nullptr;     // cos/sin tables
+    void* tw = nullptr;         // twiddles (x then y), T complex
+    FftPlan px{}, py{};
+    double* red = nullptr;      // [0] ub_sum, [1] du, [2..] partials
+    unsigned* ticket = nullptr;
+    int* err_flag = nullptr;
+    double* planes = nullptr;
+    double* planes_h = nullptr;  // pinned
+    double* stage = nullptr;     // AoS double staging (3N), lazily
+    void* opv = nullptr;         // operator scratch (lazily): vector T
+    void* opf = nullptr;
+    void* ops = nullptr;         // scalar T
+    int nblocks_flux = 0;
+    int forcing_mode = 0;
+    double forcing_value = 0;
+    double last_tau = 0, last_bd0 = 1;
+    int turb_kind = TC_TURB_NONE;
+    // instrumentation
+    unsigned long long launches = 0;
+    bool timing = false;
+    std::vector<cudaEvent_t> ev;  // pool
+    size_t ev_used = 0;
+    int timed_steps = 0;
+    double phase_ms[TC_NPHASE] = {};
+};
+
+// Phase markers of one step: slot k marks the end of phase k-1.
+static void mark(tc_handle* h, int slot, size_t base) {
+    if (!h->timing) return;
+    const size_t idx = base + (size_t)slot;
+    while (h->ev.size() <= idx) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        h->ev.push_back(e);
+    }
+    cudaEventRecord(h->ev[idx], h->st);
+}
+
+template <typename T>
+static V3<T> vec(void* base, long long N) {
+    T* b = (T*)base;
+    return V3<T>{{b, b + N, b + 2 * N}};
+}
+template <typename T>
+static CV3<T> cvec(void* base, long long N) {
+    const T* b = (const T*)base;
+    return CV3<T>{{b, b + N, b + 2 * N}};
+}
+
+template <typename T>
+static MeshDev<T> mesh_dev(const tc_handle* h) {
+    const int NZ = h->g.NZ, L = NZ + 2;
+    const T* t = (const T*)h->mesh_t;
+    const double* d = h->mesh_d;
+    MeshDev<T> m;
+    m.ZZ = t + 0 * L; m.DZ = t + 1 * L; m.DZW = t + 2 * L; m.GC1 = t + 3 * L; m.GC2 = t + 4 * L;
+    m.GCZ = t + 5 * L; m.KERG = t + 6 * L; m.cellh = t + 7 * L; m.MAT_A = t + 8 * L;
+    m.dZZ = d + 0 * L; m.dDZ = d + 1 * L; m.dDZW = d + 2 * L; m.dKERG = d + 6 * L; m.dcellh = d + 7 * L;
+    m.dMAT_A = d + 8 * L;
+    for (int i = 0; i < 6; i++) m.MAT_D[i] = h->hm.MAT_D[i];
+    m.KERG_norm2 = h->hm.KERG_norm2;
+    return m;
+}
+
+static ModeTabs mode_tabs(const tc_handle* h) {
+    ModeTabs t;
+    const int NXH = h->g.NXH, NY = h->g.NY;
+    t.cosx = h->tabs;
+    t.cosy = h->tabs + NXH;
+    t.sinx = h->tabs + NXH + NY;
+    t.siny = h->tabs + 2 * NXH + NY;
+    return t;
+}
+
+template <typename T>
+static const cplx<T>* twx(const tc_handle* h) { return (const cplx<T>*)h->tw; }
+template <typename T>
+static const cplx<T>* twy(const tc_handle* h) { return (const cplx<T>*)h->tw + h->g.NX; }
+
+static void free_all(tc_handle* h) {
+    void* ptrs[] = {h->nu_t, h->ptmp, h->spec, h->zscr, h->mesh_t, h->mesh_d, h->tabs, h->tw, h->red, h->ticket,
+                    h->err_flag, h->planes, h->stage, h->opv, h->opf, h->ops};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    for (int l = 0; l < 4; l++) {
+        if (h->vel[l]) cudaFree(h->vel[l]);
+        if (h->flux[l]) cudaFree(h->flux[l]);
+        if (h->pres[l]) cudaFree(h->pres[l]);
+    }
+    if (h->planes_h) cudaFreeHost(h->planes_h);
+    for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
+    h->ev.clear();
+    if (h->st) cudaStreamDestroy(h->st);
+}
+
+static bool is_23(int n) {
+    if (n < 2) return false;
+    while (n % 2 == 0) n /= 2;
+    while (n % 3 == 0) n /= 3;
+    return n == 1;
+}
+
+#define TC_ALLOC(ptr, bytes)                                                                        \
+    do {                                                                                            \
+        if (cudaMalloc((void**)&(ptr), (bytes)) != cudaSuccess) {                                   \
+            cudaGetLastError();                                                                     \
+            free_all(h);                                                                            \
+            delete h;                                                                               \
+            return fail(TC_E_NOMEM, "device allocation of " + std::to_string((size_t)(bytes)) + " bytes failed"); \
+        }                                                                                           \
+    } while (0)
+
+extern "C" int tc_create(const tc_params* prm, const double* zz, tc_handle** out) {
+    if (!prm || !zz || !out) return fail(TC_E_ARG, "tc_create: null argument");
+    *out = nullptr;
+    const tc_params& p = *prm;
+    if (p.scheme < 0 || p.scheme > 2) return fail(TC_E_ARG, "tc_create: unknown scheme");
+    if (p.precision != TC_FP64 && p.precision != TC_MIXED) return fail(TC_E_ARG, "tc_create: unknown precision");
+    if (!is_23(p.NX) || !is_23(p.NY) || (p.NX & 1) || (p.NY & 1))
+        return fail(TC_E_ARG, "tc_create: NX and NY must be even products of powers of 2 and 3");
+    if (p.NX < 8 || p.NY < 8) return fail(TC_E_ARG, "tc_create: NX, NY must be >= 8");
+    if (p.NZ < 6) return fail(TC_E_ARG, "tc_create: NZ must be >= 6");
+    if (p.scheme != TC_SCHEME_COLLOC && p.visc_type == TC_VISC_GALERKIN)
+        return fail(TC_E_ARG, "tc_create: Galerkin viscosity is collocated-only");
+    if (p.scheme == TC_SCHEME_COLLOC && p.visc_type == TC_VISC_NAIVE)
+        return fail(TC_E_ARG, "tc_create: NAIVE viscosity is staggered-only");
+    if (p.turb_model != TC_TURB_NONE && p.visc_type == TC_VISC_CROSS)
+        return fail(TC_E_ARG, "tc_create: a turbulence model needs NAIVE (staggered) or GALERKIN (collocated) viscosity");
+    if (!(p.hx > 0) || !(p.hy > 0) || !(p.visc > 0) || !(p.area > 0)) return fail(TC_E_ARG, "tc_create: bad mesh steps");
+    const int nzz = p.scheme == TC_SCHEME_COLLOC ? p.NZ : p.NZ + 1;
+    for (int i = 0; i + 1 < nzz; i++)
+        if (!(zz[i + 1] > zz[i])) return fail(TC_E_ARG, "tc_create: z coordinates must increase");
+    int ndev = 0;
+    TC_CUDA(cudaGetDeviceCount(&ndev));
+    if (p.device < 0 || p.device >= ndev) return fail(TC_E_ARG, "tc_create: device id out of range");
+    TC_CUDA(cudaSetDevice(p.device));
+
+    tc_handle* h = new tc_handle();
+    h->prm = p;
+    if (build_mesh(p, zz, h->hm)) {
+        delete h;
+        return fail(TC_E_NUMERIC, "tc_create: singular system for the VV4 gradient null vector");
+    }
+    Geom& g = h->g;
+    g.NX = p.NX; g.NY = p.NY; g.NZ = p.NZ; g.NXY = p.NX * p.NY;
+    g.N = (long long)g.NXY * p.NZ;
+    g.NXH = p.NX / 2 + 1;
+    g.scheme = p.scheme; g.visc_type = p.visc_type; g.turb = p.turb_model; g.stab_type = p.stab_type; g.fd_mode = p.fd_mode;
+    int lm = p.low_modes > 0 ? p.low_modes : 4;
+    lm = std::min(lm, std::min(g.NXH, (p.NY + 1) / 2));
+    g.low_modes = lm;
+    g.visc = p.visc; g.sour_dpdx = p.sour_dpdx; g.inv_ls = p.inv_length_scale; g.hx = p.hx; g.hy = p.hy;
+    g.inv_hx = 1. / p.hx; g.inv_hy = 1. / p.hy; g.area = p.area;
+    h->fp64 = p.precision == TC_FP64;
+    h->esz = h->fp64 ? 8 : 4;
+    h->turb_kind = p.turb_model;
+    if (plan_fft(p.NX, h->px) || plan_fft(p.NY, h->py)) {
+        delete h;
+        return fail(TC_E_ARG, "tc_create: FFT length not supported");
+    }
+    if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) {
+        delete h;
+        return fail(TC_E_CUDA, "tc_create: stream creation failed");
+    }
+    const size_t N = (size_t)g.N, E = h->esz;
+    for (int l = 0; l < 4; l++) {
+        TC_ALLOC(h->vel[l], 3 * N * E);
+        TC_ALLOC(h->flux[l], 3 * N * E);
+        TC_ALLOC(h->pres[l], N * E);
+    }
+    if (p.turb_model != TC_TURB_NONE) TC_ALLOC(h->nu_t, N * E);
+    TC_ALLOC(h->ptmp, N * E);
+    TC_ALLOC(h->spec, (size_t)g.NXH * g.NY * g.NZ * 2 * E);
+    TC_ALLOC(h->zscr, zsolve_scratch_bytes(g, (int)E));
+    // mesh arrays, 9 slots of NZ+2 (the last one holds MAT_A, up to 3 NZ entries)
+    const int L = g.NZ + 2;
+    const size_t mlen = (size_t)8 * L + 3 * (size_t)L;
+    TC_ALLOC(h->mesh_t, mlen * E);
+    TC_ALLOC(h->mesh_d, mlen * sizeof(double));
+    {
+        std::vector<double> md(mlen, 0.0);
+        const HostMesh& hm = h->hm;
+        auto put = [&](int slot, const std::vector<double>& v) {
+            for (size_t i = 0; i < v.size() && i < (size_t)(slot == 8 ? 3 * L : L); i++) md[(size_t)slot * L + i] = v[i];
+        };
+        put(0, hm.ZZ); put(1, hm.DZ); put(2, hm.DZW); put(3, hm.GC1); put(4, hm.GC2); put(5, hm.GCZ);
+        put(6, hm.KERG); put(7, hm.cellh); put(8, hm.MAT_A);
+        if (cudaMemcpy(h->mesh_d, md.data(), mlen * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) {
+            free_all(h); delete h;
+            return fail(TC_E_CUDA, "tc_create: mesh upload failed");
+        }
+        if (h->fp64) {
+            cudaMemcpy(h->mesh_t, md.data(), mlen * sizeof(double), cudaMemcpyHostToDevice);
+        } else {
+            std::vector<float> mf(mlen);
+            for (size_t i = 0; i < mlen; i++) mf[i] = (float)md[i];
+            cudaMemcpy(h->mesh_t, mf.data(), mlen * sizeof(float), cudaMemcpyHostToDevice);
+        }
+    }
+    // mode tables (staggered/func_global.h:208-211 cos tables; VV4 sin(pi k / N))
+    {
+        const double PI = 3.14159265358979323846;
+        std::vector<double> tb(2 * g.NXH + 2 * g.NY);
+        for (int i = 0; i < g.NXH; i++) tb[i] = std::cos(2. * PI * i / g.NX);
+        for (int i = 0; i < g.NY; i++) tb[g.NXH + i] = std::cos(2. * PI * i / g.NY);
+        for (int i = 0; i < g.NXH; i++) tb[g.NXH + g.NY + i] = std::sin(PI * i / g.NX);
+        for (int i = 0; i < g.NY; i++) tb[2 * g.NXH + g.NY + i] = std::sin(PI * i / g.NY);
+        TC_ALLOC(h->tabs, tb.size() * sizeof(double));
+        cudaMemcpy(h->tabs, tb.data(), tb.size() * sizeof(double), cudaMemcpyHostToDevice);
+    }
+    // twiddles exp(-2 pi i k / n) for n = NX then NY
+    {
+        const size_t nt = (size_t)g.NX + g.NY;
+        std::vector<double> tw(2 * nt);
+        auto fill = [&](int n, size_t off) {
+            for (int k = 0; k < n; k++) {
+                long double a = -2.0L * 3.14159265358979323846264338327950288L * (long double)k / (long double)n;
+                tw[2 * (off + k)] = (double)cosl(a);
+                tw[2 * (off + k) + 1] = (double)sinl(a);
+            }
+        };
+        fill(g.NX, 0);
+        fill(g.NY, g.NX);
+        TC_ALLOC(h->tw, 2 * nt * E);
+        if (h->fp64) cudaMemcpy(h->tw, tw.data(), 2 * nt * 8, cudaMemcpyHostToDevice);
+        else {
+            std::vector<float> tf(2 * nt);
+            for (size_t i = 0; i < 2 * nt; i++) tf[i] = (float)tw[i];
+            cudaMemcpy(h->tw, tf.data(), 2 * nt * 4, cudaMemcpyHostToDevice);
+        }
+    }
+    h->nblocks_flux = flux_grid_blocks(g);
+    TC_ALLOC(h->red, (size_t)(2 + h->nblocks_flux) * sizeof(double));
+    TC_ALLOC(h->ticket, sizeof(unsigned));
+    TC_ALLOC(h->err_flag, sizeof(int));
+    TC_ALLOC(h->planes, (size_t)g.NZ * TC_DIAG_STRIDE * sizeof(double));
+    if (cudaMallocHost((void**)&h->planes_h, (size_t)g.NZ * TC_DIAG_STRIDE * sizeof(double)) != cudaSuccess) {
+        free_all(h); delete h;
+        return fail(TC_E_NOMEM, "tc_create: pinned host allocation failed");
+    }
+    cudaMemsetAsync(h->ticket, 0, sizeof(unsigned), h->st);
+    cudaMemsetAsync(h->err_flag, 0, sizeof(int), h->st);
+    cudaMemsetAsync(h->red, 0, (size_t)(2 + h->nblocks_flux) * sizeof(double), h->st);
+    for (int l = 0; l < 4; l++) {
+        cudaMemsetAsync(h->vel[l], 0, 3 * N * E, h->st);
+        cudaMemsetAsync(h->flux[l], 0, 3 * N * E, h->st);
+        cudaMemsetAsync(h->pres[l], 0, N * E, h->st);
+    }
+    if (h->nu_t) cudaMemsetAsync(h->nu_t, 0, N * E, h->st);
+    cudaError_t e = cudaStreamSynchronize(h->st);
+    if (e != cudaSuccess) {
+        free_all(h); delete h;
+        return fail(TC_E_CUDA, std::string("tc_create: ") + cudaGetErrorString(e));
+    }
+    *out = h;
+    return TC_OK;
+}
+
+extern "C" int tc_destroy(tc_handle* h) {
+    if (!h) return TC_OK;
+    cudaSetDevice(h->prm.device);
+    cudaStreamSynchronize(h->st);
+    free_all(h);
+    delete h;
+    return TC_OK;
+}
+
+static int check_launch(const char* what) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(TC_E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    return TC_OK;
+}
+
+static int ensure_stage(tc_handle* h) {
+    if (!h->stage && cudaMalloc((void**)&h->stage, 3 * (size_t)h->g.N * sizeof(double)) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(TC_E_NOMEM, "staging allocation failed");
+    }
+    return TC_OK;
+}
+static int ensure_ops(tc_handle* h) {
+    const size_t N = (size_t)h->g.N, E = h->esz;
+    if (!h->opv && cudaMalloc(&h->opv, 3 * N * E) != cudaSuccess) return fail(TC_E_NOMEM, "operator scratch");
+    if (!h->opf && cudaMalloc(&h->opf, 3 * N * E) != cudaSuccess) return fail(TC_E_NOMEM, "operator scratch");
+    if (!h->ops && cudaMalloc(&h->ops, N * E) != cudaSuccess) return fail(TC_E_NOMEM, "operator scratch");
+    return TC_OK;
+}
+
+// ---- host <-> device transfers of AoS double data ----
+template <typename T>
+static int up_vec(tc_handle* h, const double* src, void* dst) {
+    int rc = ensure_stage(h);
+    if (rc) return rc;
+    const long long N = h->g.N;
+    TC_CUDA(cudaMemcpyAsync(h->stage, src, 3 * (size_t)N * sizeof(double), cudaMemcpyHostToDevice, h->st));
+    launch_aos_to_soa<T>(h->stage, vec<T>(dst, N), N, h->st);
+    return check_launch("aos_to_soa");
+}
+template <typename T>
+static int up_scal(tc_handle* h, const double* src, void* dst) {
+    int rc = ensure_stage(h);
+    if (rc) return rc;
+    const long long N = h->g.N;
+    TC_CUDA(cudaMemcpyAsync(h->stage, src, (size_t)N * sizeof(double), cudaMemcpyHostToDevice, h->st));
+    launch_d2t<T>(h->stage, (T*)dst, N, h->st);
+    return check_launch("d2t");
+}
+template <typename T>
+static int down_vec(tc_handle* h, const void* src, double* dst) {
+    int rc = ensure_stage(h);
+    if (rc) return rc;
+    const long long N = h->g.N;
+    launch_soa_to_aos<T>(cvec<T>((void*)src, N), h->stage, N, h->st);
+    TC_CUDA(cudaMemcpyAsync(dst, h->stage, 3 * (size_t)N * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    TC_CUDA(cudaStreamSynchronize(h->st));
+    return TC_OK;
+}
+template <typename T>
+static int down_scal(tc_handle* h, const void* src, double* dst) {
+    int rc = ensure_stage(h);
+    if (rc) return rc;
+    const long long N = h->g.N;
+    launch_t2d<T>((const T*)src, h->stage, N, h->st);
+    TC_CUDA(cudaMemcpyAsync(dst, h->stage, (size_t)N * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    TC_CUDA(cudaStreamSynchronize(h->st));
+    return TC_OK;
+}
+
+#define TC_DISPATCH(h, fn, ...) ((h)->fp64 ? fn<double>(__VA_ARGS__) : fn<float>(__VA_ARGS__))
+
+extern "C" int tc_upload_level(tc_handle* h, int level, const double* vel, const double* p) {
+    if (!h || level < 0 || level > 3) return fail(TC_E_ARG, "tc_upload_level: bad handle or level");
+    cudaSetDevice(h->prm.device);
+    int rc = TC_OK;
+    if (vel) rc = TC_DISPATCH(h, up_vec, h, vel, h->vel[level]);
+    if (!rc && p) rc = TC_DISPATCH(h, up_scal, h, p, h->pres[level]);
+    if (!rc) TC_CUDA(cudaStreamSynchronize(h->st));
+    return rc;
+}
+extern "C" int tc_download_level(tc_handle* h, int level, double* vel, double* p) {
+    if (!h || level < 0 || level > 3) return fail(TC_E_ARG, "tc_download_level: bad handle or level");
+    cudaSetDevice(h->prm.device);
+    int rc = TC_OK;
+    if (vel) rc = TC_DISPATCH(h, down_vec, h, h->vel[level], vel);
+    if (!rc && p) rc = TC_DISPATCH(h, down_scal, h, h->pres[level], p);
+    return rc;
+}
+extern "C" int tc_download_flux(tc_handle* h, int level, double* f) {
+    if (!h || level < 0 || level > 3 || !f) return fail(TC_E_ARG, "tc_download_flux: bad argument");
+    cudaSetDevice(h->prm.device);
+    return TC_DISPATCH(h, down_vec, h, h->flux[level], f);
+}
+extern "C" int tc_device_level(tc_handle* h, int level, void** vel, void** p) {
+    if (!h || level < 0 || level > 3) return fail(TC_E_ARG, "tc_device_level: bad handle or level");
+    if (vel) *vel = h->vel[level];
+    if (p) *p = h->pres[level];
+    return TC_OK;
+}
+extern "C" int tc_get_stream(tc_handle* h, void** s) {
+    if (!h || !s) return fail(TC_E_ARG, "tc_get_stream: null argument");
+    *s = (void*)h->st;
+    return TC_OK;
+}
+extern "C" int tc_sync(tc_handle* h) {
+    if (!h) return fail(TC_E_ARG, "tc_sync: null handle");
+    cudaSetDevice(h->prm.device);
+    TC_CUDA(cudaStreamSynchronize(h->st));
+    int flag = 0;
+    TC_CUDA(cudaMemcpy(&flag, h->err_flag, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag) {
+        cudaMemset(h->err_flag, 0, sizeof(int));
+        return fail(TC_E_NUMERIC, "banded pressure solve met a vanishing pivot");
+    }
+    return TC_OK;
+}
+extern "C" int tc_set_nu_t(tc_handle* h, const double* nt) {
+    if (!h || !nt) return fail(TC_E_ARG, "tc_set_nu_t: null argument");
+    if (!h->nu_t) return fail(TC_E_STATE, "tc_set_nu_t: no turbulence model configured");
+    cudaSetDevice(h->prm.device);
+    int rc = TC_DISPATCH(h, up_scal, h, nt, h->nu_t);
+    if (!rc) TC_CUDA(cudaStreamSynchronize(h->st));
+    return rc;
+}
+extern "C" int tc_get_nu_t(tc_handle* h, double* nt) {
+    if (!h || !nt) return fail(TC_E_ARG, "tc_get_nu_t: null argument");
+    if (!h->nu_t) {
+        memset(nt, 0, sizeof(double) * (size_t)h->g.N);
+        return TC_OK;
+    }
+    cudaSetDevice(h->prm.device);
+    return TC_DISPATCH(h, down_scal, h, h->nu_t, nt);
+}
+
+// ---------------------------------------------------------------------------
+// Pressure solve pipeline: RHS (vector, divergence taken) or scalar -> p
+// ---------------------------------------------------------------------------
+template <typename T>
+static void poisson(tc_handle* h, const void* rhs_vec, const void* rhs_scalar, void* p_out, size_t eb = (size_t)-1) {
+    const bool mk = eb != (size_t)-1;
+    const Geom& g = h->g;
+    DivFftArgs<T> da;
+    da.g = g;
+    da.m = mesh_dev<T>(h);
+    da.v = rhs_vec ? cvec<T>((void*)rhs_vec, g.N) : CV3<T>{{nullptr, nullptr, nullptr}};
+    da.src_scalar = (const T*)rhs_scalar;
+    da.spec = (cplx<T>*)h->spec;
+    da.px = h->px;
+    da.twx = twx<T>(h);
+    launch_div_xfft<T>(da, h->st);
+    if (mk) mark(h, 3, eb);
+    YFftArgs<T> ya{g, (cplx<T>*)h->spec, h->py, twy<T>(h), -1};
+    launch_yfft<T>(ya, h->st);
+    if (mk) mark(h, 4, eb);
+    ZSolveArgs<T> za{g, mesh_dev<T>(h), mode_tabs(h), (cplx<T>*)h->spec, h->zscr, h->err_flag};
+    launch_zsolve<T>(za, h->st);
+    if (mk) mark(h, 5, eb);
+    ya.sign = +1;
+    launch_yfft<T>(ya, h->st);
+    if (mk) mark(h, 6, eb);
+    IxFftArgs<T> ia{g, (const cplx<T>*)h->spec, (T*)p_out, h->px, twx<T>(h), (T)(1.0 / ((double)g.NX * g.NY))};
+    launch_ixfft<T>(ia, h->st);
+    if (mk) mark(h, 7, eb);
+    h->launches += 5 + (sizeof(T) == 4 ? 1 : 0);
+}
+
+template <typename T>
+static void turb_visc(tc_handle* h, const void* v) {
+    TurbArgs<T> ta{h->g, mesh_dev<T>(h), cvec<T>((void*)v, h->g.N), (T*)h->nu_t};
+    launch_turb<T>(ta, h->st);
+}
+
+template <typename T>
+static int step_impl(tc_handle* h, double tau, int cur, int order) {
+    const Geom& g = h->g;
+    const long long N = g.N;
+    const int nxt = (cur + 1) % 4, prv = (cur + 3) % 4, pr2 = (cur + 2) % 4;
+    const T inv_tau = (T)(1. / tau);
+    const T bd0 = order == 3 ? (T)(1.5 + 0.33333333333333333333) : order == 2 ? (T)1.5 : (T)1.0;
+    const T tob = (T)(tau / bd0);
+    const bool coll = g.scheme == TC_SCHEME_COLLOC;
+    const bool stab1 = coll && g.stab_type == 1;
+    const bool les = h->nu_t && h->turb_kind == TC_TURB_SMAGORINSKY;
+    const size_t eb = h->ev_used;
+    mark(h, 0, eb);
+    if (les) {
+        turb_visc<T>(h, h->vel[cur]);
+        h->launches += 1;
+    }
+    mark(h, 1, eb);
+    FluxArgs<T> fa;
+    fa.g = g;
+    fa.m = mesh_dev<T>(h);
+    fa.vel = cvec<T>(h->vel[cur], N);
+    fa.velp = cvec<T>(h->vel[prv], N);
+    fa.velq = cvec<T>(h->vel[pr2], N);
+    fa.fp = cvec<T>(h->flux[prv], N);
+    fa.fq = cvec<T>(h->flux[pr2], N);
+    fa.fout = vec<T>(h->flux[cur], N);
+    fa.rhs = vec<T>(h->flux[nxt], N);
+    fa.nu_t = (h->nu_t && h->turb_kind != TC_TURB_NONE) ? (const T*)h->nu_t : nullptr;
+    fa.pcur = stab1 ? (const T*)h->pres[cur] : nullptr;
+    fa.inv_tau = inv_tau;
+    fa.order = order;
+    const bool cfr = h->forcing_mode == 1;
+    fa.ub_partial = h->red + 2;
+    fa.ticket = h->ticket;
+    fa.ub_out = cfr ? h->red : nullptr;
+    if (coll) launch_flux_coll<T>(fa, h->st);
+    else launch_flux_stag<T>(fa, h->st);
+    h->launches += 1;
+    mark(h, 2, eb);
+    void* pdest = stab1 ? h->ptmp : h->pres[nxt];
+    poisson<T>(h, h->flux[nxt], nullptr, pdest, eb);
+    CorrArgs<T> ca;
+    ca.g = g;
+    ca.m = mesh_dev<T>(h);
+    ca.rhs = cvec<T>(h->flux[nxt], N);
+    ca.p = (const T*)pdest;
+    ca.vout = vec<T>(h->vel[nxt], N);
+    ca.pcur = stab1 ? (const T*)h->pres[cur] : nullptr;
+    ca.pnext = stab1 ? (T*)h->pres[nxt] : nullptr;
+    ca.tob = tob;
+    ca.cfr = cfr ? 1 : 0;
+    ca.cfr_target = h->forcing_value;
+    ca.cfr_scale = g.hx * g.hy / g.area;
+    double vf = g.area;
+    if (coll) {
+        double s = 0;
+        for (int iz = 1; iz < g.NZ - 1; iz++) s += h->hm.cellh[iz];
+        vf = s * g.hx * g.hy * g.NXY;
+    }
+    ca.cfr_volfac = g.area / vf;
+    ca.ub_sum = h->red;
+    ca.du_out = h->red + 1;
+    ca.grad_only = 0;
+    launch_correct<T>(ca, h->st);
+    h->launches += 1;
+    mark(h, 8, eb);
+    if (h->timing) {
+        h->ev_used += 9;
+        h->timed_steps += 1;
+    }
+    h->last_tau = tau;
+    h->last_bd0 = (double)bd0;
+    return check_launch("tc_step");
+}
+
+extern "C" int tc_step(tc_handle* h, double t, double tau, int current_field, int bdf_order) {
+    (void)t;
+    if (!h) return fail(TC_E_ARG, "tc_step: null handle");
+    if (bdf_order < 1 || bdf_order > 3) return fail(TC_E_ARG, "tc_step: wrong bdf_order");
+    if (current_field < 0 || current_field > 3) return fail(TC_E_ARG, "tc_step: current_field out of range");
+    if (!(tau > 0) || !std::isfinite(tau)) return fail(TC_E_ARG, "tc_step: tau must be positive");
+    cudaSetDevice(h->prm.device);
+    return TC_DISPATCH(h, step_impl, h, tau, current_field, bdf_order);
+}
+
+extern "C" int tc_phase_timing(tc_handle* h, int enable) {
+    if (!h) return fail(TC_E_ARG, "tc_phase_timing: null handle");
+    h->timing = enable != 0;
+    return TC_OK;
+}
+
+extern "C" int tc_phase_times(tc_handle* h, double ms[TC_NPHASE], int* nsteps) {
+    if (!h || !ms) return fail(TC_E_ARG, "tc_phase_times: null argument");
+    cudaSetDevice(h->prm.device);
+    TC_CUDA(cudaStreamSynchronize(h->st));
+    double acc[TC_NPHASE] = {};
+    for (int s = 0; s < h->timed_steps; s++)
+        for (int k = 0; k < TC_NPHASE; k++) {
+            float t = 0;
+            TC_CUDA(cudaEventElapsedTime(&t, h->ev[(size_t)s * 9 + k], h->ev[(size_t)s * 9 + k + 1]));
+            acc[k] += t;
+        }
+    for (int k = 0; k < TC_NPHASE; k++) ms[k] = acc[k];
+    if (nsteps) *nsteps = h->timed_steps;
+    h->timed_steps = 0;
+    h->ev_used = 0;
+    return TC_OK;
+}
+
+extern "C" int tc_launch_count(tc_handle* h, unsigned long long* n) {
+    if (!h || !n) return fail(TC_E_ARG, "tc_launch_count: null argument");
+    *n = h->launches;
+    return TC_OK;
+}
+
+extern "C" int tc_set_forcing(tc_handle* h, int mode, double value) {
+    if (!h || (mode != 0 && mode != 1)) return fail(TC_E_ARG, "tc_set_forcing: bad argument");
+    h->forcing_mode = mode;
+    if (mode == 0) {
+        h->prm.sour_dpdx = value;
+        h->g.sour_dpdx = value;
+    } else {
+        h->forcing_value = value;
+    }
+    return TC_OK;
+}
+
+extern "C" int tc_last_dpdx(tc_handle* h, double* dpdx) {
+    if (!h || !dpdx) return fail(TC_E_ARG, "tc_last_dpdx: null argument");
+    cudaSetDevice(h->prm.device);
+    TC_CUDA(cudaStreamSynchronize(h->st));
+    double du = 0;
+    if (h->forcing_mode == 1) TC_CUDA(cudaMemcpy(&du, h->red + 1, sizeof(double), cudaMemcpyDeviceToHost));
+    *dpdx = h->g.sour_dpdx + (h->last_tau > 0 ? du * h->last_bd0 / h->last_tau : 0.0);
+    return TC_OK;
+}
+
+extern "C" int tc_set_turb_model(tc_handle* h, int kind, const void* weights) {
+    (void)weights;
+    if (!h) return fail(TC_E_ARG, "tc_set_turb_model: null handle");
+    if (kind == TC_TURB_NONE) {
+        h->turb_kind = kind;
+        return TC_OK;
+    }
+    if (kind != TC_TURB_SMAGORINSKY) return fail(TC_E_ARG, "tc_set_turb_model: unknown model");
+    if (h->g.visc_type == TC_VISC_CROSS) return fail(TC_E_ARG, "tc_set_turb_model: CROSS viscosity has no nu_t");
+    cudaSetDevice(h->prm.device);
+    if (!h->nu_t) {
+        if (cudaMalloc(&h->nu_t, (size_t)h->g.N * h->esz) != cudaSuccess) return fail(TC_E_NOMEM, "nu_t allocation");
+        cudaMemsetAsync(h->nu_t, 0, (size_t)h->g.N * h->esz, h->st);
+    }
+    h->turb_kind = kind;
+    h->g.turb = kind;
+    return TC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Diagnostics
+// ---------------------------------------------------------------------------
+template <typename T>
+static int diag_run(tc_handle* h, int level, double tau) {
+    DiagArgs<T> a;
+    a.g = h->g;
+    a.m = mesh_dev<T>(h);
+    a.v = cvec<T>(h->vel[level], h->g.N);
+    a.p = (const T*)h->pres[level];
+    a.nu_t = (h->nu_t && h->turb_kind != TC_TURB_NONE) ? (const T*)h->nu_t : nullptr;
+    a.tau = tau;
+    a.planes = h->planes;
+    launch_diag<T>(a, h->st);
+    TC_CUDA(cudaGetLastError());
+    TC_CUDA(cudaMemcpyAsync(h->planes_h, h->planes, (size_t)h->g.NZ * TC_DIAG_STRIDE * sizeof(double),
+                            cudaMemcpyDeviceToHost, h->st));
+    TC_CUDA(cudaStreamSynchronize(h->st));
+    return TC_OK;
+}
+
+static void reduce_planes(const tc_handle* h, double integral[3], double* ke, double cfl[3], double* prof) {
+    const Geom& g = h->g;
+    const bool coll = g.scheme == TC_SCHEME_COLLOC;
+    double I0 = 0, I1 = 0, I2 = 0, K = 0, c1 = 0, c2 = 0, c3 = 0;
+    for (int z = 0; z < g.NZ; z++) {
+        const double* s = h->planes_h + (size_t)z * TC_DIAG_STRIDE;
+        const double wu = coll ? h->hm.cellh[z] : h->hm.DZ[z];
+        const double ww = coll ? h->hm.cellh[z] : (z == 0 ? 0.0 : 0.5 * (h->hm.DZ[z] + h->hm.DZ[z - 1]));
+        I0 += s[0] * wu;
+        I1 += s[1] * wu;
+        I2 += s[12] * ww;
+        K += (s[3] + s[4]) * wu + s[13] * ww;
+        c1 = std::max(c1, s[16]);
+        c2 = std::max(c2, s[17]);
+        c3 = std::max(c3, s[18]);
+        if (prof)
+            for (int k = 0; k < 12; k++) prof[z * 12 + k] = s[k] / g.NXY;
+    }
+    const double hxy = g.hx * g.hy;
+    if (integral) {
+        integral[0] = I0 * hxy;
+        integral[1] = I1 * hxy;
+        integral[2] = I2 * hxy;
+    }
+    if (ke) *ke = 0.5 * K * hxy;
+    if (cfl) {
+        cfl[0] = c1;
+        cfl[1] = c2;
+        cfl[2] = c3;
+    }
+}
+
+extern "C" int tc_diagnostics(tc_handle* h, int level, double tau, double integral[3], double* cfl, double* profiles) {
+    if (!h || level < 0 || level > 3) return fail(TC_E_ARG, "tc_diagnostics: bad handle or level");
+    cudaSetDevice(h->prm.device);
+    int rc = TC_DISPATCH(h, diag_run, h, level, tau);
+    if (rc) return rc;
+    double c[3];
+    reduce_planes(h, integral, nullptr, c, profiles);
+    if (cfl) *cfl = c[2];
+    return TC_OK;
+}
+extern "C" int tc_integral(tc_handle* h, int level, double out[3]) {
+    return tc_diagnostics(h, level, 0.0, out, nullptr, nullptr);
+}
+extern "C" int tc_kinetic_energy(tc_handle* h, int level, double* out) {
+    if (!h || !out || level < 0 || level > 3) return fail(TC_E_ARG, "tc_kinetic_energy: bad argument");
+    cudaSetDevice(h->prm.device);
+    int rc = TC_DISPATCH(h, diag_run, h, level, 0.0);
+    if (rc) return rc;
+    reduce_planes(h, nullptr, out, nullptr, nullptr);
+    return TC_OK;
+}
+extern "C" int tc_cfl(tc_handle* h, int level, double tau, int mode, double* out) {
+    if (!h || !out || level < 0 || level > 3 || mode < 1 || mode > 3) return fail(TC_E_ARG, "tc_cfl: bad argument");
+    cudaSetDevice(h->prm.device);
+    int rc = TC_DISPATCH(h, diag_run, h, level, tau);
+    if (rc) return rc;
+    double c[3];
+    reduce_planes(h, nullptr, nullptr, c, nullptr);
+    *out = c[mode - 1];
+    return TC_OK;
+}
+extern "C" int tc_profiles(tc_handle* h, int level, double* out) {
+    if (!out) return fail(TC_E_ARG, "tc_profiles: null output");
+    return tc_diagnostics(h, level, 0.0, nullptr, nullptr, out);
+}
+
+// ---------------------------------------------------------------------------
+// Operator-level entry points
+// ---------------------------------------------------------------------------
+template <typename T>
+static int op_explicit(tc_handle* h, const double* v, double* f) {
+    int rc = ensure_ops(h);
+    if (!rc) rc = up_vec<T>(h, v, h->opv);
+    if (rc) return rc;
+    FluxArgs<T> fa{};
+    fa.g = h->g;
+    fa.m = mesh_dev<T>(h);
+    fa.vel = cvec<T>(h->opv, h->g.N);
+    fa.fout = vec<T>(h->opf, h->g.N);
+    fa.nu_t = (h->nu_t && h->turb_kind != TC_TURB_NONE) ? (const T*)h->nu_t : nullptr;
+    fa.order = 0;
+    if (h->g.scheme == TC_SCHEME_COLLOC) launch_flux_coll<T>(fa, h->st);
+    else launch_flux_stag<T>(fa, h->st);
+    rc = check_launch("explicit_term");
+    return rc ? rc : down_vec<T>(h, h->opf, f);
+}
+template <typename T>
+static int op_grad(tc_handle* h, const double* p, double* g) {
+    int rc = ensure_ops(h);
+    if (!rc) rc = up_scal<T>(h, p, h->ops);
+    if (rc) return rc;
+    CorrArgs<T> ca{};
+    ca.g = h->g;
+    ca.m = mesh_dev<T>(h);
+    ca.p = (const T*)h->ops;
+    ca.vout = vec<T>(h->opv, h->g.N);
+    ca.grad_only = 1;
+    launch_correct<T>(ca, h->st);
+    rc = check_launch("apply_gradient");
+    return rc ? rc : down_vec<T>(h, h->opv, g);
+}
+template <typename T>
+static int op_div(tc_handle* h, const double* v, double* dv) {
+    int rc = ensure_ops(h);
+    if (!rc) rc = up_vec<T>(h, v, h->opv);
+    if (rc) return rc;
+    DivArgs<T> a{h->g, mesh_dev<T>(h), cvec<T>(h->opv, h->g.N), (T*)h->ops};
+    launch_divergence<T>(a, h->st);
+    rc = check_launch("apply_divergence");
+    return rc ? rc : down_scal<T>(h, h->ops, dv);
+}
+template <typename T>
+static int op_unapply(tc_handle* h, const double* v, double* p) {
+    int rc = ensure_ops(h);
+    if (!rc) rc = up_vec<T>(h, v, h->opv);
+    if (rc) return rc;
+    poisson<T>(h, h->opv, nullptr, h->ops);
+    rc = check_launch("unapply_gradient");
+    return rc ? rc : down_scal<T>(h, h->ops, p);
+}
+template <typename T>
+static int op_psolve(tc_handle* h, const double* rhs, double* p) {
+    int rc = ensure_ops(h);
+    if (!rc) rc = up_scal<T>(h, rhs, h->ops);
+    if (rc) return rc;
+    poisson<T>(h, nullptr, h->ops, h->ops);
+    rc = check_launch("pressure_solve");
+    return rc ? rc : down_scal<T>(h, h->ops, p);
+}
+template <typename T>
+static int op_turb(tc_handle* h, const double* v, double* nt) {
+    int rc = ensure_ops(h);
+    if (!rc) rc = up_vec<T>(h, v, h->opv);
+    if (rc) return rc;
+    turb_visc<T>(h, h->opv);
+    rc = check_launch("turb_visc");
+    return rc ? rc : down_scal<T>(h, h->nu_t, nt);
+}
+
+#define TC_OPCHK(h, a, b)                                                  \
+    if (!(h) || !(a) || !(b)) return fail(TC_E_ARG, "null argument");     \
+    cudaSetDevice((h)->prm.device);
+
+extern "C" int tc_op_explicit_term(tc_handle* h, const double* v, double* f) {
+    TC_OPCHK(h, v, f);
+    return TC_DISPATCH(h, op_explicit, h, v, f);
+}
+extern "C" int tc_op_apply_gradient(tc_handle* h, const double* p, double* g) {
+    TC_OPCHK(h, p, g);
+    return TC_DISPATCH(h, op_grad, h, p, g);
+}
+extern "C" int tc_op_apply_divergence(tc_handle* h, const double* v, double* dv) {
+    TC_OPCHK(h, v, dv);
+    return TC_DISPATCH(h, op_div, h, v, dv);
+}
+extern "C" int tc_op_unapply_gradient(tc_handle* h, const double* v, double* p) {
+    TC_OPCHK(h, v, p);
+    return TC_DISPATCH(h, op_unapply, h, v, p);
+}
+extern "C" int tc_op_pressure_solve(tc_handle* h, const double* rhs, double* p) {
+    TC_OPCHK(h, rhs, p);
+    return TC_DISPATCH(h, op_psolve, h, rhs, p);
+}
+extern "C" int tc_op_turb_visc(tc_handle* h, const double* v, double* nt) {
+    TC_OPCHK(h, v, nt);
+    if (!h->nu_t) return fail(TC_E_STATE, "tc_op_turb_visc: no turbulence model configured");
+    return TC_DISPATCH(h, op_turb, h, v, nt);
+}
+
+// ---------------------------------------------------------------------------
+// Seeded initial field
+// ---------------------------------------------------------------------------
+extern "C" void tc_mesh_tanh(int n, double gamma, double H, double* z) {
+    for (int j = 0; j <= n; j++) z[j] = H * (1. + std::tanh(gamma * (2. * j / n - 1.)) / std::tanh(gamma));
+}
+
+template <typename T>
+static int project_level(tc_handle* h, int level) {
+    int rc = ensure_ops(h);
+    if (rc) return rc;
+    poisson<T>(h, h->vel[level], nullptr, h->ops);
+    CorrArgs<T> ca{};
+    ca.g = h->g;
+    ca.m = mesh_dev<T>(h);
+    ca.rhs = cvec<T>(h->vel[level], h->g.N);
+    ca.p = (const T*)h->ops;
+    ca.vout = vec<T>(h->vel[level], h->g.N);
+    ca.tob = (T)1;
+    launch_correct<T>(ca, h->st);
+    return check_launch("projection");
+}
+
+extern "C" int tc_init_channel(tc_handle* h, int level, unsigned long long seed, double amp, int project) {
+    if (!h || level < 0 || level > 3) return fail(TC_E_ARG, "tc_init_channel: bad handle or level");
+    cudaSetDevice(h->prm.device);
+    const Geom& g = h->g;
+    const size_t N = (size_t)g.N;
+    std::vector<double> v(3 * N), p(N, 0.0);
+    std::mt19937_64 gen(seed);
+    const bool coll = g.scheme == TC_SCHEME_COLLOC;
+    const std::vector<double>& ZZ = h->hm.ZZ;
+    const double H = coll ? 0.5 * (ZZ[g.NZ - 1] - ZZ[0]) : 0.5 * (ZZ[g.NZ] - ZZ[0]);
+    for (size_t in = 0; in < N; in++) {
+        const int iz = (int)(in / g.NXY);
+        double r[3];
+        for (int c = 0; c < 3; c++) r[c] = amp * (2. * (double)(gen() >> 11) * (1.0 / 9007199254740992.0) - 1.);
+        const double zc = coll ? ZZ[iz] : 0.5 * (ZZ[iz] + ZZ[iz + 1]);
+        const double y = (zc - ZZ[0]) / H - 1.;
+        v[3 * in] = 1.5 * (1. - y * y) + r[0];
+        v[3 * in + 1] = r[1];
+        v[3 * in + 2] = r[2];
+        if (coll) {
+            if (iz == 0 || iz == g.NZ - 1) v[3 * in] = v[3 * in + 1] = v[3 * in + 2] = 0;
+        } else if (iz == 0) {
+            v[3 * in + 2] = 0;
+        }
+    }
+    int rc = tc_upload_level(h, level, v.data(), p.data());
+    if (rc) return rc;
+    if (project) {
+        rc = TC_DISPATCH(h, project_level, h, level);
+        if (rc) return rc;
+        TC_CUDA(cudaStreamSynchronize(h->st));
+    }
+    return TC_OK;
+}

@@ -1,0 +1,209 @@
+// tc_common.cuh -- types and device building blocks shared by the sm_100a kernels
+// of turbchannel_b200 and by the host orchestration.  Internal, not part of the ABI.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/turbch.h"
+
+namespace tc {
+
+// ---------------------------------------------------------------------------
+// Plain data passed to kernels by value
+// ---------------------------------------------------------------------------
+struct Geom {
+    int NX, NY, NZ, NXY;
+    long long N;  // cells (or nodes)
+    int NXH;      // NX/2 + 1 : kx range of the half spectrum
+    int scheme, visc_type, turb, stab_type, fd_mode, low_modes;
+    double visc, sour_dpdx, inv_ls, hx, hy, inv_hx, inv_hy, area;
+};
+
+// Mesh-derived arrays (device pointers into one allocation).  Staggered arrays
+// follow struct main_params (staggered/config.h:58-72) in the working type T;
+// collocated ones follow collocated_AB3/data_global.h:113-116 (double).  The
+// double copies serve the double-precision banded solves of the mixed mode.
+template <typename T>
+struct MeshDev {
+    const T *ZZ, *DZ, *DZW, *GC1, *GC2, *GCZ, *KERG, *MAT_A, *cellh;
+    const double *dZZ, *dDZ, *dDZW, *dKERG, *dMAT_A, *dcellh;
+    double MAT_D[6];
+    double KERG_norm2;
+};
+
+struct ModeTabs {
+    const double* cosx;  // cos(2 pi kx / NX),  kx = 0..NX/2
+    const double* cosy;  // cos(2 pi ky / NY),  ky = 0..NY-1
+    const double* sinx;  // sin(pi kx / NX)
+    const double* siny;  // sin(pi ky / NY)
+};
+
+constexpr int FFT_MAXF = 24;
+struct FftPlan {
+    int n, nf;
+    int fac[FFT_MAXF];
+};
+
+template <typename T>
+struct cplx {
+    T x, y;
+};
+
+template <typename T>
+__host__ __device__ __forceinline__ cplx<T> cmul(cplx<T> a, cplx<T> b) {
+    return {a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
+}
+
+// ---------------------------------------------------------------------------
+// Async global->shared copies (LDGSTS).  Sizes 4, 8 or 16 bytes.
+// ---------------------------------------------------------------------------
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
+    unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(sa), "l"(gmem), "n"(BYTES));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Block-wide sum; result valid in thread 0.  sbuf: >= 32 doubles of shared memory.
+__device__ __forceinline__ double block_sum(double v, double* sbuf) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    v = warp_sum(v);
+    __syncthreads();
+    if (lane == 0) sbuf[wid] = v;
+    __syncthreads();
+    double r = 0;
+    if (wid == 0) {
+        r = lane < nw ? sbuf[lane] : 0.0;
+        r = warp_sum(r);
+    }
+    return r;
+}
+
+// Deterministic grid reduction: every block stores its partial, the last block to
+// arrive sums all partials in index order and stores the total (then re-arms the
+// ticket for the next launch).  Thread 0 of each block passes its partial.
+__device__ __forceinline__ void grid_sum_finish(double partial, double* partials, unsigned* ticket, double* out,
+                                                double* sbuf) {
+    const unsigned nb = gridDim.x * gridDim.y * gridDim.z;
+    const unsigned bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    __shared__ unsigned s_last;
+    if (threadIdx.x == 0) {
+        partials[bid] = partial;
+        __threadfence();
+        unsigned t = atomicAdd(ticket, 1u);
+        s_last = (t == nb - 1);
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    double s = 0;
+    for (unsigned i = threadIdx.x; i < nb; i += blockDim.x) s += ((volatile double*)partials)[i];
+    s = block_sum(s, sbuf);
+    if (threadIdx.x == 0) {
+        *out = s;
+        *ticket = 0u;
+    }
+}
+
+__device__ __forceinline__ int wrapi(int i, int n) {
+    while (i < 0) i += n;
+    while (i >= n) i -= n;
+    return i;
+}
+
+// ---------------------------------------------------------------------------
+// Shared-memory Stockham FFT (radix 4, 2, 3), textbook Cooley-Tukey.
+// nl lines of length P.n at stride ls (complex elements) in shared memory;
+// tw[k] = exp(-2 pi i k / n), k < n.  sign -1 forward, +1 inverse (unnormalised).
+// All threads of the block take part; the result buffer is returned.
+// ---------------------------------------------------------------------------
+template <typename T, int R>
+__device__ __forceinline__ void dft_small(cplx<T>* v, int sign) {
+    if (R == 2) {
+        cplx<T> a = v[0];
+        v[0] = {a.x + v[1].x, a.y + v[1].y};
+        v[1] = {a.x - v[1].x, a.y - v[1].y};
+    } else if (R == 4) {
+        cplx<T> t0 = {v[0].x + v[2].x, v[0].y + v[2].y};
+        cplx<T> t1 = {v[0].x - v[2].x, v[0].y - v[2].y};
+        cplx<T> t2 = {v[1].x + v[3].x, v[1].y + v[3].y};
+        T dr = v[1].x - v[3].x, di = v[1].y - v[3].y;
+        cplx<T> t3 = {-sign * di, sign * dr};  // (v1 - v3) * (sign i)
+        v[0] = {t0.x + t2.x, t0.y + t2.y};
+        v[2] = {t0.x - t2.x, t0.y - t2.y};
+        v[1] = {t1.x + t3.x, t1.y + t3.y};
+        v[3] = {t1.x - t3.x, t1.y - t3.y};
+    } else {  // R == 3
+        const T s3 = (T)0.86602540378443864676372317075294;
+        cplx<T> t1 = {v[1].x + v[2].x, v[1].y + v[2].y};
+        cplx<T> t2 = {v[1].x - v[2].x, v[1].y - v[2].y};
+        cplx<T> m = {v[0].x - (T)0.5 * t1.x, v[0].y - (T)0.5 * t1.y};
+        cplx<T> e = {-sign * s3 * t2.y, sign * s3 * t2.x};
+        v[0] = {v[0].x + t1.x, v[0].y + t1.y};
+        v[1] = {m.x + e.x, m.y + e.y};
+        v[2] = {m.x - e.x, m.y - e.y};
+    }
+}
+
+template <typename T, int R>
+__device__ __forceinline__ void fft_pass(const cplx<T>* in, cplx<T>* out, int n, int Ns, int nl, int ls,
+                                         const cplx<T>* __restrict__ tw, int sign) {
+    const int nR = n / R, step = n / (Ns * R), total = nl * nR;
+    for (int b = threadIdx.x; b < total; b += blockDim.x) {
+        const int l = b / nR, j = b - l * nR;
+        const int k = j % Ns;
+        const cplx<T>* src = in + l * ls;
+        cplx<T>* dst = out + l * ls;
+        cplx<T> v[R];
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            cplx<T> a = src[j + r * nR];
+            if (r > 0 && k > 0) {
+                cplx<T> w = tw[r * k * step];
+                if (sign > 0) w.y = -w.y;
+                a = cmul(a, w);
+            }
+            v[r] = a;
+        }
+        dft_small<T, R>(v, sign);
+        const int d = (j / Ns) * Ns * R + k;
+#pragma unroll
+        for (int r = 0; r < R; r++) dst[d + r * Ns] = v[r];
+    }
+}
+
+template <typename T>
+__device__ cplx<T>* fft_lines(cplx<T>* A, cplx<T>* B, int nl, int ls, const FftPlan& P, const cplx<T>* tw,
+                              int sign) {
+    int Ns = 1;
+    for (int f = 0; f < P.nf; f++) {
+        const int R = P.fac[f];
+        __syncthreads();
+        if (R == 4) fft_pass<T, 4>(A, B, P.n, Ns, nl, ls, tw, sign);
+        else if (R == 2) fft_pass<T, 2>(A, B, P.n, Ns, nl, ls, tw, sign);
+        else fft_pass<T, 3>(A, B, P.n, Ns, nl, ls, tw, sign);
+        cplx<T>* s = A;
+        A = B;
+        B = s;
+        Ns *= R;
+    }
+    __syncthreads();
+    return A;
+}
+
+}  // namespace tc
