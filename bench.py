@@ -54,12 +54,17 @@ def peaks():
     return FALLBACK_HBM_GBS, "fallback"
 
 
+GRID = None  # (NX, NY, NZ) override for profiling runs (--grid); not a bench number
+
+
 def workload_params(precision: int, device: int, small: bool = False):
     import turbchannel_b200 as tb
 
     w = dict(WORKLOAD)
     if small:
         w.update(NX=96, NY=96, NZ=64)
+    if GRID:
+        w.update(NX=GRID[0], NY=GRID[1], NZ=GRID[2])
     p, zz = tb.channel_params(w["scheme"], w["NX"], w["NY"], w["NZ"], w["Lx"], w["Ly"], w["Re_b"], w["gamma"],
                               precision=precision, device=device)
     return p, zz, w
@@ -292,7 +297,15 @@ def main():
     ap.add_argument("--small", action="store_true", help="96x64x96 grid (quick check, not a bench number)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--only", choices=["mixed", "fp64"], help="time one precision only (profiling)")
+    ap.add_argument("--grid", type=int, nargs=3, metavar=("NX", "NY", "NZ"),
+                    help="override the grid (profiling runs; not a bench number)")
     args = ap.parse_args()
+    global GRID
+    if args.grid:
+        GRID = tuple(args.grid)
+    if args.only == "mixed":
+        args.no_fp64 = True
     args.warmup = max(3, args.warmup)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -309,6 +322,17 @@ def main():
     peak, peak_kind = peaks()
     import turbchannel_b200 as tb
 
+    if args.only == "fp64":
+        a = time_arm(tb.FP64, args.steps, args.warmup, local, dist_ctx, small=args.small, clocks=False)
+        a["steps"] = args.steps
+        r64, sr64, pp64 = roofline_for(a, peak, 8)
+        if rank == 0:
+            print(json.dumps({"fp64_only": True, "ms_per_step": a["ms"] / args.steps, "roofline": r64,
+                              "step_roofline": sr64, "phases_ms": pp64}), flush=True)
+        a["solver"].close()
+        if dist_ctx:
+            dist_ctx.close()
+        return
     mixed = time_arm(tb.MIXED, args.steps, args.warmup, local, dist_ctx, small=args.small)
     mixed["steps"] = args.steps
     roof, step_roof, per_phase = roofline_for(mixed, peak, 4)
@@ -336,6 +360,8 @@ def main():
 
     if rank == 0:
         w = WORKLOAD if not args.small else dict(WORKLOAD, NX=96, NY=96, NZ=64)
+        if GRID:
+            w = dict(WORKLOAD, NX=GRID[0], NY=GRID[1], NZ=GRID[2])
         roof["peak_kind"] = f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind
         line = {
             "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world, "steps": args.steps,

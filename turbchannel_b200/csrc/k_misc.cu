@@ -35,6 +35,7 @@ __global__ void __launch_bounds__(KX* KY) k_correct(CorrArgs<T> a, int tz) {
         du = (T)d;
         if (blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0) *a.du_out = d;
     }
+#pragma unroll 4
     for (int z = zb; z < ze; z++) {
         const size_t pl = (size_t)z * NXY, id = pl + (size_t)iy * NX + ix;
         const T p0 = __ldg(p + id);
@@ -78,10 +79,9 @@ __global__ void __launch_bounds__(KX* KY) k_correct(CorrArgs<T> a, int tz) {
     }
 }
 
+// Short z-columns (4 planes per thread) keep enough loads in flight per SM.
 static void column_shape(const Geom& g, dim3& grid, int& tz) {
-    const int tiles = ((g.NX + KX - 1) / KX) * ((g.NY + KY - 1) / KY);
-    const int nch = std::max(1, (148 * 8 + tiles - 1) / tiles);
-    tz = std::max(1, (g.NZ + nch - 1) / nch);
+    tz = 4;
     grid = dim3((g.NX + KX - 1) / KX, (g.NY + KY - 1) / KY, (g.NZ + tz - 1) / tz);
 }
 

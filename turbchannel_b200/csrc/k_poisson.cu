@@ -149,14 +149,12 @@ __device__ void normalize_mean_mode(const ZSolveArgs<T>& a) {
     }
 }
 
+// x: the mode's column (stride zs between z), sc: its elimination coefficients
+// (stride M between rows).
 template <typename C, typename T, int SCHEME>
-__device__ void zsolve_mode(const ZSolveArgs<T>& a, int kx, int ky, C* sc) {
+__device__ void zsolve_mode_at(const ZSolveArgs<T>& a, int kx, int ky, C* sc, cplx<T>* x, size_t zs, size_t M) {
     const Geom& g = a.g;
     const int NZ = g.NZ;
-    const size_t M = (size_t)g.NXH * g.NY;
-    const size_t m = (size_t)kx * g.NY + ky;
-    cplx<T>* x = a.spec + m;
-    const size_t zs = M;  // spec stride between z-planes
     const bool pin = (kx == 0 && ky == 0);
     if (SCHEME == TC_SCHEME_HW2 || SCHEME == TC_SCHEME_COLLOC) {
         const C* MA = pickm<C>(a.m.MAT_A, a.m.dMAT_A);
@@ -314,25 +312,61 @@ __global__ void __launch_bounds__(128) k_zsolve_all(ZSolveArgs<T> a, int skip_lo
     const int kx = (int)(m / g.NY), ky = (int)(m - (size_t)kx * g.NY);
     const int LM = g.low_modes;
     if (skip_low && kx < LM && (ky < LM || ky > g.NY - LM)) return;
-    zsolve_mode<C, T, SCHEME>(a, kx, ky, reinterpret_cast<C*>(a.scratch) + m);
+    zsolve_mode_at<C, T, SCHEME>(a, kx, ky, reinterpret_cast<C*>(a.scratch) + m, a.spec + m, M, M);
     if (!skip_low && m == 0) normalize_mean_mode(a);
 }
 
 // The low-|k| modes (kx < LM, |ky| < LM) in double; mode (0,0) also normalised.
+// One CTA per mode: the column is staged into shared memory by all threads (so
+// the sequential elimination by one thread runs at shared-memory latency), the
+// elimination coefficients stay in shared memory, the result is written back by
+// all threads.
 template <typename T, int SCHEME>
-__global__ void __launch_bounds__(64) k_zsolve_low(ZSolveArgs<T> a) {
+__global__ void __launch_bounds__(128) k_zsolve_low(ZSolveArgs<T> a) {
+    extern __shared__ __align__(16) unsigned char smraw[];
     const Geom& g = a.g;
     const int LM = g.low_modes, nky = 2 * LM - 1;
-    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= LM * nky) return;
+    const int idx = blockIdx.x;
     const int kx = idx / nky, j = idx - kx * nky;
     const int ky = j < LM ? j : g.NY - (j - LM + 1);
     if (kx >= g.NXH || ky < 0 || ky >= g.NY) return;
+    const int NZ = g.NZ;
     const size_t M = (size_t)g.NXH * g.NY;
     const size_t m = (size_t)kx * g.NY + ky;
-    zsolve_mode<double, T, SCHEME>(a, kx, ky, reinterpret_cast<double*>(a.scratch) + m);
-    if (m == 0) normalize_mean_mode(a);
-    (void)M;
+    cplx<double>* xs = reinterpret_cast<cplx<double>*>(smraw);
+    double* sc = reinterpret_cast<double*>(xs + NZ);
+    for (int i = threadIdx.x; i < NZ; i += blockDim.x) {
+        const cplx<T> v = a.spec[(size_t)i * M + m];
+        xs[i] = {(double)v.x, (double)v.y};
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ZSolveArgs<double> b;
+        b.g = g;
+        b.g.NXH = 1;
+        b.g.NY = 1;  // a single column: stride 1 between z, mode index 0
+        b.m.MAT_A = a.m.dMAT_A; b.m.DZ = a.m.dDZ; b.m.DZW = a.m.dDZW; b.m.KERG = a.m.dKERG; b.m.cellh = a.m.dcellh;
+        b.m.ZZ = a.m.dZZ; b.m.GC1 = b.m.GC2 = b.m.GCZ = nullptr;
+        b.m.dMAT_A = a.m.dMAT_A; b.m.dDZ = a.m.dDZ; b.m.dDZW = a.m.dDZW; b.m.dKERG = a.m.dKERG;
+        b.m.dcellh = a.m.dcellh; b.m.dZZ = a.m.dZZ;
+        for (int k = 0; k < 6; k++) b.m.MAT_D[k] = a.m.MAT_D[k];
+        b.m.KERG_norm2 = a.m.KERG_norm2;
+        b.tabs = a.tabs;
+        b.spec = xs;
+        b.scratch = sc;
+        b.err_flag = a.err_flag;
+        zsolve_mode_at<double, double, SCHEME>(b, kx, ky, sc, xs, 1, 1);
+        if (m == 0) {
+            b.g.NXH = 1;
+            b.g.NY = 1;
+            normalize_mean_mode(b);
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < NZ; i += blockDim.x) {
+        const cplx<double> v = xs[i];
+        a.spec[(size_t)i * M + m] = {(T)v.x, (T)v.y};
+    }
 }
 
 size_t zsolve_scratch_bytes(const Geom& g, int elem_bytes) {
@@ -353,7 +387,11 @@ static void zsolve_scheme(const ZSolveArgs<T>& a, cudaStream_t s) {
         // only in time: the launches are stream-ordered).
         k_zsolve_all<float, T, SCHEME><<<(unsigned)((M + 127) / 128), 128, 0, s>>>(a, 1);
         const int nlow = a.g.low_modes * (2 * a.g.low_modes - 1);
-        k_zsolve_low<T, SCHEME><<<(nlow + 63) / 64, 64, 0, s>>>(a);
+        const int nc = SCHEME == TC_SCHEME_VV4 ? 3 : 1;
+        const size_t smem = (size_t)a.g.NZ * (sizeof(cplx<double>) + nc * sizeof(double));
+        auto k = k_zsolve_low<T, SCHEME>;
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k<<<nlow, 128, smem, s>>>(a);
     }
 }
 
