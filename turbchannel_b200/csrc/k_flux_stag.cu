@@ -17,23 +17,75 @@
 namespace tc {
 
 constexpr int STX = 32, STY = 8;
+constexpr int SG = 4;  // x-halo of the shared tile: a multiple of the 16-byte chunk for float and double
 
 template <typename T, int H>
 struct RingAcc {
-    static constexpr int PW = STX + 2 * H, PH = STY + 2 * H, PL = PW * PH, RS = 2 * H + 2;
+    static constexpr int PW = STX + 2 * SG, PH = STY + 2 * H, PL = PW * PH, RS = 2 * H + 2;
     const T* ring;
     int zs, tx, ty;
     __device__ __forceinline__ T operator()(int c, int dx, int dy, int dz) const {
         const int slot = (zs + dz) & (RS - 1);
-        return ring[((slot * 3 + c) * PH + ty + H + dy) * PW + tx + H + dx];
+        return ring[((slot * 3 + c) * PH + ty + H + dy) * PW + tx + SG + dx];
     }
 };
 
-template <typename T, int SCHEME, int VISC, bool LES, int ORDER>
+// One plane of the tile plus halo (3 components) into ring slot z & (RS-1).
+// VEC: 16-byte LDGSTS per chunk (the x-halo is chunk aligned, so periodic wrap is a
+// whole-chunk shift); otherwise element-wise copies.
+template <typename T, int H, bool VEC>
+__device__ __forceinline__ void load_plane(T* ring, const T* const* vel, int z, int x0, int y0, int NX, int NY,
+                                           size_t NXY) {
+    using ACC = RingAcc<T, H>;
+    constexpr int PW = ACC::PW, PH = ACC::PH, PL = ACC::PL, RS = ACC::RS;
+    T* dst = ring + (z & (RS - 1)) * 3 * PL;
+    if (VEC) {
+        constexpr int CH = 16 / sizeof(T), NCH = PW / CH, PER = PH * NCH;
+        for (int e = threadIdx.x; e < 3 * PER; e += blockDim.x) {
+            const int c = e / PER, r = e - c * PER, py = r / NCH, ch = r - py * NCH;
+            const int gy = wrapi(y0 - H + py, NY), gx = wrapi(x0 - SG + ch * CH, NX);
+            cp_async<16>(dst + c * PL + py * PW + ch * CH, vel[c] + (size_t)z * NXY + (size_t)gy * NX + gx);
+        }
+    } else {
+        for (int e = threadIdx.x; e < 3 * PL; e += blockDim.x) {
+            const int c = e / PL, r = e - c * PL, py = r / PW, px = r - py * PW;
+            const int gx = wrapi(x0 - SG + px, NX), gy = wrapi(y0 - H + py, NY);
+            cp_async<sizeof(T)>(dst + e, vel[c] + (size_t)z * NXY + (size_t)gy * NX + gx);
+        }
+    }
+}
+
+template <typename T, int SCHEME, int VISC, bool LES, bool INT>
+__device__ __forceinline__ void flux_cell(const RingAcc<T, SCHEME == TC_SCHEME_VV4 ? 3 : 1>& A, const StagZ<T>& mz,
+                                          T gcz, const FluxArgs<T>& a, int ix, int iy, int xm, int xp, int ym,
+                                          int yp, size_t NXY, T f[3]) {
+    T cf[3], vf[3];
+    if constexpr (SCHEME == TC_SCHEME_VV4) conv_vv4<T, RingAcc<T, 3>, INT>(A, mz, gcz, cf);
+    else conv_hw2<T, RingAcc<T, 1>, INT>(A, mz, cf);
+    if constexpr (VISC == TC_VISC_CROSS) {
+        visc_cross<T, RingAcc<T, SCHEME == TC_SCHEME_VV4 ? 3 : 1>, INT>(A, mz, vf);
+    } else {
+        const T* nt = a.nu_t;
+        const int z = mz.iz;
+        const T visc = mz.visc;
+        auto MU = [&](int dx, int dy, int dz) -> T {
+            if (!LES) return visc;
+            const int xx = dx < 0 ? xm : (dx > 0 ? xp : ix);
+            const int yy = dy < 0 ? ym : (dy > 0 ? yp : iy);
+            return visc + __ldg(nt + (size_t)(z + dz) * NXY + (size_t)yy * a.g.NX + xx);
+        };
+        visc_naive<T, RingAcc<T, SCHEME == TC_SCHEME_VV4 ? 3 : 1>, decltype(MU), INT>(A, MU, mz, vf);
+    }
+    f[0] = ((T)a.g.sour_dpdx + cf[0]) + vf[0];
+    f[1] = (T(0) + cf[1]) + vf[1];
+    f[2] = (T(0) + cf[2]) + vf[2];
+}
+
+template <typename T, int SCHEME, int VISC, bool LES, int ORDER, bool VEC>
 __global__ void __launch_bounds__(STX* STY, 2) k_flux_stag(FluxArgs<T> a, int tz) {
     constexpr int H = SCHEME == TC_SCHEME_VV4 ? 3 : 1;
     using ACC = RingAcc<T, H>;
-    constexpr int PW = ACC::PW, PL = ACC::PL, RS = ACC::RS;
+    constexpr int RS = ACC::RS;
     extern __shared__ __align__(16) unsigned char smraw[];
     T* ring = reinterpret_cast<T*>(smraw);
     __shared__ double sbuf[32];
@@ -46,16 +98,10 @@ __global__ void __launch_bounds__(STX* STY, 2) k_flux_stag(FluxArgs<T> a, int tz
     const int zb = blockIdx.z * tz, ze = min(NZ, zb + tz);
     const int ix = x0 + tx, iy = y0 + ty;
     const bool active = ix < NX && iy < NY;
+    // interior planes: no wall special case of the scheme applies
+    const int zlo = SCHEME == TC_SCHEME_VV4 ? 3 : 1, zhi = SCHEME == TC_SCHEME_VV4 ? NZ - 4 : NZ - 2;
 
-    auto load_plane = [&](int z) {
-        T* dst = ring + (z & (RS - 1)) * 3 * PL;
-        for (int e = threadIdx.x; e < 3 * PL; e += blockDim.x) {
-            const int c = e / PL, r = e - c * PL, py = r / PW, px = r - py * PW;
-            const int gx = wrapi(x0 - H + px, NX), gy = wrapi(y0 - H + py, NY);
-            cp_async<sizeof(T)>(dst + e, a.vel.c[c] + (size_t)z * NXY + (size_t)gy * NX + gx);
-        }
-    };
-    for (int z = max(0, zb - H); z <= min(NZ - 1, zb + H); z++) load_plane(z);
+    for (int z = max(0, zb - H); z <= min(NZ - 1, zb + H); z++) load_plane<T, H, VEC>(ring, a.vel.c, z, x0, y0, NX, NY, NXY);
     cp_async_commit();
 
     StagZ<T> mz;
@@ -73,34 +119,32 @@ __global__ void __launch_bounds__(STX* STY, 2) k_flux_stag(FluxArgs<T> a, int tz
     double ub = 0.0;
 
     for (int z = zb; z < ze; z++) {
-        if (z + 1 < ze && z + H + 1 < NZ) load_plane(z + H + 1);
+        if (z + 1 < ze && z + H + 1 < NZ) load_plane<T, H, VEC>(ring, a.vel.c, z + H + 1, x0, y0, NX, NY, NXY);
         cp_async_commit();
+        const size_t id = (size_t)z * NXY + (size_t)iy * NX + ix;
+        // history of this cell, issued before the stencil so its latency overlaps it
+        T hp[3], hq[3], vp[3], vq[3];
+        if (ORDER >= 2 && active) {
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                hp[c] = __ldg(a.fp.c[c] + id);
+                vp[c] = __ldg(a.velp.c[c] + id);
+                if (ORDER == 3) {
+                    hq[c] = __ldg(a.fq.c[c] + id);
+                    vq[c] = __ldg(a.velq.c[c] + id);
+                }
+            }
+        }
         cp_async_wait<1>();
         __syncthreads();
         if (active) {
             mz.iz = z;
             const ACC A{ring, z & (RS - 1), tx, ty};
-            T cf[3], vf[3];
-            if (SCHEME == TC_SCHEME_VV4) conv_vv4(A, mz, a.m.GCZ[z], cf);
-            else conv_hw2(A, mz, cf);
-            if (VISC == TC_VISC_CROSS) {
-                visc_cross(A, mz, vf);
-            } else {
-                const T* nt = a.nu_t;
-                auto MU = [&](int dx, int dy, int dz) -> T {
-                    if (!LES) return (T)g.visc;
-                    const int xx = dx < 0 ? xm : (dx > 0 ? xp : ix);
-                    const int yy = dy < 0 ? ym : (dy > 0 ? yp : iy);
-                    return (T)g.visc + __ldg(nt + (size_t)(z + dz) * NXY + (size_t)yy * NX + xx);
-                };
-                visc_naive(A, MU, mz, vf);
-            }
+            const T gcz = SCHEME == TC_SCHEME_VV4 ? a.m.GCZ[z] : T(0);
             T f[3];
-            f[0] = ((T)g.sour_dpdx + cf[0]) + vf[0];
-            f[1] = (T(0) + cf[1]) + vf[1];
-            f[2] = (T(0) + cf[2]) + vf[2];
+            if (z >= zlo && z <= zhi) flux_cell<T, SCHEME, VISC, LES, true>(A, mz, gcz, a, ix, iy, xm, xp, ym, yp, NXY, f);
+            else flux_cell<T, SCHEME, VISC, LES, false>(A, mz, gcz, a, ix, iy, xm, xp, ym, yp, NXY, f);
             if (z == 0) f[2] = 0;
-            const size_t id = (size_t)z * NXY + (size_t)iy * NX + ix;
 #pragma unroll
             for (int c = 0; c < 3; c++) a.fout.c[c][id] = f[c];
             if (ORDER > 0) {
@@ -108,15 +152,11 @@ __global__ void __launch_bounds__(STX* STY, 2) k_flux_stag(FluxArgs<T> a, int tz
 #pragma unroll
                 for (int c = 0; c < 3; c++) {
                     const T vn = A(c, 0, 0, 0);
-                    if (ORDER == 1) {
-                        r[c] = f[c] + inv_tau * vn;
-                    } else if (ORDER == 2) {
-                        r[c] = (T(2.) * f[c] - a.fp.c[c][id]) + inv_tau * (2 * vn - T(0.5) * a.velp.c[c][id]);
-                    } else {
-                        r[c] = ((3 * f[c] - 3 * a.fp.c[c][id]) + a.fq.c[c][id]) +
-                               inv_tau * ((3 * vn - T(1.5) * a.velp.c[c][id]) +
-                                          T(0.33333333333333333333) * a.velq.c[c][id]);
-                    }
+                    if (ORDER == 1) r[c] = f[c] + inv_tau * vn;
+                    else if (ORDER == 2) r[c] = (T(2.) * f[c] - hp[c]) + inv_tau * (2 * vn - T(0.5) * vp[c]);
+                    else
+                        r[c] = ((3 * f[c] - 3 * hp[c]) + hq[c]) +
+                               inv_tau * ((3 * vn - T(1.5) * vp[c]) + T(0.33333333333333333333) * vq[c]);
                     a.rhs.c[c][id] = r[c];
                 }
                 ub += (double)r[0] * (double)a.m.DZ[z];
@@ -147,13 +187,10 @@ int flux_grid_blocks(const Geom& g) {
 template <typename T, int SCHEME, int VISC, bool LES, int ORDER>
 static void run(const FluxArgs<T>& a, cudaStream_t s) {
     constexpr int H = SCHEME == TC_SCHEME_VV4 ? 3 : 1;
-    constexpr size_t smem = sizeof(T) * (2 * H + 2) * 3 * (STX + 2 * H) * (STY + 2 * H);
-    static bool attr = false;
-    auto kern = k_flux_stag<T, SCHEME, VISC, LES, ORDER>;
-    if (!attr) {
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        attr = true;
-    }
+    constexpr size_t smem = sizeof(T) * (2 * H + 2) * 3 * RingAcc<T, H>::PL;
+    const bool vec = a.g.NX % (16 / (int)sizeof(T)) == 0;
+    auto kern = vec ? k_flux_stag<T, SCHEME, VISC, LES, ORDER, true> : k_flux_stag<T, SCHEME, VISC, LES, ORDER, false>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     dim3 grid;
     int tz;
     flux_stag_shape(a.g, grid, tz);

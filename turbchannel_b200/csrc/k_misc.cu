@@ -16,6 +16,42 @@ constexpr int KX = 32, KY = 8;
 // staggered/func_global.h:939-941, collocated_AB3/func_global.h:430-448.
 // Each thread marches a column of z; x/y neighbours of p come through L1.
 // ---------------------------------------------------------------------------
+// Gradient of p at (ix, iy, z) from the column values p(z-2..z+1) and the x/y
+// neighbours (plane z) loaded by the caller.
+template <typename T, int SCHEME>
+__device__ __forceinline__ void grad_at(const CorrArgs<T>& a, int z, int NZ, T p0, T pxm, T pxmm, T pxp, T pym, T pymm,
+                                        T pyp, T pzm, T pzmm, T pzp, T gp[3]) {
+    const T ihx = (T)a.g.inv_hx, ihy = (T)a.g.inv_hy;
+    if (SCHEME == TC_SCHEME_HW2) {
+        gp[0] = ihx * (p0 - pxm);
+        gp[1] = ihy * (p0 - pym);
+        gp[2] = z == 0 ? T(0) : (p0 - pzm) * (2 / (a.m.DZ[z] + a.m.DZ[z - 1]));
+    } else if (SCHEME == TC_SCHEME_VV4) {
+        const T g1 = a.m.GC1[z], g2 = a.m.GC2[z];
+        gp[0] = ihx * (g1 * (p0 - pxm) + g2 * (pxp - pxmm));
+        gp[1] = ihy * (g1 * (p0 - pym) + g2 * (pyp - pymm));
+        if (z == 0) {
+            gp[2] = 0;
+        } else {
+            const T pr = z == NZ - 1 ? -p0 : pzp;
+            const T pll = z == 1 ? -pzm : pzmm;
+            gp[2] = ((p0 - pzm) - T(0.03703703703703703703) * (pr - pll)) * a.m.GCZ[z];
+        }
+    } else {
+        if (z == 0 || z == NZ - 1) {
+            gp[0] = gp[1] = gp[2] = 0;
+        } else {
+            gp[0] = T(0.5) * ihx * (pxp - pxm);
+            gp[1] = T(0.5) * ihy * (pyp - pym);
+            gp[2] = T(0.5) * (pzp - pzm) / a.m.cellh[z];
+        }
+    }
+}
+
+// Each thread owns a column of ZC planes; all loads of the column are issued
+// before any arithmetic so that they are in flight together.
+constexpr int ZC = 4;
+
 template <typename T, int SCHEME, bool STAB1, bool GRADONLY>
 __global__ void __launch_bounds__(KX* KY) k_correct(CorrArgs<T> a, int tz) {
     const Geom& g = a.g;
@@ -23,11 +59,10 @@ __global__ void __launch_bounds__(KX* KY) k_correct(CorrArgs<T> a, int tz) {
     const size_t NXY = (size_t)NX * NY;
     const int ix = blockIdx.x * KX + threadIdx.x % KX, iy = blockIdx.y * KY + threadIdx.x / KX;
     if (ix >= NX || iy >= NY) return;
-    const int zb = blockIdx.z * tz, ze = min(NZ, zb + tz);
+    const int zb = blockIdx.z * ZC;
     const int xm = wrapi(ix - 1, NX), xmm = wrapi(ix - 2, NX), xp = wrapi(ix + 1, NX);
     const int ym = wrapi(iy - 1, NY), ymm = wrapi(iy - 2, NY), yp = wrapi(iy + 1, NY);
-    const T* p = a.p;
-    const T ihx = (T)g.inv_hx, ihy = (T)g.inv_hy;
+    const T* __restrict__ p = a.p;
     T du = 0;
     if (!GRADONLY && a.cfr) {
         const double ub = (*a.ub_sum) * a.cfr_scale * (double)a.tob;
@@ -35,53 +70,54 @@ __global__ void __launch_bounds__(KX* KY) k_correct(CorrArgs<T> a, int tz) {
         du = (T)d;
         if (blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0) *a.du_out = d;
     }
-#pragma unroll 4
-    for (int z = zb; z < ze; z++) {
-        const size_t pl = (size_t)z * NXY, id = pl + (size_t)iy * NX + ix;
-        const T p0 = __ldg(p + id);
-        T gp[3];
-        if (SCHEME == TC_SCHEME_HW2) {
-            gp[0] = ihx * (p0 - __ldg(p + pl + (size_t)iy * NX + xm));
-            gp[1] = ihy * (p0 - __ldg(p + pl + (size_t)ym * NX + ix));
-            gp[2] = z == 0 ? T(0) : (p0 - __ldg(p + id - NXY)) * (2 / (a.m.DZ[z] + a.m.DZ[z - 1]));
-        } else if (SCHEME == TC_SCHEME_VV4) {
-            const T g1 = a.m.GC1[z], g2 = a.m.GC2[z];
-            gp[0] = ihx * (g1 * (p0 - __ldg(p + pl + (size_t)iy * NX + xm)) +
-                           g2 * (__ldg(p + pl + (size_t)iy * NX + xp) - __ldg(p + pl + (size_t)iy * NX + xmm)));
-            gp[1] = ihy * (g1 * (p0 - __ldg(p + pl + (size_t)ym * NX + ix)) +
-                           g2 * (__ldg(p + pl + (size_t)yp * NX + ix) - __ldg(p + pl + (size_t)ymm * NX + ix)));
-            if (z == 0) {
-                gp[2] = 0;
-            } else {
-                const T pl1 = __ldg(p + id - NXY);
-                const T pr = z == NZ - 1 ? -p0 : __ldg(p + id + NXY);
-                const T pll = z == 1 ? -pl1 : __ldg(p + id - 2 * NXY);
-                gp[2] = ((p0 - pl1) - T(0.03703703703703703703) * (pr - pll)) * a.m.GCZ[z];
-            }
-        } else {
-            if (z == 0 || z == NZ - 1) {
-                gp[0] = gp[1] = gp[2] = 0;
-            } else {
-                gp[0] = T(0.5) * ihx * (__ldg(p + pl + (size_t)iy * NX + xp) - __ldg(p + pl + (size_t)iy * NX + xm));
-                gp[1] = T(0.5) * ihy * (__ldg(p + pl + (size_t)yp * NX + ix) - __ldg(p + pl + (size_t)ym * NX + ix));
-                gp[2] = T(0.5) * (__ldg(p + id + NXY) - __ldg(p + id - NXY)) / a.m.cellh[z];
-            }
+    // column values p(zb-2 .. zb+ZC) at (ix, iy); zero outside the domain (never used there)
+    T col[ZC + 3];
+#pragma unroll
+    for (int k = 0; k < ZC + 3; k++) {
+        const int z = zb - 2 + k;
+        col[k] = (z >= 0 && z < NZ) ? __ldg(p + (size_t)z * NXY + (size_t)iy * NX + ix) : T(0);
+    }
+    T nb[ZC][6], rh[ZC][3], pc[ZC];
+#pragma unroll
+    for (int k = 0; k < ZC; k++) {
+        const int z = zb + k;
+        if (z >= NZ) break;
+        const size_t pl = (size_t)z * NXY;
+        nb[k][0] = __ldg(p + pl + (size_t)iy * NX + xm);
+        nb[k][1] = __ldg(p + pl + (size_t)iy * NX + xmm);
+        nb[k][2] = __ldg(p + pl + (size_t)iy * NX + xp);
+        nb[k][3] = __ldg(p + pl + (size_t)ym * NX + ix);
+        nb[k][4] = __ldg(p + pl + (size_t)ymm * NX + ix);
+        nb[k][5] = __ldg(p + pl + (size_t)yp * NX + ix);
+        if (!GRADONLY) {
+            const size_t id = pl + (size_t)iy * NX + ix;
+#pragma unroll
+            for (int c = 0; c < 3; c++) rh[k][c] = __ldg(a.rhs.c[c] + id);
+            if (STAB1) pc[k] = __ldg(a.pcur + id);
         }
+    }
+#pragma unroll
+    for (int k = 0; k < ZC; k++) {
+        const int z = zb + k;
+        if (z >= NZ) break;
+        const size_t id = (size_t)z * NXY + (size_t)iy * NX + ix;
+        T gp[3];
+        grad_at<T, SCHEME>(a, z, NZ, col[k + 2], nb[k][0], nb[k][1], nb[k][2], nb[k][3], nb[k][4], nb[k][5], col[k + 1],
+                           col[k], col[k + 3], gp);
         if (GRADONLY) {
 #pragma unroll
             for (int c = 0; c < 3; c++) a.vout.c[c][id] = gp[c];
         } else {
 #pragma unroll
-            for (int c = 0; c < 3; c++) a.vout.c[c][id] = (a.rhs.c[c][id] - gp[c]) * a.tob;
+            for (int c = 0; c < 3; c++) a.vout.c[c][id] = (rh[k][c] - gp[c]) * a.tob;
             if (a.cfr && !(SCHEME == TC_SCHEME_COLLOC && (z == 0 || z == NZ - 1))) a.vout.c[0][id] += du;
-            if (STAB1) a.pnext[id] = p0 + a.pcur[id];
+            if (STAB1) a.pnext[id] = col[k + 2] + pc[k];
         }
     }
 }
 
-// Short z-columns (4 planes per thread) keep enough loads in flight per SM.
 static void column_shape(const Geom& g, dim3& grid, int& tz) {
-    tz = 4;
+    tz = ZC;
     grid = dim3((g.NX + KX - 1) / KX, (g.NY + KY - 1) / KY, (g.NZ + tz - 1) / tz);
 }
 

@@ -42,7 +42,7 @@ __global__ void __launch_bounds__(256) k_div_xfft(DivFftArgs<T> a, int rows) {
         const int r = e / NX, x = e - r * NX;
         Ar[2 * ((r >> 1) * NX + x) + (r & 1)] = div_at<T, SCHEME, SCALAR>(g, a.m, a.v, a.src_scalar, x, y0 + r, z);
     }
-    const cplx<T>* R = fft_lines(A, B, nl, NX, a.px, a.twx, -1);
+    const cplx<T>* R = fft_lines_any(A, B, nl, NX, a.px, a.twx, -1);
     for (int e = threadIdx.x; e < NXH * rows; e += blockDim.x) {
         const int kx = e / rows, r = e - kx * rows, l = r >> 1;
         const cplx<T> Zk = R[l * NX + kx], Zm = R[l * NX + (kx == 0 ? 0 : NX - kx)];
@@ -91,7 +91,7 @@ __global__ void __launch_bounds__(256) k_yfft(YFftArgs<T> a, int lines) {
     cplx<T>* B = A + lines * NY;
     cplx<T>* src = a.spec + L0 * NY;
     for (int e = threadIdx.x; e < nl * NY; e += blockDim.x) A[e] = src[e];
-    const cplx<T>* R = fft_lines(A, B, nl, NY, a.py, a.twy, a.sign);
+    const cplx<T>* R = fft_lines_any(A, B, nl, NY, a.py, a.twy, a.sign);
     for (int e = threadIdx.x; e < nl * NY; e += blockDim.x) src[e] = R[e];
 }
 
@@ -150,15 +150,18 @@ __device__ void normalize_mean_mode(const ZSolveArgs<T>& a) {
 }
 
 // x: the mode's column (stride zs between z), sc: its elimination coefficients
-// (stride M between rows).
+// (stride M between rows); MA, DZ, DZW: the banded-matrix mesh arrays (global or
+// shared memory).  Rows are fetched ZR at a time ahead of the recurrence so their
+// load latency overlaps it.
+constexpr int ZR = 4;
+
 template <typename C, typename T, int SCHEME>
-__device__ void zsolve_mode_at(const ZSolveArgs<T>& a, int kx, int ky, C* sc, cplx<T>* x, size_t zs, size_t M) {
+__device__ void zsolve_mode_at(const ZSolveArgs<T>& a, int kx, int ky, C* sc, cplx<T>* x, size_t zs, size_t M,
+                               const C* MA, const C* DZ, const C* DZW) {
     const Geom& g = a.g;
     const int NZ = g.NZ;
     const bool pin = (kx == 0 && ky == 0);
     if (SCHEME == TC_SCHEME_HW2 || SCHEME == TC_SCHEME_COLLOC) {
-        const C* MA = pickm<C>(a.m.MAT_A, a.m.dMAT_A);
-        const C* DZ = SCHEME == TC_SCHEME_HW2 ? pickm<C>(a.m.DZ, a.m.dDZ) : pickm<C>(a.m.DZ, a.m.dDZ);
         C MM;
         if (SCHEME == TC_SCHEME_HW2) {
             MM = 2 * ((1 - (C)a.tabs.cosx[kx]) * (C)g.inv_hx * (C)g.inv_hx + (1 - (C)a.tabs.cosy[ky]) * (C)g.inv_hy * (C)g.inv_hy);
@@ -179,41 +182,59 @@ __device__ void zsolve_mode_at(const ZSolveArgs<T>& a, int kx, int ky, C* sc, cp
         stc(x, prev);
         C pp = MA[1] * ib0;
         sc[0] = pp;
-        for (int i = 1; i <= NZ - 1; i++) {
-            C d;
-            if (SCHEME == TC_SCHEME_HW2) {
-                d = -MA[i] - DZ[i] * MM;
-                if (i != NZ - 1) d -= MA[i + 1];
-            } else {
-                const C mm = (g.fd_mode && (i == NZ - 1)) ? C(0) : MM;
-                d = 0;
-                d -= MA[i] + DZ[i - 1] * mm;
-                if (i != NZ - 1) d -= MA[i + 1] + DZ[i] * mm;
+        for (int i0 = 1; i0 <= NZ - 1; i0 += ZR) {
+            cplx<C> xv[ZR];
+#pragma unroll
+            for (int k = 0; k < ZR; k++)
+                if (i0 + k <= NZ - 1) xv[k] = ldc<C>(x + (size_t)(i0 + k) * zs);
+#pragma unroll
+            for (int k = 0; k < ZR; k++) {
+                const int i = i0 + k;
+                if (i > NZ - 1) break;
+                C d;
+                if (SCHEME == TC_SCHEME_HW2) {
+                    d = -MA[i] - DZ[i] * MM;
+                    if (i != NZ - 1) d -= MA[i + 1];
+                } else {
+                    const C mm = (g.fd_mode && (i == NZ - 1)) ? C(0) : MM;
+                    d = 0;
+                    d -= MA[i] + DZ[i - 1] * mm;
+                    if (i != NZ - 1) d -= MA[i + 1] + DZ[i] * mm;
+                }
+                d -= MA[i] * pp;
+                d = 1 / d;
+                if (i != NZ - 1) {
+                    pp = MA[i + 1] * d;
+                    sc[(size_t)i * M] = pp;
+                }
+                cplx<C> xi = xv[k];
+                xi.x = (xi.x - MA[i] * prev.x) * d;
+                xi.y = (xi.y - MA[i] * prev.y) * d;
+                stc(x + (size_t)i * zs, xi);
+                prev = xi;
             }
-            d -= MA[i] * pp;
-            d = 1 / d;
-            if (i != NZ - 1) {
-                pp = MA[i + 1] * d;
-                sc[(size_t)i * M] = pp;
-            }
-            cplx<C> xi = ldc<C>(x + i * zs);
-            xi.x = (xi.x - MA[i] * prev.x) * d;
-            xi.y = (xi.y - MA[i] * prev.y) * d;
-            stc(x + i * zs, xi);
-            prev = xi;
         }
-        for (int i = NZ - 2; i >= 0; i--) {
-            cplx<C> xi = ldc<C>(x + i * zs);
-            const C p = sc[(size_t)i * M];
-            xi.x -= prev.x * p;
-            xi.y -= prev.y * p;
-            stc(x + i * zs, xi);
-            prev = xi;
+        for (int i0 = NZ - 2; i0 >= 0; i0 -= ZR) {
+            cplx<C> xv[ZR];
+            C pv[ZR];
+#pragma unroll
+            for (int k = 0; k < ZR; k++)
+                if (i0 - k >= 0) {
+                    xv[k] = ldc<C>(x + (size_t)(i0 - k) * zs);
+                    pv[k] = sc[(size_t)(i0 - k) * M];
+                }
+#pragma unroll
+            for (int k = 0; k < ZR; k++) {
+                const int i = i0 - k;
+                if (i < 0) break;
+                cplx<C> xi = xv[k];
+                xi.x -= prev.x * pv[k];
+                xi.y -= prev.y * pv[k];
+                stc(x + (size_t)i * zs, xi);
+                prev = xi;
+            }
         }
     } else {  // VV4, staggered/func_global.h:110-189
-        const C* MA = pickm<C>(a.m.MAT_A, a.m.dMAT_A);
-        const C* DZ = pickm<C>(a.m.DZ, a.m.dDZ);
-        const C* DZW = pickm<C>(a.m.DZW, a.m.dDZW);
         const C C27 = C(0.03703703703703703703), C9 = C(0.11111111111111111111);
         const C sx = (C)a.tabs.sinx[kx], sy = (C)a.tabs.siny[ky];
         const C s3x = 3 * sx - 4 * sx * sx * sx, s3y = 3 * sy - 4 * sy * sy * sy;
@@ -221,90 +242,112 @@ __device__ void zsolve_mode_at(const ZSolveArgs<T>& a, int kx, int ky, C* sc, cp
         const C tiny = C(1e-30);
         C b[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};  // b[j][k]: row i-3+j, coefficient of x_{row+k+1}
         cplx<C> xr[3] = {{0, 0}, {0, 0}, {0, 0}};       // eliminated rhs of rows i-3, i-2, i-1
-        for (int i = 0; i < NZ; i++) {
-            C row[7] = {0, 0, 0, 0, 0, 0, 0};
-            C sum = 0;
+        for (int i0 = 0; i0 < NZ; i0 += ZR) {
+            cplx<C> xv[ZR];
 #pragma unroll
-            for (int k = 0; k < 3; k++) {
-                if (i + k - 3 < 0 || i + k - 3 >= NZ) continue;
-                row[k] = MA[i * 3 + k];
-                sum += MA[i * 3 + k];
-            }
+            for (int k = 0; k < ZR; k++)
+                if (i0 + k < NZ) xv[k] = ldc<C>(x + (size_t)(i0 + k) * zs);
 #pragma unroll
-            for (int k = 1; k <= 3; k++) {
-                if (i + k >= NZ) continue;
-                row[3 + k] = MA[(i + k) * 3 + 3 - k];
-                sum += MA[(i + k) * 3 + 3 - k];
-            }
-            if (i <= 2) row[3] = (C)a.m.MAT_D[i];
-            else if (i >= NZ - 3) row[3] = (C)a.m.MAT_D[i - (NZ - 3) + 3];
-            else row[3] = -sum;
-            if (pin && i == 0) row[3] *= 2;
-            {
-                C ci = DZ[i] * sx - C27 * DZW[i] * s3x;
-                row[3] -= 4 * ihx * ihx * ci * ci / (DZ[i] - C9 * DZW[i]);
-                ci = DZ[i] * sy - C27 * DZW[i] * s3y;
-                row[3] -= 4 * ihy * ihy * ci * ci / (DZ[i] - C9 * DZW[i]);
-            }
-            cplx<C> xi = ldc<C>(x + (size_t)i * zs);
+            for (int kk = 0; kk < ZR; kk++) {
+                const int i = i0 + kk;
+                if (i >= NZ) break;
+                C row[7] = {0, 0, 0, 0, 0, 0, 0};
+                C sum = 0;
 #pragma unroll
-            for (int j = -3; j < 0; j++) {
-                if (i + j < 0) continue;
-                const C mult = -row[3 + j];
+                for (int k = 0; k < 3; k++) {
+                    if (i + k - 3 < 0 || i + k - 3 >= NZ) continue;
+                    row[k] = MA[i * 3 + k];
+                    sum += MA[i * 3 + k];
+                }
 #pragma unroll
                 for (int k = 1; k <= 3; k++) {
-                    if (i + j + k >= NZ) continue;
-                    row[3 + j + k] += mult * b[3 + j][k - 1];
+                    if (i + k >= NZ) continue;
+                    row[3 + k] = MA[(i + k) * 3 + 3 - k];
+                    sum += MA[(i + k) * 3 + 3 - k];
                 }
-                xi.x += mult * xr[3 + j].x;
-                xi.y += mult * xr[3 + j].y;
+                if (i <= 2) row[3] = (C)a.m.MAT_D[i];
+                else if (i >= NZ - 3) row[3] = (C)a.m.MAT_D[i - (NZ - 3) + 3];
+                else row[3] = -sum;
+                if (pin && i == 0) row[3] *= 2;
+                {
+                    C ci = DZ[i] * sx - C27 * DZW[i] * s3x;
+                    row[3] -= 4 * ihx * ihx * ci * ci / (DZ[i] - C9 * DZW[i]);
+                    ci = DZ[i] * sy - C27 * DZW[i] * s3y;
+                    row[3] -= 4 * ihy * ihy * ci * ci / (DZ[i] - C9 * DZW[i]);
+                }
+                cplx<C> xi = xv[kk];
+#pragma unroll
+                for (int j = -3; j < 0; j++) {
+                    if (i + j < 0) continue;
+                    const C mult = -row[3 + j];
+#pragma unroll
+                    for (int k = 1; k <= 3; k++) {
+                        if (i + j + k >= NZ) continue;
+                        row[3 + j + k] += mult * b[3 + j][k - 1];
+                    }
+                    xi.x += mult * xr[3 + j].x;
+                    xi.y += mult * xr[3 + j].y;
+                }
+                if (fabs((double)row[3]) < (double)tiny) {
+                    if (a.err_flag) atomicExch(a.err_flag, 1);
+                    cplx<T> bad = {(T)(sizeof(T) == 8 ? -1e50 : -1e30), (T)0};
+                    x[0] = bad;
+                    return;
+                }
+                const C mult = C(1) / row[3];
+                C nb[3];
+#pragma unroll
+                for (int k = 1; k <= 3; k++) nb[k - 1] = (i + k >= NZ) ? C(0) : row[3 + k] * mult;
+                xi.x *= mult;
+                xi.y *= mult;
+                stc(x + (size_t)i * zs, xi);
+#pragma unroll
+                for (int k = 0; k < 3; k++) sc[((size_t)i * 3 + k) * M] = nb[k];
+#pragma unroll
+                for (int j = 0; j < 2; j++) {
+                    xr[j] = xr[j + 1];
+#pragma unroll
+                    for (int k = 0; k < 3; k++) b[j][k] = b[j + 1][k];
+                }
+                xr[2] = xi;
+#pragma unroll
+                for (int k = 0; k < 3; k++) b[2][k] = nb[k];
             }
-            if (fabs((double)row[3]) < (double)tiny) {
-                if (a.err_flag) atomicExch(a.err_flag, 1);
-                cplx<T> bad = {(T)(sizeof(T) == 8 ? -1e50 : -1e30), (T)0};
-                x[0] = bad;
-                return;
-            }
-            const C mult = C(1) / row[3];
-            C nb[3];
-#pragma unroll
-            for (int k = 1; k <= 3; k++) nb[k - 1] = (i + k >= NZ) ? C(0) : row[3 + k] * mult;
-            xi.x *= mult;
-            xi.y *= mult;
-            stc(x + (size_t)i * zs, xi);
-#pragma unroll
-            for (int k = 0; k < 3; k++) sc[((size_t)i * 3 + k) * M] = nb[k];
-#pragma unroll
-            for (int j = 0; j < 2; j++) {
-                xr[j] = xr[j + 1];
-#pragma unroll
-                for (int k = 0; k < 3; k++) b[j][k] = b[j + 1][k];
-            }
-            xr[2] = xi;
-#pragma unroll
-            for (int k = 0; k < 3; k++) b[2][k] = nb[k];
         }
         cplx<C> xs[3] = {{0, 0}, {0, 0}, {0, 0}};  // x_{i+1}, x_{i+2}, x_{i+3}
-        for (int i = NZ - 1; i >= 0; i--) {
-            cplx<C> xi = ldc<C>(x + (size_t)i * zs);
+        for (int i0 = NZ - 1; i0 >= 0; i0 -= ZR) {
+            cplx<C> xv[ZR];
+            C bv[ZR][3];
 #pragma unroll
-            for (int j = 1; j <= 3; j++) {
-                if (i + j >= NZ) continue;
-                const C bb = sc[((size_t)i * 3 + j - 1) * M];
-                xi.x -= bb * xs[j - 1].x;
-                xi.y -= bb * xs[j - 1].y;
+            for (int k = 0; k < ZR; k++)
+                if (i0 - k >= 0) {
+                    xv[k] = ldc<C>(x + (size_t)(i0 - k) * zs);
+#pragma unroll
+                    for (int j = 0; j < 3; j++) bv[k][j] = sc[((size_t)(i0 - k) * 3 + j) * M];
+                }
+#pragma unroll
+            for (int kk = 0; kk < ZR; kk++) {
+                const int i = i0 - kk;
+                if (i < 0) break;
+                cplx<C> xi = xv[kk];
+#pragma unroll
+                for (int j = 1; j <= 3; j++) {
+                    if (i + j >= NZ) continue;
+                    xi.x -= bv[kk][j - 1] * xs[j - 1].x;
+                    xi.y -= bv[kk][j - 1] * xs[j - 1].y;
+                }
+                stc(x + (size_t)i * zs, xi);
+                xs[2] = xs[1];
+                xs[1] = xs[0];
+                xs[0] = xi;
             }
-            stc(x + (size_t)i * zs, xi);
-            xs[2] = xs[1];
-            xs[1] = xs[0];
-            xs[0] = xi;
         }
     }
 }
 
 // All modes (FP64) or, in the mixed mode, all modes outside the low set (float).
 template <typename C, typename T, int SCHEME>
-__global__ void __launch_bounds__(128) k_zsolve_all(ZSolveArgs<T> a, int skip_low) {
+__global__ void __launch_bounds__(64) k_zsolve_all(ZSolveArgs<T> a, int skip_low) {
     const Geom& g = a.g;
     const size_t M = (size_t)g.NXH * g.NY;
     const size_t m = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -312,7 +355,9 @@ __global__ void __launch_bounds__(128) k_zsolve_all(ZSolveArgs<T> a, int skip_lo
     const int kx = (int)(m / g.NY), ky = (int)(m - (size_t)kx * g.NY);
     const int LM = g.low_modes;
     if (skip_low && kx < LM && (ky < LM || ky > g.NY - LM)) return;
-    zsolve_mode_at<C, T, SCHEME>(a, kx, ky, reinterpret_cast<C*>(a.scratch) + m, a.spec + m, M, M);
+    zsolve_mode_at<C, T, SCHEME>(a, kx, ky, reinterpret_cast<C*>(a.scratch) + m, a.spec + m, M, M,
+                                 pickm<C>(a.m.MAT_A, a.m.dMAT_A), pickm<C>(a.m.DZ, a.m.dDZ),
+                                 pickm<C>(a.m.DZW, a.m.dDZW));
     if (!skip_low && m == 0) normalize_mean_mode(a);
 }
 
@@ -333,12 +378,20 @@ __global__ void __launch_bounds__(128) k_zsolve_low(ZSolveArgs<T> a) {
     const int NZ = g.NZ;
     const size_t M = (size_t)g.NXH * g.NY;
     const size_t m = (size_t)kx * g.NY + ky;
+    const int nc = SCHEME == TC_SCHEME_VV4 ? 3 : 1;
+    const int nma = SCHEME == TC_SCHEME_VV4 ? 3 * NZ : NZ;
     cplx<double>* xs = reinterpret_cast<cplx<double>*>(smraw);
     double* sc = reinterpret_cast<double*>(xs + NZ);
+    double* sMA = sc + (size_t)nc * NZ;
+    double* sDZ = sMA + nma;
+    double* sDZW = sDZ + NZ;
     for (int i = threadIdx.x; i < NZ; i += blockDim.x) {
         const cplx<T> v = a.spec[(size_t)i * M + m];
         xs[i] = {(double)v.x, (double)v.y};
+        sDZ[i] = a.m.dDZ[i];
+        sDZW[i] = a.m.dDZW[i];
     }
+    for (int i = threadIdx.x; i < nma; i += blockDim.x) sMA[i] = a.m.dMAT_A[i];
     __syncthreads();
     if (threadIdx.x == 0) {
         ZSolveArgs<double> b;
@@ -355,7 +408,7 @@ __global__ void __launch_bounds__(128) k_zsolve_low(ZSolveArgs<T> a) {
         b.spec = xs;
         b.scratch = sc;
         b.err_flag = a.err_flag;
-        zsolve_mode_at<double, double, SCHEME>(b, kx, ky, sc, xs, 1, 1);
+        zsolve_mode_at<double, double, SCHEME>(b, kx, ky, sc, xs, 1, 1, sMA, sDZ, sDZW);
         if (m == 0) {
             b.g.NXH = 1;
             b.g.NY = 1;
@@ -379,16 +432,17 @@ template <typename T, int SCHEME>
 static void zsolve_scheme(const ZSolveArgs<T>& a, cudaStream_t s) {
     const size_t M = (size_t)a.g.NXH * a.g.NY;
     if (sizeof(T) == sizeof(double)) {
-        k_zsolve_all<double, T, SCHEME><<<(unsigned)((M + 127) / 128), 128, 0, s>>>(a, 0);
+        k_zsolve_all<double, T, SCHEME><<<(unsigned)((M + 63) / 64), 64, 0, s>>>(a, 0);
     } else {
         // Modes outside the low set in float first, then the low set in double.  Both
         // launches share the scratch buffer, which is sized for double entries; the
         // float kernel indexes it as float (so the low-set double entries are disjoint
         // only in time: the launches are stream-ordered).
-        k_zsolve_all<float, T, SCHEME><<<(unsigned)((M + 127) / 128), 128, 0, s>>>(a, 1);
+        k_zsolve_all<float, T, SCHEME><<<(unsigned)((M + 63) / 64), 64, 0, s>>>(a, 1);
         const int nlow = a.g.low_modes * (2 * a.g.low_modes - 1);
         const int nc = SCHEME == TC_SCHEME_VV4 ? 3 : 1;
-        const size_t smem = (size_t)a.g.NZ * (sizeof(cplx<double>) + nc * sizeof(double));
+        const int nma = SCHEME == TC_SCHEME_VV4 ? 3 * a.g.NZ : a.g.NZ;
+        const size_t smem = (size_t)a.g.NZ * (sizeof(cplx<double>) + nc * sizeof(double)) + (size_t)(nma + 2 * a.g.NZ) * sizeof(double);
         auto k = k_zsolve_low<T, SCHEME>;
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         k<<<nlow, 128, smem, s>>>(a);
@@ -440,7 +494,7 @@ __global__ void __launch_bounds__(256) k_ixfft(IxFftArgs<T> a, int rows) {
         }
         A[l * NX + k] = {av.x - bv.y, av.y + bv.x};
     }
-    const cplx<T>* R = fft_lines(A, B, nl, NX, a.px, a.twx, +1);
+    const cplx<T>* R = fft_lines_any(A, B, nl, NX, a.px, a.twx, +1);
     const T sc = a.scale;
     for (int e = threadIdx.x; e < rows * NX; e += blockDim.x) {
         const int r = e / NX, x = e - r * NX;

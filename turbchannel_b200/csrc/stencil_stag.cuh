@@ -10,6 +10,9 @@
 //   visc_naive : staggered/func_global.h:564-625   (stress divergence, mu = visc+nu_t,
 //                including the reference's mu(XR(YR)) weight in sxy_190)
 //   abs_strain : staggered/func_global.h:823-870
+// The INT template flag compiles a plane-interior copy: every wall special case of
+// the reference is a test on iz, and for 3 <= iz <= NZ-4 (VV4) or 1 <= iz <= NZ-2
+// (HW2) all of them are false, so INT = true drops them at compile time.
 #pragma once
 #include "tc_common.cuh"
 
@@ -23,7 +26,7 @@ struct StagZ {  // wall-normal metric at the current plane
     T hx, hy, ihx, ihy, visc;
 };
 
-template <typename T, typename ACC>
+template <typename T, typename ACC, bool INT = false>
 __device__ __forceinline__ void conv_hw2(const ACC& A, const StagZ<T>& m, T s[3]) {
 #define U(a, b, c) A(0, a, b, c)
 #define V(a, b, c) A(1, a, b, c)
@@ -31,28 +34,28 @@ __device__ __forceinline__ void conv_hw2(const ACC& A, const StagZ<T>& m, T s[3]
     const int iz = m.iz, NZ = m.NZ;
     const T* DZ = m.DZ;
     const T inv_hz = T(1) / DZ[iz];
-    const T inv_hz_alt = T(2) / (DZ[iz] + (iz == 0 ? T(0) : DZ[iz - 1]));
+    const T inv_hz_alt = T(2) / (DZ[iz] + ((!INT && iz == 0) ? T(0) : DZ[iz - 1]));
     const T U0 = U(0, 0, 0), V0 = V(0, 0, 0), W0 = W(0, 0, 0);
     s[0] = s[1] = s[2] = 0;
     T a = U0 + U(1, 0, 0), c = U0 + U(-1, 0, 0);
     s[0] -= (a * a - c * c) * m.ihx;
     s[0] -= ((U0 + U(0, 1, 0)) * (V(0, 1, 0) + V(-1, 1, 0)) - (U0 + U(0, -1, 0)) * (V0 + V(-1, 0, 0))) * m.ihy;
-    if (iz != NZ - 1) s[0] -= (U0 + U(0, 0, 1)) * (W(0, 0, 1) + W(-1, 0, 1)) * inv_hz;
-    if (iz != 0) s[0] += (U0 + U(0, 0, -1)) * (W0 + W(-1, 0, 0)) * inv_hz;
+    if ((INT || iz != NZ - 1)) s[0] -= (U0 + U(0, 0, 1)) * (W(0, 0, 1) + W(-1, 0, 1)) * inv_hz;
+    if ((INT || iz != 0)) s[0] += (U0 + U(0, 0, -1)) * (W0 + W(-1, 0, 0)) * inv_hz;
 
     s[1] -= ((V0 + V(1, 0, 0)) * (U(1, 0, 0) + U(1, -1, 0)) - (V0 + V(-1, 0, 0)) * (U0 + U(0, -1, 0))) * m.ihx;
     a = V0 + V(0, 1, 0);
     c = V0 + V(0, -1, 0);
     s[1] -= (a * a - c * c) * m.ihy;
-    if (iz != NZ - 1) s[1] -= (V0 + V(0, 0, 1)) * (W(0, 0, 1) + W(0, -1, 1)) * inv_hz;
-    if (iz != 0) s[1] += (V0 + V(0, 0, -1)) * (W0 + W(0, -1, 0)) * inv_hz;
+    if ((INT || iz != NZ - 1)) s[1] -= (V0 + V(0, 0, 1)) * (W(0, 0, 1) + W(0, -1, 1)) * inv_hz;
+    if ((INT || iz != 0)) s[1] += (V0 + V(0, 0, -1)) * (W0 + W(0, -1, 0)) * inv_hz;
 
-    if (iz != 0) {
+    if ((INT || iz != 0)) {
         s[2] -= ((W0 + W(1, 0, 0)) * (U(1, 0, 0) * DZ[iz] + U(1, 0, -1) * DZ[iz - 1]) -
                  (W0 + W(-1, 0, 0)) * (U0 * DZ[iz] + U(0, 0, -1) * DZ[iz - 1])) * m.ihx * inv_hz_alt;
         s[2] -= ((W0 + W(0, 1, 0)) * (V(0, 1, 0) * DZ[iz] + V(0, 1, -1) * DZ[iz - 1]) -
                  (W0 + W(0, -1, 0)) * (V0 * DZ[iz] + V(0, 0, -1) * DZ[iz - 1])) * m.ihy * inv_hz_alt;
-        a = W0 + (iz == NZ - 1 ? T(0) : W(0, 0, 1));
+        a = W0 + ((!INT && iz == NZ - 1) ? T(0) : W(0, 0, 1));
         s[2] -= a * a * inv_hz_alt;
         a = W0 + W(0, 0, -1);
         s[2] += a * a * inv_hz_alt;
@@ -62,7 +65,7 @@ __device__ __forceinline__ void conv_hw2(const ACC& A, const StagZ<T>& m, T s[3]
     s[2] *= T(0.25);
 }
 
-template <typename T, typename ACC>
+template <typename T, typename ACC, bool INT = false>
 __device__ __forceinline__ void conv_vv4(const ACC& A, const StagZ<T>& m, T gcz, T s[3]) {
     const int iz = m.iz, NZ = m.NZ;
     const T *DZ = m.DZ, *DZW = m.DZW;
@@ -86,20 +89,20 @@ __device__ __forceinline__ void conv_vv4(const ACC& A, const StagZ<T>& m, T gcz,
     }
     {  // u: z-faces
         T wzl, wzr, wbzl, wbzr;
-        if (iz == 0) wzl = 0;
+        if ((!INT && iz == 0)) wzl = 0;
         else wzl = hxhy * (9 * (W0 + W(-1, 0, 0)) - (W(-2, 0, 0) + W(1, 0, 0)));
-        if (iz == NZ - 1) wzr = 0;
+        if ((!INT && iz == NZ - 1)) wzr = 0;
         else wzr = hxhy * (9 * (W(0, 0, 1) + W(-1, 0, 1)) - (W(-2, 0, 1) + W(1, 0, 1)));
-        if (iz == 1) wbzl = 0;
-        else if (iz == 0) wbzl = wzr;
+        if ((!INT && iz == 1)) wbzl = 0;
+        else if ((!INT && iz == 0)) wbzl = wzr;
         else wbzl = hxhy * (9 * (W(0, 0, -1) + W(-1, 0, -1)) - (W(-2, 0, -1) + W(1, 0, -1)));
-        if (iz == NZ - 2) wbzr = 0;
-        else if (iz == NZ - 1) wbzr = wzl;
+        if ((!INT && iz == NZ - 2)) wbzr = 0;
+        else if ((!INT && iz == NZ - 1)) wbzr = wzl;
         else wbzr = hxhy * (9 * (W(0, 0, 2) + W(-1, 0, 2)) - (W(-2, 0, 2) + W(1, 0, 2)));
-        T uzr = iz == NZ - 1 ? T(0) : U0 + U(0, 0, 1);
-        T uzrr = U0 + (iz == NZ - 3 ? -U(0, 0, 2) : iz == NZ - 2 ? T(0) : iz == NZ - 1 ? U(0, 0, -2) : U(0, 0, 3));
-        T uzl = iz == 0 ? T(0) : U(0, 0, -1) + U0;
-        T uzll = U0 + (iz == 2 ? -U(0, 0, -2) : iz == 1 ? T(0) : iz == 0 ? U(0, 0, 2) : U(0, 0, -3));
+        T uzr = (!INT && iz == NZ - 1) ? T(0) : U0 + U(0, 0, 1);
+        T uzrr = U0 + ((!INT && iz == NZ - 3) ? -U(0, 0, 2) : (!INT && iz == NZ - 2) ? T(0) : (!INT && iz == NZ - 1) ? U(0, 0, -2) : U(0, 0, 3));
+        T uzl = (!INT && iz == 0) ? T(0) : U(0, 0, -1) + U0;
+        T uzll = U0 + ((!INT && iz == 2) ? -U(0, 0, -2) : (!INT && iz == 1) ? T(0) : (!INT && iz == 0) ? U(0, 0, 2) : U(0, 0, -3));
         s[0] += wzr * uzr - C27 * wbzr * uzrr - wzl * uzl + C27 * wbzl * uzll;
     }
     {  // v: x-faces
@@ -118,80 +121,80 @@ __device__ __forceinline__ void conv_vv4(const ACC& A, const StagZ<T>& m, T gcz,
     }
     {  // v: z-faces
         T wzl, wzr, wbzl, wbzr;
-        if (iz == 0) wzl = 0;
+        if ((!INT && iz == 0)) wzl = 0;
         else wzl = hxhy * (9 * (W0 + W(0, -1, 0)) - (W(0, -2, 0) + W(0, 1, 0)));
-        if (iz == NZ - 1) wzr = 0;
+        if ((!INT && iz == NZ - 1)) wzr = 0;
         else wzr = hxhy * (9 * (W(0, 0, 1) + W(0, -1, 1)) - (W(0, -2, 1) + W(0, 1, 1)));
-        if (iz == 1) wbzl = 0;
-        else if (iz == 0) wbzl = wzr;
+        if ((!INT && iz == 1)) wbzl = 0;
+        else if ((!INT && iz == 0)) wbzl = wzr;
         else wbzl = hxhy * (9 * (W(0, 0, -1) + W(0, -1, -1)) - (W(0, -2, -1) + W(0, 1, -1)));
-        if (iz == NZ - 2) wbzr = 0;
-        else if (iz == NZ - 1) wbzr = wzl;
+        if ((!INT && iz == NZ - 2)) wbzr = 0;
+        else if ((!INT && iz == NZ - 1)) wbzr = wzl;
         else wbzr = hxhy * (9 * (W(0, 0, 2) + W(0, -1, 2)) - (W(0, -2, 2) + W(0, 1, 2)));
-        T vzr = iz == NZ - 1 ? T(0) : V0 + V(0, 0, 1);
-        T vzrr = V0 + (iz == NZ - 3 ? -V(0, 0, 2) : iz == NZ - 2 ? T(0) : iz == NZ - 1 ? V(0, 0, -2) : V(0, 0, 3));
-        T vzl = iz == 0 ? T(0) : V(0, 0, -1) + V0;
-        T vzll = V0 + (iz == 2 ? -V(0, 0, -2) : iz == 1 ? T(0) : iz == 0 ? V(0, 0, 2) : V(0, 0, -3));
+        T vzr = (!INT && iz == NZ - 1) ? T(0) : V0 + V(0, 0, 1);
+        T vzrr = V0 + ((!INT && iz == NZ - 3) ? -V(0, 0, 2) : (!INT && iz == NZ - 2) ? T(0) : (!INT && iz == NZ - 1) ? V(0, 0, -2) : V(0, 0, 3));
+        T vzl = (!INT && iz == 0) ? T(0) : V(0, 0, -1) + V0;
+        T vzll = V0 + ((!INT && iz == 2) ? -V(0, 0, -2) : (!INT && iz == 1) ? T(0) : (!INT && iz == 0) ? V(0, 0, 2) : V(0, 0, -3));
         s[1] += wzr * vzr - C27 * wbzr * vzrr - wzl * vzl + C27 * wbzl * vzll;
     }
-    if (iz != 0) {
+    if ((INT || iz != 0)) {
         {  // w: x-faces, mass flux averaged to the w-face in z
             T br, bl, bbr, bbl;
             br = 9 * (U(1, 0, 0) * DZ[iz] + U(1, 0, -1) * DZ[iz - 1]);
-            br -= (iz == 1) ? -U(1, 0, -1) * DZ[0] : U(1, 0, -2) * DZ[iz - 2];
-            br -= (iz == NZ - 1) ? -U(1, 0, 0) * DZ[NZ - 1] : U(1, 0, 1) * DZ[iz + 1];
+            br -= ((!INT && iz == 1)) ? -U(1, 0, -1) * DZ[0] : U(1, 0, -2) * DZ[iz - 2];
+            br -= ((!INT && iz == NZ - 1)) ? -U(1, 0, 0) * DZ[NZ - 1] : U(1, 0, 1) * DZ[iz + 1];
             br *= hy;
             bl = 9 * (U0 * DZ[iz] + U(0, 0, -1) * DZ[iz - 1]);
-            bl -= (iz == 1) ? -U(0, 0, -1) * DZ[0] : U(0, 0, -2) * DZ[iz - 2];
-            bl -= (iz == NZ - 1) ? -U0 * DZ[NZ - 1] : U(0, 0, 1) * DZ[iz + 1];
+            bl -= ((!INT && iz == 1)) ? -U(0, 0, -1) * DZ[0] : U(0, 0, -2) * DZ[iz - 2];
+            bl -= ((!INT && iz == NZ - 1)) ? -U0 * DZ[NZ - 1] : U(0, 0, 1) * DZ[iz + 1];
             bl *= hy;
             bbr = 9 * (U(2, 0, 0) * DZW[iz] + U(2, 0, -1) * DZW[iz - 1]);
-            bbr -= (iz == 1) ? -U(2, 0, -1) * DZW[0] : U(2, 0, -2) * DZW[iz - 2];
-            bbr -= (iz == NZ - 1) ? -U(2, 0, 0) * DZW[NZ - 1] : U(2, 0, 1) * DZW[iz + 1];
+            bbr -= ((!INT && iz == 1)) ? -U(2, 0, -1) * DZW[0] : U(2, 0, -2) * DZW[iz - 2];
+            bbr -= ((!INT && iz == NZ - 1)) ? -U(2, 0, 0) * DZW[NZ - 1] : U(2, 0, 1) * DZW[iz + 1];
             bbr *= hy;
             bbl = 9 * (U(-1, 0, 0) * DZW[iz] + U(-1, 0, -1) * DZW[iz - 1]);
-            bbl -= (iz == 1) ? -U(-1, 0, -1) * DZW[0] : U(-1, 0, -2) * DZW[iz - 2];
-            bbl -= (iz == NZ - 1) ? -U(-1, 0, 0) * DZW[NZ - 1] : U(-1, 0, 1) * DZW[iz + 1];
+            bbl -= ((!INT && iz == 1)) ? -U(-1, 0, -1) * DZW[0] : U(-1, 0, -2) * DZW[iz - 2];
+            bbl -= ((!INT && iz == NZ - 1)) ? -U(-1, 0, 0) * DZW[NZ - 1] : U(-1, 0, 1) * DZW[iz + 1];
             bbl *= hy;
             s[2] += br * (W0 + W(1, 0, 0)) - C27 * bbr * (W0 + W(3, 0, 0)) - bl * (W(-1, 0, 0) + W0) + C27 * bbl * (W(-3, 0, 0) + W0);
         }
         {  // w: y-faces (scaled by hy as in staggered/func_global.h:475-487)
             T br, bl, bbr, bbl;
             br = 9 * (V(0, 1, 0) * DZ[iz] + V(0, 1, -1) * DZ[iz - 1]);
-            br -= (iz == 1) ? -V(0, 1, -1) * DZ[0] : V(0, 1, -2) * DZ[iz - 2];
-            br -= (iz == NZ - 1) ? -V(0, 1, 0) * DZ[NZ - 1] : V(0, 1, 1) * DZ[iz + 1];
+            br -= ((!INT && iz == 1)) ? -V(0, 1, -1) * DZ[0] : V(0, 1, -2) * DZ[iz - 2];
+            br -= ((!INT && iz == NZ - 1)) ? -V(0, 1, 0) * DZ[NZ - 1] : V(0, 1, 1) * DZ[iz + 1];
             br *= hy;
             bl = 9 * (V0 * DZ[iz] + V(0, 0, -1) * DZ[iz - 1]);
-            bl -= (iz == 1) ? -V(0, 0, -1) * DZ[0] : V(0, 0, -2) * DZ[iz - 2];
-            bl -= (iz == NZ - 1) ? -V0 * DZ[NZ - 1] : V(0, 0, 1) * DZ[iz + 1];
+            bl -= ((!INT && iz == 1)) ? -V(0, 0, -1) * DZ[0] : V(0, 0, -2) * DZ[iz - 2];
+            bl -= ((!INT && iz == NZ - 1)) ? -V0 * DZ[NZ - 1] : V(0, 0, 1) * DZ[iz + 1];
             bl *= hy;
             bbr = 9 * (V(0, 2, 0) * DZW[iz] + V(0, 2, -1) * DZW[iz - 1]);
-            bbr -= (iz == 1) ? -V(0, 2, -1) * DZW[0] : V(0, 2, -2) * DZW[iz - 2];
-            bbr -= (iz == NZ - 1) ? -V(0, 2, 0) * DZW[NZ - 1] : V(0, 2, 1) * DZW[iz + 1];
+            bbr -= ((!INT && iz == 1)) ? -V(0, 2, -1) * DZW[0] : V(0, 2, -2) * DZW[iz - 2];
+            bbr -= ((!INT && iz == NZ - 1)) ? -V(0, 2, 0) * DZW[NZ - 1] : V(0, 2, 1) * DZW[iz + 1];
             bbr *= hy;
             bbl = 9 * (V(0, -1, 0) * DZW[iz] + V(0, -1, -1) * DZW[iz - 1]);
-            bbl -= (iz == 1) ? -V(0, -1, -1) * DZW[0] : V(0, -1, -2) * DZW[iz - 2];
-            bbl -= (iz == NZ - 1) ? -V(0, -1, 0) * DZW[NZ - 1] : V(0, -1, 1) * DZW[iz + 1];
+            bbl -= ((!INT && iz == 1)) ? -V(0, -1, -1) * DZW[0] : V(0, -1, -2) * DZW[iz - 2];
+            bbl -= ((!INT && iz == NZ - 1)) ? -V(0, -1, 0) * DZW[NZ - 1] : V(0, -1, 1) * DZW[iz + 1];
             bbl *= hy;
             s[2] += br * (W0 + W(0, 1, 0)) - C27 * bbr * (W0 + W(0, 3, 0)) - bl * (W(0, -1, 0) + W0) + C27 * bbl * (W(0, -3, 0) + W0);
         }
         {  // w: z-faces
             T wzl = W(0, 0, -1);
-            T wzr = iz == NZ - 1 ? T(0) : W(0, 0, 1);
-            T wzll = iz == 1 ? W0 : W(0, 0, -2);
-            T wzrr = iz == NZ - 2 ? T(0) : iz == NZ - 1 ? W0 : W(0, 0, 2);
-            T wzlll = iz == 1 ? W(0, 0, 1) : iz == 2 ? W(0, 0, -1) : W(0, 0, -3);
-            T wzrrr = iz == NZ - 3 ? T(0) : iz == NZ - 2 ? W(0, 0, 1) : iz == NZ - 1 ? W(0, 0, -1) : W(0, 0, 3);
+            T wzr = (!INT && iz == NZ - 1) ? T(0) : W(0, 0, 1);
+            T wzll = (!INT && iz == 1) ? W0 : W(0, 0, -2);
+            T wzrr = (!INT && iz == NZ - 2) ? T(0) : (!INT && iz == NZ - 1) ? W0 : W(0, 0, 2);
+            T wzlll = (!INT && iz == 1) ? W(0, 0, 1) : (!INT && iz == 2) ? W(0, 0, -1) : W(0, 0, -3);
+            T wzrrr = (!INT && iz == NZ - 3) ? T(0) : (!INT && iz == NZ - 2) ? W(0, 0, 1) : (!INT && iz == NZ - 1) ? W(0, 0, -1) : W(0, 0, 3);
             T bl = hxhy * (9 * (wzl + W0) - (wzll + wzr));
             T br = hxhy * (9 * (W0 + wzr) - (wzl + wzrr));
             T bbl = hxhy * (9 * (wzll + wzl) - (wzlll + W0));
             T bbr = hxhy * (9 * (wzr + wzrr) - (W0 + wzrrr));
             s[2] += br * (W0 + wzr) - bl * (wzl + W0);
-            if (iz < NZ - 2) s[2] -= C27 * bbr * (W0 + wzrrr);
-            else if (iz == NZ - 2) s[2] -= C27 * bbr * (-W(0, 0, 1) + W0);
+            if ((INT || iz < NZ - 2)) s[2] -= C27 * bbr * (W0 + wzrrr);
+            else if ((!INT && iz == NZ - 2)) s[2] -= C27 * bbr * (-W(0, 0, 1) + W0);
             else s[2] -= C27 * bbr * (W(0, 0, -1) + W0);
-            if (iz > 2) s[2] += C27 * bbl * (wzlll + W0);
-            else if (iz == 2) s[2] += C27 * bbl * (-W(0, 0, -1) + W0);
+            if ((INT || iz > 2)) s[2] += C27 * bbl * (wzlll + W0);
+            else if ((!INT && iz == 2)) s[2] += C27 * bbl * (-W(0, 0, -1) + W0);
             else s[2] += C27 * bbl * (W(0, 0, 1) + W0);
         }
     }
@@ -201,12 +204,12 @@ __device__ __forceinline__ void conv_vv4(const ACC& A, const StagZ<T>& m, T gcz,
     s[2] *= (-T(1. / 32.) * m.ihx * m.ihy * gcz);
 }
 
-template <typename T, typename ACC>
+template <typename T, typename ACC, bool INT = false>
 __device__ __forceinline__ void visc_cross(const ACC& A, const StagZ<T>& m, T s[3]) {
     const int iz = m.iz, NZ = m.NZ;
     const T* DZ = m.DZ;
     const T inv_hz = T(1) / DZ[iz];
-    const T inv_hz_alt = T(2) / (DZ[iz] + (iz == 0 ? T(0) : DZ[iz - 1]));
+    const T inv_hz_alt = T(2) / (DZ[iz] + ((!INT && iz == 0) ? T(0) : DZ[iz - 1]));
 #pragma unroll
     for (int c = 0; c < 3; c++) {
         const T v0 = A(c, 0, 0, 0);
@@ -214,7 +217,7 @@ __device__ __forceinline__ void visc_cross(const ACC& A, const StagZ<T>& m, T s[
         s[c] += m.ihy * m.ihy * (A(c, 0, 1, 0) + A(c, 0, -1, 0) - T(2.) * v0);
     }
     const T U0 = U(0, 0, 0), V0 = V(0, 0, 0), W0 = W(0, 0, 0);
-    if (iz != NZ - 1) {
+    if ((INT || iz != NZ - 1)) {
         const T up = T(2) / (DZ[iz] + DZ[iz + 1]);
         s[0] += (U(0, 0, 1) - U0) * up * inv_hz;
         s[1] += (V(0, 0, 1) - V0) * up * inv_hz;
@@ -225,7 +228,7 @@ __device__ __forceinline__ void visc_cross(const ACC& A, const StagZ<T>& m, T s[
         s[1] += (-V0) * up * inv_hz;
         s[2] += (-W0) * inv_hz * inv_hz_alt;
     }
-    if (iz != 0) {
+    if ((INT || iz != 0)) {
         s[0] += (U(0, 0, -1) - U0) * inv_hz_alt * inv_hz;
         s[1] += (V(0, 0, -1) - V0) * inv_hz_alt * inv_hz;
         s[2] += (W(0, 0, -1) - W0) * (T(1) / DZ[iz - 1]) * inv_hz_alt;
@@ -239,13 +242,13 @@ __device__ __forceinline__ void visc_cross(const ACC& A, const StagZ<T>& m, T s[
 }
 
 // MUF(dx, dy, dz) returns visc + nu_t at the displaced cell (or visc for DNS).
-template <typename T, typename ACC, typename MUF>
+template <typename T, typename ACC, typename MUF, bool INT = false>
 __device__ __forceinline__ void visc_naive(const ACC& A, const MUF& MU, const StagZ<T>& m, T s[3]) {
     const int iz = m.iz, NZ = m.NZ;
     const T *DZ = m.DZ, ihx = m.ihx, ihy = m.ihy, visc = m.visc;
     const T inv_hz = T(1) / DZ[iz];
-    const T up = 2 / (DZ[iz] + (iz == NZ - 1 ? T(0) : DZ[iz + 1]));
-    const T dn = 2 / (DZ[iz] + (iz == 0 ? T(0) : DZ[iz - 1]));
+    const T up = 2 / (DZ[iz] + ((!INT && iz == NZ - 1) ? T(0) : DZ[iz + 1]));
+    const T dn = 2 / (DZ[iz] + ((!INT && iz == 0) ? T(0) : DZ[iz - 1]));
     const T U0 = U(0, 0, 0), V0 = V(0, 0, 0), W0 = W(0, 0, 0);
     const T q = T(0.25);
     const T mu0 = MU(0, 0, 0), muxl = MU(-1, 0, 0), muyl = MU(0, -1, 0);
@@ -256,9 +259,9 @@ __device__ __forceinline__ void visc_naive(const ACC& A, const MUF& MU, const St
     const T sxy910 = ((U(0, 1, 0) - U0) * ihy + (V(0, 1, 0) - V(-1, 1, 0)) * ihx) * q * (mu0 + muxl + MU(0, 1, 0) + MU(-1, 1, 0));
     const T sxy990 = ((U0 - U(0, -1, 0)) * ihy + (V0 - V(-1, 0, 0)) * ihx) * q * (muyl + MU(-1, -1, 0) + mu0 + muxl);
     s[0] += (sxy910 - sxy990) * ihy;
-    const T sxz901 = (iz == NZ - 1) ? (-2 * U0 * inv_hz * visc)
+    const T sxz901 = ((!INT && iz == NZ - 1)) ? (-2 * U0 * inv_hz * visc)
                                     : ((U(0, 0, 1) - U0) * up + (W(0, 0, 1) - W(-1, 0, 1)) * ihx) * q * (mu0 + muxl + MU(0, 0, 1) + MU(-1, 0, 1));
-    const T sxz909 = (iz == 0) ? (2 * U0 * inv_hz * visc)
+    const T sxz909 = ((!INT && iz == 0)) ? (2 * U0 * inv_hz * visc)
                                : ((U0 - U(0, 0, -1)) * dn + (W0 - W(-1, 0, 0)) * ihx) * q * (MU(0, 0, -1) + MU(-1, 0, -1) + mu0 + muxl);
     s[0] += (sxz901 - sxz909) * inv_hz;
 
@@ -267,18 +270,18 @@ __device__ __forceinline__ void visc_naive(const ACC& A, const MUF& MU, const St
     const T syy000 = 2 * (V(0, 1, 0) - V0) * ihy * mu0;
     const T syy080 = 2 * (V0 - V(0, -1, 0)) * ihy * muyl;
     s[1] += (syy000 - syy080) * ihy;
-    const T syz091 = (iz == NZ - 1) ? (-2 * V0 * inv_hz * visc)
+    const T syz091 = ((!INT && iz == NZ - 1)) ? (-2 * V0 * inv_hz * visc)
                                     : ((V(0, 0, 1) - V0) * up + (W(0, 0, 1) - W(0, -1, 1)) * ihy) * q * (mu0 + muyl + MU(0, 0, 1) + MU(0, -1, 1));
-    const T syz099 = (iz == 0) ? (2 * V0 * inv_hz * visc)
+    const T syz099 = ((!INT && iz == 0)) ? (2 * V0 * inv_hz * visc)
                                : ((V0 - V(0, 0, -1)) * dn + (W0 - W(0, -1, 0)) * ihy) * q * (MU(0, 0, -1) + MU(0, -1, -1) + mu0 + muyl);
     s[1] += (syz091 - syz099) * inv_hz;
 
-    if (iz == 0) return;
+    if ((!INT && iz == 0)) return;
     const T sxz109 = ((U(1, 0, 0) - U(1, 0, -1)) * dn + (W(1, 0, 0) - W0) * ihx) * q * (MU(0, 0, -1) + MU(1, 0, -1) + mu0 + MU(1, 0, 0));
     s[2] += (sxz109 - sxz909) * ihx;
     const T syz019 = ((V(0, 1, 0) - V(0, 1, -1)) * dn + (W(0, 1, 0) - W0) * ihy) * q * (MU(0, 0, -1) + MU(0, 1, -1) + mu0 + MU(0, 1, 0));
     s[2] += (syz019 - syz099) * ihy;
-    const T szz000 = 2 * ((iz == NZ - 1 ? T(0) : W(0, 0, 1)) - W0) * inv_hz * mu0;
+    const T szz000 = 2 * (((!INT && iz == NZ - 1) ? T(0) : W(0, 0, 1)) - W0) * inv_hz * mu0;
     const T szz008 = 2 * (W0 - W(0, 0, -1)) * MU(0, 0, -1) / DZ[iz - 1];
     s[2] += (szz000 - szz008) * dn;
 }

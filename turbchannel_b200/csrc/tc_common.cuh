@@ -206,4 +206,101 @@ __device__ cplx<T>* fft_lines(cplx<T>* A, cplx<T>* B, int nl, int ls, const FftP
     return A;
 }
 
+// ---------------------------------------------------------------------------
+// The same transform with the length known at compile time: the radix sequence,
+// strides and every index division fold into constants.  fft_lines_any picks
+// the compiled length or falls back to the runtime plan.
+// ---------------------------------------------------------------------------
+template <int N>
+struct FftFac {
+    static constexpr int count() {
+        int m = N, c = 0;
+        while (m % 4 == 0) { m /= 4; c++; }
+        while (m % 2 == 0) { m /= 2; c++; }
+        while (m % 3 == 0) { m /= 3; c++; }
+        return c;
+    }
+    static constexpr int radix(int i) {
+        int m = N, c = 0;
+        while (m % 4 == 0) { if (c == i) return 4; m /= 4; c++; }
+        while (m % 2 == 0) { if (c == i) return 2; m /= 2; c++; }
+        while (m % 3 == 0) { if (c == i) return 3; m /= 3; c++; }
+        return 1;
+    }
+    static constexpr int ns(int i) {
+        int n = 1;
+        for (int k = 0; k < i; k++) n *= radix(k);
+        return n;
+    }
+};
+
+template <typename T, int N, int R, int Ns>
+__device__ __forceinline__ void fft_pass_c(const cplx<T>* in, cplx<T>* out, int nl, int ls,
+                                           const cplx<T>* __restrict__ tw, int sign) {
+    constexpr int nR = N / R, step = N / (Ns * R);
+    const int total = nl * nR;
+    for (int b = threadIdx.x; b < total; b += blockDim.x) {
+        const int l = b / nR, j = b - l * nR;
+        const int k = j % Ns;
+        const cplx<T>* src = in + l * ls;
+        cplx<T>* dst = out + l * ls;
+        cplx<T> v[R];
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            cplx<T> a = src[j + r * nR];
+            if (r > 0 && Ns > 1) {
+                cplx<T> w = tw[r * k * step];
+                if (sign > 0) w.y = -w.y;
+                a = cmul(a, w);
+            }
+            v[r] = a;
+        }
+        dft_small<T, R>(v, sign);
+        const int d = (j / Ns) * Ns * R + k;
+#pragma unroll
+        for (int r = 0; r < R; r++) dst[d + r * Ns] = v[r];
+    }
+}
+
+template <typename T, int N, int F>
+__device__ __forceinline__ void fft_passes_c(cplx<T>*& A, cplx<T>*& B, int nl, int ls, const cplx<T>* tw, int sign) {
+    if constexpr (F < FftFac<N>::count()) {
+        constexpr int R = FftFac<N>::radix(F), Ns = FftFac<N>::ns(F);
+        __syncthreads();
+        fft_pass_c<T, N, R, Ns>(A, B, nl, ls, tw, sign);
+        cplx<T>* s = A;
+        A = B;
+        B = s;
+        fft_passes_c<T, N, F + 1>(A, B, nl, ls, tw, sign);
+    }
+}
+
+template <typename T, int N>
+__device__ __forceinline__ cplx<T>* fft_lines_n(cplx<T>* A, cplx<T>* B, int nl, int ls, const cplx<T>* tw, int sign) {
+    fft_passes_c<T, N, 0>(A, B, nl, ls, tw, sign);
+    __syncthreads();
+    return A;
+}
+
+template <typename T>
+__device__ cplx<T>* fft_lines_any(cplx<T>* A, cplx<T>* B, int nl, int ls, const FftPlan& P, const cplx<T>* tw,
+                                  int sign) {
+    switch (P.n) {
+        case 16: return fft_lines_n<T, 16>(A, B, nl, ls, tw, sign);
+        case 24: return fft_lines_n<T, 24>(A, B, nl, ls, tw, sign);
+        case 32: return fft_lines_n<T, 32>(A, B, nl, ls, tw, sign);
+        case 48: return fft_lines_n<T, 48>(A, B, nl, ls, tw, sign);
+        case 64: return fft_lines_n<T, 64>(A, B, nl, ls, tw, sign);
+        case 96: return fft_lines_n<T, 96>(A, B, nl, ls, tw, sign);
+        case 128: return fft_lines_n<T, 128>(A, B, nl, ls, tw, sign);
+        case 192: return fft_lines_n<T, 192>(A, B, nl, ls, tw, sign);
+        case 256: return fft_lines_n<T, 256>(A, B, nl, ls, tw, sign);
+        case 384: return fft_lines_n<T, 384>(A, B, nl, ls, tw, sign);
+        case 512: return fft_lines_n<T, 512>(A, B, nl, ls, tw, sign);
+        case 768: return fft_lines_n<T, 768>(A, B, nl, ls, tw, sign);
+        case 1024: return fft_lines_n<T, 1024>(A, B, nl, ls, tw, sign);
+        default: return fft_lines(A, B, nl, ls, P, tw, sign);
+    }
+}
+
 }  // namespace tc
