@@ -16,54 +16,66 @@
 
 namespace tc {
 
-constexpr int STX = 32, STY = 8;
-constexpr int SG = 4;  // x-halo of the shared tile: a multiple of the 16-byte chunk for float and double
+constexpr int STX = 32, STY = 8;  // threads per CTA: 32 x 8
+constexpr int SG = 4;              // x-halo of the shared tile (a whole 16-byte chunk for float and double)
 
-template <typename T, int H>
+// CY: cells per thread along y (the tile is 32 x 8*CY cells).
+template <typename T, int H, int CY>
 struct RingAcc {
-    static constexpr int PW = STX + 2 * SG, PH = STY + 2 * H, PL = PW * PH, RS = 2 * H + 2;
+    static constexpr int PW = STX + 2 * SG, PH = STY * CY + 2 * H, PL = PW * PH, RS = 2 * H + 2;
     const T* ring;
-    int zs, tx, ty;
+    int zs, tx, ty;  // ty: cell row inside the tile
     __device__ __forceinline__ T operator()(int c, int dx, int dy, int dz) const {
         const int slot = (zs + dz) & (RS - 1);
         return ring[((slot * 3 + c) * PH + ty + H + dy) * PW + tx + SG + dx];
     }
 };
 
-// One plane of the tile plus halo (3 components) into ring slot z & (RS-1).
-// VEC: 16-byte LDGSTS per chunk (the x-halo is chunk aligned, so periodic wrap is a
-// whole-chunk shift); otherwise element-wise copies.
-template <typename T, int H, bool VEC>
-__device__ __forceinline__ void load_plane(T* ring, const T* const* vel, int z, int x0, int y0, int NX, int NY,
-                                           size_t NXY) {
-    using ACC = RingAcc<T, H>;
-    constexpr int PW = ACC::PW, PH = ACC::PH, PL = ACC::PL, RS = ACC::RS;
-    T* dst = ring + (z & (RS - 1)) * 3 * PL;
-    if (VEC) {
-        constexpr int CH = 16 / sizeof(T), NCH = PW / CH, PER = PH * NCH;
-        for (int e = threadIdx.x; e < 3 * PER; e += blockDim.x) {
-            const int c = e / PER, r = e - c * PER, py = r / NCH, ch = r - py * NCH;
-            const int gy = wrapi(y0 - H + py, NY), gx = wrapi(x0 - SG + ch * CH, NX);
-            cp_async<16>(dst + c * PL + py * PW + ch * CH, vel[c] + (size_t)z * NXY + (size_t)gy * NX + gx);
-        }
-    } else {
-        for (int e = threadIdx.x; e < 3 * PL; e += blockDim.x) {
-            const int c = e / PL, r = e - c * PL, py = r / PW, px = r - py * PW;
-            const int gx = wrapi(x0 - SG + px, NX), gy = wrapi(y0 - H + py, NY);
-            cp_async<sizeof(T)>(dst + e, vel[c] + (size_t)z * NXY + (size_t)gy * NX + gx);
+// Plane-invariant part of this thread's share of the tile copy: for chunk k, the
+// shared-memory offset inside a ring slot and the global element offset without
+// the z term.  VEC: 16-byte chunks (the x-halo is chunk aligned, so the periodic
+// wrap moves whole chunks); otherwise single elements.
+template <typename T, int H, int CY, bool VEC>
+struct TileCopy {
+    using ACC = RingAcc<T, H, CY>;
+    static constexpr int CH = VEC ? 16 / sizeof(T) : 1, NCH = ACC::PW / CH, PER = ACC::PH * NCH;
+    static constexpr int TOTAL = 3 * PER, NK = (TOTAL + STX * STY - 1) / (STX * STY);
+    int sofs[NK];
+    unsigned gofs[NK];  // < 2^32: checked on the host (3 N elements)
+    __device__ __forceinline__ void init(int x0, int y0, int NX, int NY, long long N) {
+#pragma unroll
+        for (int k = 0; k < NK; k++) {
+            const int e = threadIdx.x + k * STX * STY;
+            if (e < TOTAL) {
+                const int c = e / PER, r = e - c * PER, py = r / NCH, ch = r - py * NCH;
+                const int gy = wrapi(y0 - H + py, NY), gx = wrapi(x0 - SG + ch * CH, NX);
+                sofs[k] = c * ACC::PL + py * ACC::PW + ch * CH;
+                gofs[k] = (unsigned)((long long)c * N + (long long)gy * NX + gx);
+            } else {
+                sofs[k] = -1;
+                gofs[k] = 0;
+            }
         }
     }
-}
+    __device__ __forceinline__ void load(T* ring, const T* base, int z, size_t NXY) const {
+        T* dst = ring + (z & (ACC::RS - 1)) * 3 * ACC::PL;
+        const T* src = base + (size_t)z * NXY;
+#pragma unroll
+        for (int k = 0; k < NK; k++)
+            if (sofs[k] >= 0) cp_async<CH * sizeof(T)>(dst + sofs[k], src + gofs[k]);
+    }
+};
 
-template <typename T, int SCHEME, int VISC, bool LES, bool INT>
-__device__ __forceinline__ void flux_cell(const RingAcc<T, SCHEME == TC_SCHEME_VV4 ? 3 : 1>& A, const StagZ<T>& mz,
+template <typename T, int SCHEME, int VISC, bool LES, bool INT, int CY>
+__device__ __forceinline__ void flux_cell(const RingAcc<T, SCHEME == TC_SCHEME_VV4 ? 3 : 1, CY>& A, const StagZ<T>& mz,
                                           T gcz, const FluxArgs<T>& a, int ix, int iy, int xm, int xp, int ym,
                                           int yp, size_t NXY, T f[3]) {
+    using ACC = RingAcc<T, SCHEME == TC_SCHEME_VV4 ? 3 : 1, CY>;
     T cf[3], vf[3];
-    if constexpr (SCHEME == TC_SCHEME_VV4) conv_vv4<T, RingAcc<T, 3>, INT>(A, mz, gcz, cf);
-    else conv_hw2<T, RingAcc<T, 1>, INT>(A, mz, cf);
+    if constexpr (SCHEME == TC_SCHEME_VV4) conv_vv4<T, ACC, INT>(A, mz, gcz, cf);
+    else conv_hw2<T, ACC, INT>(A, mz, cf);
     if constexpr (VISC == TC_VISC_CROSS) {
-        visc_cross<T, RingAcc<T, SCHEME == TC_SCHEME_VV4 ? 3 : 1>, INT>(A, mz, vf);
+        visc_cross<T, ACC, INT>(A, mz, vf);
     } else {
         const T* nt = a.nu_t;
         const int z = mz.iz;
@@ -74,17 +86,17 @@ __device__ __forceinline__ void flux_cell(const RingAcc<T, SCHEME == TC_SCHEME_V
             const int yy = dy < 0 ? ym : (dy > 0 ? yp : iy);
             return visc + __ldg(nt + (size_t)(z + dz) * NXY + (size_t)yy * a.g.NX + xx);
         };
-        visc_naive<T, RingAcc<T, SCHEME == TC_SCHEME_VV4 ? 3 : 1>, decltype(MU), INT>(A, MU, mz, vf);
+        visc_naive<T, ACC, decltype(MU), INT>(A, MU, mz, vf);
     }
     f[0] = ((T)a.g.sour_dpdx + cf[0]) + vf[0];
     f[1] = (T(0) + cf[1]) + vf[1];
     f[2] = (T(0) + cf[2]) + vf[2];
 }
 
-template <typename T, int SCHEME, int VISC, bool LES, int ORDER, bool VEC>
+template <typename T, int SCHEME, int VISC, bool LES, int ORDER, bool VEC, int CY>
 __global__ void __launch_bounds__(STX* STY, 2) k_flux_stag(FluxArgs<T> a, int tz) {
     constexpr int H = SCHEME == TC_SCHEME_VV4 ? 3 : 1;
-    using ACC = RingAcc<T, H>;
+    using ACC = RingAcc<T, H, CY>;
     constexpr int RS = ACC::RS;
     extern __shared__ __align__(16) unsigned char smraw[];
     T* ring = reinterpret_cast<T*>(smraw);
@@ -93,15 +105,17 @@ __global__ void __launch_bounds__(STX* STY, 2) k_flux_stag(FluxArgs<T> a, int tz
     const Geom& g = a.g;
     const int NX = g.NX, NY = g.NY, NZ = g.NZ;
     const size_t NXY = (size_t)NX * NY;
-    const int tx = threadIdx.x % STX, ty = threadIdx.x / STX;
-    const int x0 = blockIdx.x * STX, y0 = blockIdx.y * STY;
+    const int tx = threadIdx.x % STX, tyt = threadIdx.x / STX;
+    const int x0 = blockIdx.x * STX, y0 = blockIdx.y * (STY * CY);
     const int zb = blockIdx.z * tz, ze = min(NZ, zb + tz);
-    const int ix = x0 + tx, iy = y0 + ty;
-    const bool active = ix < NX && iy < NY;
+    const int ix = x0 + tx;
     // interior planes: no wall special case of the scheme applies
     const int zlo = SCHEME == TC_SCHEME_VV4 ? 3 : 1, zhi = SCHEME == TC_SCHEME_VV4 ? NZ - 4 : NZ - 2;
 
-    for (int z = max(0, zb - H); z <= min(NZ - 1, zb + H); z++) load_plane<T, H, VEC>(ring, a.vel.c, z, x0, y0, NX, NY, NXY);
+    TileCopy<T, H, CY, VEC> cp;
+    cp.init(x0, y0, NX, NY, g.N);
+    const T* vbase = a.vel.c[0];  // the three components are consecutive blocks of N
+    for (int z = max(0, zb - H); z <= min(NZ - 1, zb + H); z++) cp.load(ring, vbase, z, NXY);
     cp_async_commit();
 
     StagZ<T> mz;
@@ -114,37 +128,48 @@ __global__ void __launch_bounds__(STX* STY, 2) k_flux_stag(FluxArgs<T> a, int tz
     mz.ihy = (T)g.inv_hy;
     mz.visc = (T)g.visc;
     const int xm = wrapi(ix - 1, NX), xp = wrapi(ix + 1, NX);
-    const int ym = wrapi(iy - 1, NY), yp = wrapi(iy + 1, NY);
     const T inv_tau = a.inv_tau;
     double ub = 0.0;
 
     for (int z = zb; z < ze; z++) {
-        if (z + 1 < ze && z + H + 1 < NZ) load_plane<T, H, VEC>(ring, a.vel.c, z + H + 1, x0, y0, NX, NY, NXY);
+        if (z + 1 < ze && z + H + 1 < NZ) cp.load(ring, vbase, z + H + 1, NXY);
         cp_async_commit();
-        const size_t id = (size_t)z * NXY + (size_t)iy * NX + ix;
-        // history of this cell, issued before the stencil so its latency overlaps it
-        T hp[3], hq[3], vp[3], vq[3];
-        if (ORDER >= 2 && active) {
+        // history of this thread's cells, issued before the stencil so its latency overlaps it
+        T hp[CY][3], hq[CY][3], vp[CY][3], vq[CY][3];
+        if (ORDER >= 2) {
 #pragma unroll
-            for (int c = 0; c < 3; c++) {
-                hp[c] = __ldg(a.fp.c[c] + id);
-                vp[c] = __ldg(a.velp.c[c] + id);
-                if (ORDER == 3) {
-                    hq[c] = __ldg(a.fq.c[c] + id);
-                    vq[c] = __ldg(a.velq.c[c] + id);
+            for (int q = 0; q < CY; q++) {
+                const int iy = y0 + tyt * CY + q;
+                if (ix < NX && iy < NY) {
+                    const size_t id = (size_t)z * NXY + (size_t)iy * NX + ix;
+#pragma unroll
+                    for (int c = 0; c < 3; c++) {
+                        hp[q][c] = __ldg(a.fp.c[c] + id);
+                        vp[q][c] = __ldg(a.velp.c[c] + id);
+                        if (ORDER == 3) {
+                            hq[q][c] = __ldg(a.fq.c[c] + id);
+                            vq[q][c] = __ldg(a.velq.c[c] + id);
+                        }
+                    }
                 }
             }
         }
         cp_async_wait<1>();
         __syncthreads();
-        if (active) {
-            mz.iz = z;
+        mz.iz = z;
+        const T gcz = SCHEME == TC_SCHEME_VV4 ? a.m.GCZ[z] : T(0);
+        const bool inner = z >= zlo && z <= zhi;
+#pragma unroll
+        for (int q = 0; q < CY; q++) {
+            const int ty = tyt * CY + q, iy = y0 + ty;
+            if (ix >= NX || iy >= NY) continue;
+            const int ym = wrapi(iy - 1, NY), yp = wrapi(iy + 1, NY);
             const ACC A{ring, z & (RS - 1), tx, ty};
-            const T gcz = SCHEME == TC_SCHEME_VV4 ? a.m.GCZ[z] : T(0);
             T f[3];
-            if (z >= zlo && z <= zhi) flux_cell<T, SCHEME, VISC, LES, true>(A, mz, gcz, a, ix, iy, xm, xp, ym, yp, NXY, f);
-            else flux_cell<T, SCHEME, VISC, LES, false>(A, mz, gcz, a, ix, iy, xm, xp, ym, yp, NXY, f);
+            if (inner) flux_cell<T, SCHEME, VISC, LES, true, CY>(A, mz, gcz, a, ix, iy, xm, xp, ym, yp, NXY, f);
+            else flux_cell<T, SCHEME, VISC, LES, false, CY>(A, mz, gcz, a, ix, iy, xm, xp, ym, yp, NXY, f);
             if (z == 0) f[2] = 0;
+            const size_t id = (size_t)z * NXY + (size_t)iy * NX + ix;
 #pragma unroll
             for (int c = 0; c < 3; c++) a.fout.c[c][id] = f[c];
             if (ORDER > 0) {
@@ -153,10 +178,10 @@ __global__ void __launch_bounds__(STX* STY, 2) k_flux_stag(FluxArgs<T> a, int tz
                 for (int c = 0; c < 3; c++) {
                     const T vn = A(c, 0, 0, 0);
                     if (ORDER == 1) r[c] = f[c] + inv_tau * vn;
-                    else if (ORDER == 2) r[c] = (T(2.) * f[c] - hp[c]) + inv_tau * (2 * vn - T(0.5) * vp[c]);
+                    else if (ORDER == 2) r[c] = (T(2.) * f[c] - hp[q][c]) + inv_tau * (2 * vn - T(0.5) * vp[q][c]);
                     else
-                        r[c] = ((3 * f[c] - 3 * hp[c]) + hq[c]) +
-                               inv_tau * ((3 * vn - T(1.5) * vp[c]) + T(0.33333333333333333333) * vq[c]);
+                        r[c] = ((3 * f[c] - 3 * hp[q][c]) + hq[q][c]) +
+                               inv_tau * ((3 * vn - T(1.5) * vp[q][c]) + T(0.33333333333333333333) * vq[q][c]);
                     a.rhs.c[c][id] = r[c];
                 }
                 ub += (double)r[0] * (double)a.m.DZ[z];
@@ -170,30 +195,39 @@ __global__ void __launch_bounds__(STX* STY, 2) k_flux_stag(FluxArgs<T> a, int tz
     }
 }
 
-static void flux_stag_shape(const Geom& g, dim3& grid, int& tz) {
-    const int tiles = ((g.NX + STX - 1) / STX) * ((g.NY + STY - 1) / STY);
+// cells per thread along y: two for float (more reuse per shared-memory load),
+// one for double (register budget of 2 CTAs/SM)
+template <typename T>
+constexpr int flux_cy() { return sizeof(T) == 4 ? 2 : 1; }
+
+static void flux_stag_shape(const Geom& g, int cy, dim3& grid, int& tz) {
+    const int ty = STY * cy;
+    const int tiles = ((g.NX + STX - 1) / STX) * ((g.NY + ty - 1) / ty);
     int nch = std::max(1, (148 * 8 + tiles - 1) / tiles);
     tz = std::max(4, (g.NZ + nch - 1) / nch);
-    grid = dim3((g.NX + STX - 1) / STX, (g.NY + STY - 1) / STY, (g.NZ + tz - 1) / tz);
+    grid = dim3((g.NX + STX - 1) / STX, (g.NY + ty - 1) / ty, (g.NZ + tz - 1) / tz);
 }
 
+// upper bound of the flux kernels' grid sizes (sizes the partial-sum buffer)
 int flux_grid_blocks(const Geom& g) {
     dim3 gr;
     int tz;
-    flux_stag_shape(g, gr, tz);
+    flux_stag_shape(g, 1, gr, tz);
     return (int)(gr.x * gr.y * gr.z);
 }
 
 template <typename T, int SCHEME, int VISC, bool LES, int ORDER>
 static void run(const FluxArgs<T>& a, cudaStream_t s) {
     constexpr int H = SCHEME == TC_SCHEME_VV4 ? 3 : 1;
-    constexpr size_t smem = sizeof(T) * (2 * H + 2) * 3 * RingAcc<T, H>::PL;
+    constexpr int CY = flux_cy<T>();
+    constexpr size_t smem = sizeof(T) * (2 * H + 2) * 3 * RingAcc<T, H, CY>::PL;
     const bool vec = a.g.NX % (16 / (int)sizeof(T)) == 0;
-    auto kern = vec ? k_flux_stag<T, SCHEME, VISC, LES, ORDER, true> : k_flux_stag<T, SCHEME, VISC, LES, ORDER, false>;
+    auto kern = vec ? k_flux_stag<T, SCHEME, VISC, LES, ORDER, true, CY>
+                    : k_flux_stag<T, SCHEME, VISC, LES, ORDER, false, CY>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     dim3 grid;
     int tz;
-    flux_stag_shape(a.g, grid, tz);
+    flux_stag_shape(a.g, CY, grid, tz);
     kern<<<grid, STX * STY, smem, s>>>(a, tz);
 }
 

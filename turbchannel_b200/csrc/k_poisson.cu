@@ -28,8 +28,9 @@ namespace tc {
 // ---------------------------------------------------------------------------
 // divergence + forward x-FFT
 // ---------------------------------------------------------------------------
-template <typename T, int SCHEME, bool SCALAR>
-__global__ void __launch_bounds__(256) k_div_xfft(DivFftArgs<T> a, int rows) {
+template <typename T, int SCHEME, bool SCALAR, int ROWS>
+__global__ void __launch_bounds__(256) k_div_xfft(DivFftArgs<T> a) {
+    constexpr int rows = ROWS;
     extern __shared__ __align__(16) unsigned char smraw[];
     const Geom& g = a.g;
     const int NX = g.NX, NY = g.NY, NXH = g.NXH;
@@ -66,9 +67,9 @@ void launch_div_xfft(const DivFftArgs<T>& a, cudaStream_t s) {
     dim3 grid(a.g.NY / rows, a.g.NZ);
 #define TC_LDX(SCH, SC)                                                                                 \
     {                                                                                                   \
-        auto k = k_div_xfft<T, SCH, SC>;                                                                \
+        auto k = rows == 8 ? k_div_xfft<T, SCH, SC, 8> : rows == 4 ? k_div_xfft<T, SCH, SC, 4> : k_div_xfft<T, SCH, SC, 2>; \
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);               \
-        k<<<grid, 256, smem, s>>>(a, rows);                                                             \
+        k<<<grid, 256, smem, s>>>(a);                                                                   \
     }
     if (a.src_scalar) TC_LDX(TC_SCHEME_HW2, true)
     else if (a.g.scheme == TC_SCHEME_HW2) TC_LDX(TC_SCHEME_HW2, false)
@@ -90,9 +91,16 @@ __global__ void __launch_bounds__(256) k_yfft(YFftArgs<T> a, int lines) {
     cplx<T>* A = reinterpret_cast<cplx<T>*>(smraw);
     cplx<T>* B = A + lines * NY;
     cplx<T>* src = a.spec + L0 * NY;
-    for (int e = threadIdx.x; e < nl * NY; e += blockDim.x) A[e] = src[e];
+    // nl*NY complex values, contiguous and 16-byte aligned (NY even)
+    constexpr int PC = 16 / sizeof(cplx<T>);  // complex values per 16-byte chunk
+    const int nch = nl * NY / PC;
+    for (int e = threadIdx.x; e < nch; e += blockDim.x) cp_async<16>(A + e * PC, src + e * PC);
+    cp_async_commit();
+    cp_async_wait<0>();
     const cplx<T>* R = fft_lines_any(A, B, nl, NY, a.py, a.twy, a.sign);
-    for (int e = threadIdx.x; e < nl * NY; e += blockDim.x) src[e] = R[e];
+    const int4* r4 = reinterpret_cast<const int4*>(R);
+    int4* d4 = reinterpret_cast<int4*>(src);
+    for (int e = threadIdx.x; e < nch; e += blockDim.x) d4[e] = r4[e];
 }
 
 template <typename T>
@@ -429,7 +437,7 @@ size_t zsolve_scratch_bytes(const Geom& g, int elem_bytes) {
 }
 
 template <typename T, int SCHEME>
-static void zsolve_scheme(const ZSolveArgs<T>& a, cudaStream_t s) {
+static void zsolve_scheme(const ZSolveArgs<T>& a, cudaStream_t s, cudaStream_t side, cudaEvent_t fork, cudaEvent_t join) {
     const size_t M = (size_t)a.g.NXH * a.g.NY;
     if (sizeof(T) == sizeof(double)) {
         k_zsolve_all<double, T, SCHEME><<<(unsigned)((M + 63) / 64), 64, 0, s>>>(a, 0);
@@ -438,29 +446,36 @@ static void zsolve_scheme(const ZSolveArgs<T>& a, cudaStream_t s) {
         // launches share the scratch buffer, which is sized for double entries; the
         // float kernel indexes it as float (so the low-set double entries are disjoint
         // only in time: the launches are stream-ordered).
-        k_zsolve_all<float, T, SCHEME><<<(unsigned)((M + 63) / 64), 64, 0, s>>>(a, 1);
+        // the low modes (double, few and sequential) run on a side stream next to the
+        // float modes; the two sets are disjoint
+        cudaEventRecord(fork, s);
+        cudaStreamWaitEvent(side, fork, 0);
         const int nlow = a.g.low_modes * (2 * a.g.low_modes - 1);
         const int nc = SCHEME == TC_SCHEME_VV4 ? 3 : 1;
         const int nma = SCHEME == TC_SCHEME_VV4 ? 3 * a.g.NZ : a.g.NZ;
         const size_t smem = (size_t)a.g.NZ * (sizeof(cplx<double>) + nc * sizeof(double)) + (size_t)(nma + 2 * a.g.NZ) * sizeof(double);
         auto k = k_zsolve_low<T, SCHEME>;
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k<<<nlow, 128, smem, s>>>(a);
+        k<<<nlow, 128, smem, side>>>(a);
+        cudaEventRecord(join, side);
+        k_zsolve_all<float, T, SCHEME><<<(unsigned)((M + 63) / 64), 64, 0, s>>>(a, 1);
+        cudaStreamWaitEvent(s, join, 0);
     }
 }
 
 template <typename T>
-void launch_zsolve(const ZSolveArgs<T>& a, cudaStream_t s) {
-    if (a.g.scheme == TC_SCHEME_VV4) zsolve_scheme<T, TC_SCHEME_VV4>(a, s);
-    else if (a.g.scheme == TC_SCHEME_HW2) zsolve_scheme<T, TC_SCHEME_HW2>(a, s);
-    else zsolve_scheme<T, TC_SCHEME_COLLOC>(a, s);
+void launch_zsolve(const ZSolveArgs<T>& a, cudaStream_t s, cudaStream_t side, cudaEvent_t fork, cudaEvent_t join) {
+    if (a.g.scheme == TC_SCHEME_VV4) zsolve_scheme<T, TC_SCHEME_VV4>(a, s, side, fork, join);
+    else if (a.g.scheme == TC_SCHEME_HW2) zsolve_scheme<T, TC_SCHEME_HW2>(a, s, side, fork, join);
+    else zsolve_scheme<T, TC_SCHEME_COLLOC>(a, s, side, fork, join);
 }
 
 // ---------------------------------------------------------------------------
 // inverse x-FFT (complex-to-real, two rows per complex FFT) and scaling
 // ---------------------------------------------------------------------------
-template <typename T>
-__global__ void __launch_bounds__(256) k_ixfft(IxFftArgs<T> a, int rows) {
+template <typename T, int ROWS>
+__global__ void __launch_bounds__(256) k_ixfft(IxFftArgs<T> a) {
+    constexpr int rows = ROWS;
     extern __shared__ __align__(16) unsigned char smraw[];
     const Geom& g = a.g;
     const int NX = g.NX, NY = g.NY, NXH = g.NXH;
@@ -473,7 +488,7 @@ __global__ void __launch_bounds__(256) k_ixfft(IxFftArgs<T> a, int rows) {
         const int kx = e / rows, r = e - kx * rows;
         tile[r * NXH + kx] = a.spec[((size_t)z * NXH + kx) * NY + y0 + r];
     }
-    __syncthreads();
+    __syncthreads();  // (row-major tile: rows x NXH)
     const int nh = NX / 2;
     for (int e = threadIdx.x; e < nl * NX; e += blockDim.x) {
         const int l = e / NX, k = e - l * NX;
@@ -508,17 +523,17 @@ void launch_ixfft(const IxFftArgs<T>& a, cudaStream_t s) {
     const int rows = pick_rows(a.g.NX, a.g.NY, sizeof(cplx<T>));
     const size_t nl = rows / 2;
     const size_t smem = (nl * a.g.NX + std::max(nl * a.g.NX, (size_t)rows * a.g.NXH)) * sizeof(cplx<T>);
-    auto k = k_ixfft<T>;
+    auto k = rows == 8 ? k_ixfft<T, 8> : rows == 4 ? k_ixfft<T, 4> : k_ixfft<T, 2>;
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k<<<dim3(a.g.NY / rows, a.g.NZ), 256, smem, s>>>(a, rows);
+    k<<<dim3(a.g.NY / rows, a.g.NZ), 256, smem, s>>>(a);
 }
 
 template void launch_div_xfft<double>(const DivFftArgs<double>&, cudaStream_t);
 template void launch_div_xfft<float>(const DivFftArgs<float>&, cudaStream_t);
 template void launch_yfft<double>(const YFftArgs<double>&, cudaStream_t);
 template void launch_yfft<float>(const YFftArgs<float>&, cudaStream_t);
-template void launch_zsolve<double>(const ZSolveArgs<double>&, cudaStream_t);
-template void launch_zsolve<float>(const ZSolveArgs<float>&, cudaStream_t);
+template void launch_zsolve<double>(const ZSolveArgs<double>&, cudaStream_t, cudaStream_t, cudaEvent_t, cudaEvent_t);
+template void launch_zsolve<float>(const ZSolveArgs<float>&, cudaStream_t, cudaStream_t, cudaEvent_t, cudaEvent_t);
 template void launch_ixfft<double>(const IxFftArgs<double>&, cudaStream_t);
 template void launch_ixfft<float>(const IxFftArgs<float>&, cudaStream_t);
 

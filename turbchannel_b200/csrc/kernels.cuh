@@ -137,7 +137,8 @@ template <typename T> void launch_flux_stag(const FluxArgs<T>& a, cudaStream_t s
 template <typename T> void launch_flux_coll(const FluxArgs<T>& a, cudaStream_t s);
 template <typename T> void launch_div_xfft(const DivFftArgs<T>& a, cudaStream_t s);
 template <typename T> void launch_yfft(const YFftArgs<T>& a, cudaStream_t s);
-template <typename T> void launch_zsolve(const ZSolveArgs<T>& a, cudaStream_t s);
+template <typename T> void launch_zsolve(const ZSolveArgs<T>& a, cudaStream_t s, cudaStream_t side, cudaEvent_t fork,
+                                       cudaEvent_t join);
 template <typename T> void launch_ixfft(const IxFftArgs<T>& a, cudaStream_t s);
 template <typename T> void launch_correct(const CorrArgs<T>& a, cudaStream_t s);
 template <typename T> void launch_turb(const TurbArgs<T>& a, cudaStream_t s);

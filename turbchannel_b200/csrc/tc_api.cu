@@ -181,6 +181,8 @@ struct tc_handle {
     Geom g;
     HostMesh hm;
     cudaStream_t st = nullptr;
+    cudaStream_t side = nullptr;  // low-wavenumber double solves of the mixed mode
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     bool fp64 = true;
     size_t esz = 8;
     void* vel[4] = {};
@@ -284,6 +286,9 @@ static void free_all(tc_handle* h) {
     if (h->planes_h) cudaFreeHost(h->planes_h);
     for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
     h->ev.clear();
+    if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+    if (h->ev_join) cudaEventDestroy(h->ev_join);
+    if (h->side) cudaStreamDestroy(h->side);
     if (h->st) cudaStreamDestroy(h->st);
 }
 
@@ -352,9 +357,18 @@ extern "C" int tc_create(const tc_params* prm, const double* zz, tc_handle** out
         delete h;
         return fail(TC_E_ARG, "tc_create: FFT length not supported");
     }
-    if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) {
+    if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+        free_all(h);
         delete h;
         return fail(TC_E_CUDA, "tc_create: stream creation failed");
+    }
+    if ((long long)3 * g.N >= 4294967296LL) {
+        free_all(h);
+        delete h;
+        return fail(TC_E_ARG, "tc_create: grid too large (3 N must stay below 2^32)");
     }
     const size_t N = (size_t)g.N, E = h->esz;
     for (int l = 0; l < 4; l++) {
@@ -606,7 +620,7 @@ static void poisson(tc_handle* h, const void* rhs_vec, const void* rhs_scalar, v
     launch_yfft<T>(ya, h->st);
     if (mk) mark(h, 4, eb);
     ZSolveArgs<T> za{g, mesh_dev<T>(h), mode_tabs(h), (cplx<T>*)h->spec, h->zscr, h->err_flag};
-    launch_zsolve<T>(za, h->st);
+    launch_zsolve<T>(za, h->st, h->side, h->ev_fork, h->ev_join);
     if (mk) mark(h, 5, eb);
     ya.sign = +1;
     launch_yfft<T>(ya, h->st);
