@@ -18,6 +18,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libturbch_b200.so")
+DRIVER_SRC = os.path.join(HERE, "driver", "turbch_run.cpp")
+DRIVER = os.path.join(HERE, "turbch_run")
 
 NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -56,6 +58,10 @@ def build(verbose: bool = False, jobs: int | None = None) -> str:
         list(ex.map(run, cmds))
     if cmds or not _newer(LIB, objs):
         run([NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"])
+    # the command-line driver links the library with an rpath to its directory
+    if not _newer(DRIVER, [DRIVER_SRC, LIB] + headers):
+        run(["g++", "-O2", "-std=c++17", "-I", os.path.join(HERE, "..", "include"), DRIVER_SRC, "-o", DRIVER,
+             "-L", HERE, "-lturbch_b200", f"-Wl,-rpath,{HERE}", "-Wl,-rpath,$ORIGIN"])
     return LIB
 
 
