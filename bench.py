@@ -43,6 +43,10 @@ WORKLOAD = dict(scheme=1, NX=384, NY=384, NZ=256, Lx=2 * math.pi, Ly=math.pi, Re
 PHASE_WORDS = {"turb": 2, "flux": 21, "div_xfft": 4, "yfft": 2, "zsolve": 2, "iyfft": 2, "ixfft": 2, "correct": 7}
 STEP_WORDS = 40
 FALLBACK_HBM_GBS = 6650.0
+# DRAM bytes per cell of one launch (dram__bytes_read.sum + dram__bytes_write.sum) from
+# the ncu capture summarised in profiles/flux_vv4_192x128x192.md (4.7 M cells, inputs
+# larger than L2); traffic grows with the cell count, so it is scaled to the grid.
+TRAFFIC_BYTES_PER_CELL = {("flux", 4): 376.33e6 / 4718592, ("flux", 8): 798.1e6 / 4718592}
 
 
 def peaks():
@@ -169,8 +173,9 @@ def roofline_for(arm, peak_gbs, word_bytes):
     dom = max(per, key=lambda k: per[k])
     bytes_alg = PHASE_WORDS[dom] * word_bytes * N
     ach = bytes_alg / (per[dom] * 1e-3) / 1e9
+    tpc = TRAFFIC_BYTES_PER_CELL.get((dom, word_bytes))
     roof = {"kernel": dom, "bound": "hbm", "achieved": round(ach, 1), "peak": peak_gbs, "unit": "GB/s",
-            "frac": round(ach / peak_gbs, 4), "traffic": None,
+            "frac": round(ach / peak_gbs, 4), "traffic": None if tpc is None else round(tpc * N),
             "bytes_per_launch_alg": bytes_alg, "ms_per_launch": round(per[dom], 5)}
     step_ms = arm["ms"] / arm["steps"]
     step_ach = STEP_WORDS * word_bytes * N / (step_ms * 1e-3) / 1e9
