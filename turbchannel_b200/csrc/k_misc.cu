@@ -249,30 +249,33 @@ void launch_divergence(const DivArgs<T>& a, cudaStream_t s) {
 constexpr int NDIAG = 16;
 static_assert(NDIAG + 3 == TC_DIAG_STRIDE, "diagnostics layout");
 
+// Stage 1: CTA (z, s) reduces chunk s of plane z into part[(z*S + s)*STRIDE + k];
+// stage 2 sums the S chunks of every (z, k) in index order (deterministic).
 template <typename T>
-__global__ void __launch_bounds__(256) k_diag(DiagArgs<T> a) {
+__global__ void __launch_bounds__(256) k_diag(DiagArgs<T> a, double* part, int S) {
     const Geom& g = a.g;
-    const int z = blockIdx.x;
+    const int z = blockIdx.x, s = blockIdx.y;
     const int NX = g.NX, NY = g.NY, NZ = g.NZ;
     const size_t NXY = (size_t)NX * NY;
+    const size_t per = (NXY + S - 1) / S, j0 = (size_t)s * per, j1 = min(NXY, j0 + per);
     const bool coll = g.scheme == TC_SCHEME_COLLOC;
-    double s[NDIAG];
+    double sm[NDIAG];
 #pragma unroll
-    for (int k = 0; k < NDIAG; k++) s[k] = 0;
+    for (int k = 0; k < NDIAG; k++) sm[k] = 0;
     double mconv = 0, mvisc = 0, mboth = 0;
     const double ihx = g.inv_hx, ihy = g.inv_hy;
     const double ihz = coll ? 1.0 / (double)a.m.cellh[z] : 1.0 / (double)a.m.DZ[z];
     const double kv = coll ? (g.visc_type == TC_VISC_GALERKIN ? 2.0 : 1.0) : (g.visc_type != TC_VISC_CROSS ? 2.0 : 1.0);
     const double lap = ihx * ihx + ihy * ihy + ihz * ihz;
-    for (size_t j = threadIdx.x; j < NXY; j += blockDim.x) {
+    for (size_t j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
         const size_t id = (size_t)z * NXY + j;
         const double u = a.v.c[0][id], v = a.v.c[1][id], w = a.v.c[2][id];
         const double wc = coll ? w : 0.5 * (w + (z == NZ - 1 ? 0.0 : (double)a.v.c[2][id + NXY]));
-        s[0] += u; s[1] += v; s[2] += wc;
-        s[3] += u * u; s[4] += v * v; s[5] += wc * wc; s[6] += u * v; s[7] += u * wc; s[8] += v * wc;
+        sm[0] += u; sm[1] += v; sm[2] += wc;
+        sm[3] += u * u; sm[4] += v * v; sm[5] += wc * wc; sm[6] += u * v; sm[7] += u * wc; sm[8] += v * wc;
         double nt = 0;
         if (a.nu_t) {
-            s[9] += a.nu_t[id];
+            sm[9] += a.nu_t[id];
             if (!coll) nt = a.nu_t[id];
             else if (z != 0 && z != NZ - 1) {
                 const int ix = (int)(j % NX), iy = (int)(j / NX);
@@ -284,7 +287,7 @@ __global__ void __launch_bounds__(256) k_diag(DiagArgs<T> a) {
             }
         }
         const double p = a.p ? (double)a.p[id] : 0.0;
-        s[10] += p; s[11] += p * p; s[12] += w; s[13] += w * w;
+        sm[10] += p; sm[11] += p * p; sm[12] += w; sm[13] += w * w;
         const double cc = a.tau * (fabs(u) * ihx + fabs(v) * ihy + fabs(w) * ihz);
         const double cv = 4 * kv * a.tau * ((double)g.visc + nt) * lap;
         mconv = fmax(mconv, cc);
@@ -295,7 +298,7 @@ __global__ void __launch_bounds__(256) k_diag(DiagArgs<T> a) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
     for (int k = 0; k < NDIAG; k++) {
-        const double r = warp_sum(s[k]);
+        const double r = warp_sum(sm[k]);
         if (lane == 0) sb[k][wid] = r;
     }
     mconv = warp_max(mconv);
@@ -311,13 +314,36 @@ __global__ void __launch_bounds__(256) k_diag(DiagArgs<T> a) {
         const int k = threadIdx.x;
         double r = sb[k][0];
         for (int w2 = 1; w2 < (int)(blockDim.x >> 5); w2++) r = k < NDIAG ? r + sb[k][w2] : fmax(r, sb[k][w2]);
-        a.planes[(size_t)z * TC_DIAG_STRIDE + k] = r;
+        part[((size_t)z * S + s) * TC_DIAG_STRIDE + k] = r;
     }
+}
+
+__global__ void k_diag_finish(const double* part, double* planes, int NZ, int S) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= NZ * TC_DIAG_STRIDE) return;
+    const int z = t / TC_DIAG_STRIDE, k = t - z * TC_DIAG_STRIDE;
+    double r = part[((size_t)z * S) * TC_DIAG_STRIDE + k];
+    for (int s = 1; s < S; s++) {
+        const double x = part[((size_t)z * S + s) * TC_DIAG_STRIDE + k];
+        r = k < NDIAG ? r + x : fmax(r, x);
+    }
+    planes[(size_t)z * TC_DIAG_STRIDE + k] = r;
+}
+
+int diag_chunks(const Geom& g) {
+    // about 8 warps per SM worth of CTAs in total, at most one chunk per 2048 cells
+    const long long nxy = (long long)g.NX * g.NY;
+    int S = (int)std::min<long long>(64, std::max<long long>(1, nxy / 2048));
+    while (S > 1 && (long long)S * g.NZ > 148 * 32) S--;
+    return S;
 }
 
 template <typename T>
 void launch_diag(const DiagArgs<T>& a, cudaStream_t s) {
-    k_diag<T><<<a.g.NZ, 256, 0, s>>>(a);
+    const int S = diag_chunks(a.g);
+    k_diag<T><<<dim3(a.g.NZ, S), 256, 0, s>>>(a, a.part, S);
+    const int n = a.g.NZ * TC_DIAG_STRIDE;
+    k_diag_finish<<<(n + 255) / 256, 256, 0, s>>>(a.part, a.planes, a.g.NZ, S);
 }
 
 // ---------------------------------------------------------------------------

@@ -130,6 +130,7 @@ struct DiagArgs {
     const T* nu_t;
     double tau;
     double* planes;  // NZ x TC_DIAG_STRIDE
+    double* part;    // NZ x diag_chunks() x TC_DIAG_STRIDE partial sums
 };
 constexpr int TC_DIAG_STRIDE = 19;
 
@@ -152,6 +153,7 @@ template <typename T> void launch_d2t(const double* src, T* dst, long long n, cu
 template <typename T> void launch_t2d(const T* src, double* dst, long long n, cudaStream_t s);
 
 size_t zsolve_scratch_bytes(const Geom& g, int elem_bytes);
+int diag_chunks(const Geom& g);
 int flux_grid_blocks(const Geom& g);
 
 }  // namespace tc

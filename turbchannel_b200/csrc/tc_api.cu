@@ -201,6 +201,7 @@ struct tc_handle {
     unsigned* ticket = nullptr;
     int* err_flag = nullptr;
     double* planes = nullptr;
+    double* diag_part = nullptr;  // per-chunk partial sums of the diagnostics
     double* planes_h = nullptr;  // pinned
     double* stage = nullptr;     // AoS double staging (3N), lazily
     void* opv = nullptr;         // operator scratch (lazily): vector T
@@ -275,7 +276,7 @@ static const cplx<T>* twy(const tc_handle* h) { return (const cplx<T>*)h->tw + h
 
 static void free_all(tc_handle* h) {
     void* ptrs[] = {h->nu_t, h->ptmp, h->spec, h->zscr, h->mesh_t, h->mesh_d, h->tabs, h->tw, h->red, h->ticket,
-                    h->err_flag, h->planes, h->stage, h->opv, h->opf, h->ops};
+                    h->err_flag, h->planes, h->diag_part, h->stage, h->opv, h->opf, h->ops};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (int l = 0; l < 4; l++) {
@@ -442,6 +443,7 @@ extern "C" int tc_create(const tc_params* prm, const double* zz, tc_handle** out
     TC_ALLOC(h->ticket, sizeof(unsigned));
     TC_ALLOC(h->err_flag, sizeof(int));
     TC_ALLOC(h->planes, (size_t)g.NZ * TC_DIAG_STRIDE * sizeof(double));
+    TC_ALLOC(h->diag_part, (size_t)g.NZ * diag_chunks(g) * TC_DIAG_STRIDE * sizeof(double));
     if (cudaMallocHost((void**)&h->planes_h, (size_t)g.NZ * TC_DIAG_STRIDE * sizeof(double)) != cudaSuccess) {
         free_all(h); delete h;
         return fail(TC_E_NOMEM, "tc_create: pinned host allocation failed");
@@ -807,6 +809,7 @@ static int diag_run(tc_handle* h, int level, double tau) {
     a.nu_t = (h->nu_t && h->turb_kind != TC_TURB_NONE) ? (const T*)h->nu_t : nullptr;
     a.tau = tau;
     a.planes = h->planes;
+    a.part = h->diag_part;
     launch_diag<T>(a, h->st);
     TC_CUDA(cudaGetLastError());
     TC_CUDA(cudaMemcpyAsync(h->planes_h, h->planes, (size_t)h->g.NZ * TC_DIAG_STRIDE * sizeof(double),
