@@ -131,6 +131,16 @@ int tc_op_turb_visc(tc_handle* h, const double* vel_aos, double* nu_t);         
 int tc_set_nu_t(tc_handle* h, const double* nu_t);
 int tc_get_nu_t(tc_handle* h, double* nu_t);
 
+/* Pressure solve (same result as tc_op_pressure_solve) on DEVICE buffers of N cells in
+ * the handle's working precision (double for TC_FP64, float for TC_MIXED; rhs and p
+ * may alias), enqueued on the handle's stream; no counterpart in the reference.  It
+ * allocates nothing: the z-solve's elimination coefficients live in a static device
+ * array of 32 MiB shared by all calls on a device, so the z-solve's
+ * (NX/2+1)*NY*NZ*c*8 bytes (c = 3 for VV4, 1 otherwise) must fit (else TC_E_ARG),
+ * and calls whose launches overlap in time race on it.  The first call on a device
+ * looks the array up (and may load the module): make it before any stream capture. */
+int tc_op_pressure_solve_static(tc_handle* h, const void* rhs, void* p);
+
 /* Seeded channel initial field on level `level`: u = 1.5(1 - y^2) + noise, v, w =
  * noise, noise uniform in [-amp, amp] from MT19937-64(seed) drawn 3 per cell in
  * index order; wall DOFs zero; projected divergence-free with the solver's own

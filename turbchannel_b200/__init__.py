@@ -42,6 +42,7 @@ EXPORTS = [
     "tc_diagnostics", "tc_op_explicit_term", "tc_op_apply_gradient", "tc_op_apply_divergence",
     "tc_op_unapply_gradient", "tc_op_pressure_solve", "tc_op_turb_visc", "tc_set_nu_t", "tc_get_nu_t",
     "tc_init_channel", "tc_mesh_tanh", "tc_phase_timing", "tc_phase_times", "tc_launch_count",
+    "tc_op_pressure_solve_static",
 ]
 NPHASE = 8
 PHASES = ["turb", "flux", "div_xfft", "yfft", "zsolve", "iyfft", "ixfft", "correct"]
@@ -82,7 +83,7 @@ def load_library(path: str = LIB_PATH):
     L.tc_profiles.argtypes = [vp, ip, vp]
     L.tc_diagnostics.argtypes = [vp, ip, C.c_double, vp, dp, vp]
     for fn in ("tc_op_explicit_term", "tc_op_apply_gradient", "tc_op_apply_divergence", "tc_op_unapply_gradient",
-               "tc_op_pressure_solve", "tc_op_turb_visc"):
+               "tc_op_pressure_solve", "tc_op_turb_visc", "tc_op_pressure_solve_static"):
         getattr(L, fn).argtypes = [vp, vp, vp]
     L.tc_set_nu_t.argtypes = [vp, vp]
     L.tc_get_nu_t.argtypes = [vp, vp]

@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <random>
 #include <string>
 #include <vector>
@@ -1045,4 +1046,88 @@ extern "C" int tc_init_channel(tc_handle* h, int level, unsigned long long seed,
         TC_CUDA(cudaStreamSynchronize(h->st));
     }
     return TC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Pressure solve on device buffers that allocates nothing at call time.
+//
+// tc_op_pressure_solve works on host arrays: on first use it allocates operator
+// buffers and a staging buffer with cudaMalloc.  Some callers cannot do that: a host
+// code that hands (nearly) all of HBM to its own pool or caching allocator up front
+// has no device memory left for a library to allocate, and a latency-critical time
+// loop cannot take cudaMalloc's implicit device-wide synchronisation.  This variant
+// takes the right-hand side and the result as device pointers in the handle's working
+// precision and runs the same launches as the step's pressure solve, with one change:
+// the z-solve's elimination coefficients live in a file-scope static device array
+// (below) instead of the handle's scratch buffer.
+//
+// * Setup: the first call on a device looks the array up with cudaGetSymbolAddress
+//   (which may load this module into the context), so it should come before any
+//   stream capture; later calls on that device only read the cached address.
+// * Size limit: the z-solve needs (NX/2+1)*NY*NZ*c*8 bytes (c = 3 for VV4, 1
+//   otherwise); problems above TC_STATIC_ZSCR_BYTES (32 MiB) are rejected with
+//   TC_E_ARG.
+// * Nothing in the array has to start at zero: the forward sweep writes every
+//   coefficient of a mode before the backward sweep reads it.
+// * The array is shared by every call on a device (every handle, stream and host
+//   thread): calls whose launches overlap in time race on it.  Serialise them, e.g.
+//   by issuing them on one stream.
+// ---------------------------------------------------------------------------
+static constexpr size_t TC_STATIC_ZSCR_BYTES = (size_t)32 << 20;
+static __device__ __align__(256) unsigned char g_static_zscr[TC_STATIC_ZSCR_BYTES];
+
+static std::mutex g_static_mu;
+static void* g_static_zscr_ptr[64] = {};
+
+// Address of g_static_zscr on device `dev` (which must be current).
+static int static_zscr(int dev, void** out) {
+    if (dev < 0 || dev >= 64) return fail(TC_E_ARG, "static z-solve scratch: device index out of range");
+    std::lock_guard<std::mutex> lk(g_static_mu);
+    if (!g_static_zscr_ptr[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_static_zscr);
+        if (e != cudaSuccess || !p)
+            return fail(TC_E_CUDA, std::string("cudaGetSymbolAddress(static z-solve scratch): ") + cudaGetErrorString(e));
+        g_static_zscr_ptr[dev] = p;
+    }
+    *out = g_static_zscr_ptr[dev];
+    return TC_OK;
+}
+
+template <typename T>
+static int poisson_static(tc_handle* h, const void* rhs, void* p_out, void* scratch) {
+    const Geom& g = h->g;
+    DivFftArgs<T> da;
+    da.g = g;
+    da.m = mesh_dev<T>(h);
+    da.v = CV3<T>{{nullptr, nullptr, nullptr}};
+    da.src_scalar = (const T*)rhs;
+    da.spec = (cplx<T>*)h->spec;
+    da.px = h->px;
+    da.twx = twx<T>(h);
+    launch_div_xfft<T>(da, h->st);
+    YFftArgs<T> ya{g, (cplx<T>*)h->spec, h->py, twy<T>(h), -1};
+    launch_yfft<T>(ya, h->st);
+    ZSolveArgs<T> za{g, mesh_dev<T>(h), mode_tabs(h), (cplx<T>*)h->spec, scratch, h->err_flag};
+    launch_zsolve<T>(za, h->st, h->side, h->ev_fork, h->ev_join);
+    ya.sign = +1;
+    launch_yfft<T>(ya, h->st);
+    IxFftArgs<T> ia{g, (const cplx<T>*)h->spec, (T*)p_out, h->px, twx<T>(h), (T)(1.0 / ((double)g.NX * g.NY))};
+    launch_ixfft<T>(ia, h->st);
+    h->launches += 5 + (sizeof(T) == 4 ? 1 : 0);
+    return check_launch("pressure_solve_static");
+}
+
+extern "C" int tc_op_pressure_solve_static(tc_handle* h, const void* rhs, void* p) {
+    if (!h || !rhs || !p) return fail(TC_E_ARG, "tc_op_pressure_solve_static: null handle or buffer");
+    const size_t need = zsolve_scratch_bytes(h->g, (int)h->esz);
+    if (need > TC_STATIC_ZSCR_BYTES)
+        return fail(TC_E_ARG, "tc_op_pressure_solve_static: the z-solve needs " + std::to_string(need) +
+                                  " bytes of scratch ((NX/2+1)*NY*NZ*c*8, c = 3 for VV4, 1 otherwise), above the "
+                                  "static array's " + std::to_string(TC_STATIC_ZSCR_BYTES) + " bytes");
+    TC_CUDA(cudaSetDevice(h->prm.device));
+    void* scr = nullptr;
+    const int rc = static_zscr(h->prm.device, &scr);
+    if (rc) return rc;
+    return TC_DISPATCH(h, poisson_static, h, rhs, p, scr);
 }
