@@ -214,10 +214,19 @@ def e2e_arm(arm, steps, device):
     e1.record(stream)
     e1.synchronize()
     ms = e0.elapsed_time(e1)
+    # the per-step diagnostics alone (kernel, copy of the plane sums, host wait)
+    nd = min(steps, 50)
+    e0.record(stream)
+    for _ in range(nd):
+        S.diagnostics(cur, tau)
+    e1.record(stream)
+    e1.synchronize()
+    diag_ms = e0.elapsed_time(e1) / nd
     diag_bytes = p["NZ"] * 19 * 8
     field_bytes = 4 * N * 8
     return dict(value=N * steps / (ms * 1e-3), unit="cell-steps/s", ms_per_step=ms / steps,
-                h2d_bytes_per_step=field_bytes // steps, d2h_bytes_per_step=diag_bytes + field_bytes // steps)
+                h2d_bytes_per_step=field_bytes // steps, d2h_bytes_per_step=diag_bytes + field_bytes // steps,
+                diagnostics_ms=round(diag_ms, 4))
 
 
 def cpu_baseline(small=False, budget_s=20.0, max_steps=3):

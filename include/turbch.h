@@ -131,7 +131,7 @@ int tc_op_turb_visc(tc_handle* h, const double* vel_aos, double* nu_t);         
 int tc_set_nu_t(tc_handle* h, const double* nu_t);
 int tc_get_nu_t(tc_handle* h, double* nu_t);
 
-/* Pressure solve (same result as tc_op_pressure_solve) on DEVICE buffers of N cells in
+/* Pressure solve (tc_op_pressure_solve's result up to round-off) on DEVICE buffers of N cells in
  * the handle's working precision (double for TC_FP64, float for TC_MIXED; rhs and p
  * may alias), enqueued on the handle's stream; no counterpart in the reference.  It
  * allocates nothing: the z-solve's elimination coefficients live in a static device

@@ -250,14 +250,34 @@ constexpr int NDIAG = 16;
 static_assert(NDIAG + 3 == TC_DIAG_STRIDE, "diagnostics layout");
 
 // Stage 1: CTA (z, s) reduces chunk s of plane z into part[(z*S + s)*STRIDE + k];
-// stage 2 sums the S chunks of every (z, k) in index order (deterministic).
+// stage 2 sums the S chunks of every (z, k) in index order (deterministic).  Chunks
+// are multiples of 4 cells (NX*NY is), read as 16-byte vectors of 4 cells, so each
+// thread keeps 5-6 vector loads in flight per iteration.
+template <typename T>
+struct Acc4 {
+    T v[4];
+};
+template <typename T>
+__device__ __forceinline__ Acc4<T> ld4(const T* p) {
+    Acc4<T> r;
+    if constexpr (sizeof(T) == 4) {
+        const float4 q = __ldg(reinterpret_cast<const float4*>(p));
+        r.v[0] = q.x; r.v[1] = q.y; r.v[2] = q.z; r.v[3] = q.w;
+    } else {
+        const double2 q0 = __ldg(reinterpret_cast<const double2*>(p));
+        const double2 q1 = __ldg(reinterpret_cast<const double2*>(p) + 1);
+        r.v[0] = q0.x; r.v[1] = q0.y; r.v[2] = q1.x; r.v[3] = q1.y;
+    }
+    return r;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256) k_diag(DiagArgs<T> a, double* part, int S) {
     const Geom& g = a.g;
     const int z = blockIdx.x, s = blockIdx.y;
-    const int NX = g.NX, NY = g.NY, NZ = g.NZ;
-    const size_t NXY = (size_t)NX * NY;
-    const size_t per = (NXY + S - 1) / S, j0 = (size_t)s * per, j1 = min(NXY, j0 + per);
+    const int NX = g.NX, NZ = g.NZ;
+    const size_t NXY = (size_t)NX * g.NY;
+    const size_t per = ((NXY + 4 * S - 1) / (4 * S)) * 4, j0 = (size_t)s * per, j1 = min(NXY, j0 + per);
     const bool coll = g.scheme == TC_SCHEME_COLLOC;
     double sm[NDIAG];
 #pragma unroll
@@ -267,32 +287,43 @@ __global__ void __launch_bounds__(256) k_diag(DiagArgs<T> a, double* part, int S
     const double ihz = coll ? 1.0 / (double)a.m.cellh[z] : 1.0 / (double)a.m.DZ[z];
     const double kv = coll ? (g.visc_type == TC_VISC_GALERKIN ? 2.0 : 1.0) : (g.visc_type != TC_VISC_CROSS ? 2.0 : 1.0);
     const double lap = ihx * ihx + ihy * ihy + ihz * ihz;
-    for (size_t j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
-        const size_t id = (size_t)z * NXY + j;
-        const double u = a.v.c[0][id], v = a.v.c[1][id], w = a.v.c[2][id];
-        const double wc = coll ? w : 0.5 * (w + (z == NZ - 1 ? 0.0 : (double)a.v.c[2][id + NXY]));
-        sm[0] += u; sm[1] += v; sm[2] += wc;
-        sm[3] += u * u; sm[4] += v * v; sm[5] += wc * wc; sm[6] += u * v; sm[7] += u * wc; sm[8] += v * wc;
-        double nt = 0;
-        if (a.nu_t) {
-            sm[9] += a.nu_t[id];
-            if (!coll) nt = a.nu_t[id];
-            else if (z != 0 && z != NZ - 1) {
-                const int ix = (int)(j % NX), iy = (int)(j / NX);
-                const int xm = ix == 0 ? NX - 1 : ix - 1, ym = iy == 0 ? NY - 1 : iy - 1;
-                const T* n = a.nu_t;
-                const size_t p0 = (size_t)z * NXY, p1 = p0 - NXY;
-                nt = 0.125 * ((double)n[p0 + iy * NX + ix] + n[p0 + iy * NX + xm] + n[p0 + ym * NX + ix] + n[p0 + ym * NX + xm] +
-                              n[p1 + iy * NX + ix] + n[p1 + iy * NX + xm] + n[p1 + ym * NX + ix] + n[p1 + ym * NX + xm]);
+    const size_t pl = (size_t)z * NXY;
+    const bool wtop = !coll && z == NZ - 1;  // staggered: w above the top cell is the wall (0)
+    for (size_t j = j0 + 4 * threadIdx.x; j < j1; j += 4 * blockDim.x) {
+        const size_t id = pl + j;
+        const Acc4<T> U = ld4(a.v.c[0] + id), V = ld4(a.v.c[1] + id), W = ld4(a.v.c[2] + id);
+        Acc4<T> WN, P, NT;
+        if (!coll && !wtop) WN = ld4(a.v.c[2] + id + NXY);
+        if (a.p) P = ld4(a.p + id);
+        if (a.nu_t) NT = ld4(a.nu_t + id);
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const double u = U.v[q], v = V.v[q], w = W.v[q];
+            const double wc = coll ? w : 0.5 * (w + (wtop ? 0.0 : (double)WN.v[q]));
+            sm[0] += u; sm[1] += v; sm[2] += wc;
+            sm[3] += u * u; sm[4] += v * v; sm[5] += wc * wc; sm[6] += u * v; sm[7] += u * wc; sm[8] += v * wc;
+            double nt = 0;
+            if (a.nu_t) {
+                sm[9] += (double)NT.v[q];
+                if (!coll) nt = NT.v[q];
+                else if (z != 0 && z != NZ - 1) {
+                    const size_t jj = j + q;
+                    const int ix = (int)(jj % NX), iy = (int)(jj / NX);
+                    const int xm = ix == 0 ? NX - 1 : ix - 1, ym = iy == 0 ? g.NY - 1 : iy - 1;
+                    const T* n = a.nu_t;
+                    const size_t p0 = pl, p1 = p0 - NXY;
+                    nt = 0.125 * ((double)n[p0 + iy * NX + ix] + n[p0 + iy * NX + xm] + n[p0 + ym * NX + ix] + n[p0 + ym * NX + xm] +
+                                  n[p1 + iy * NX + ix] + n[p1 + iy * NX + xm] + n[p1 + ym * NX + ix] + n[p1 + ym * NX + xm]);
+                }
             }
+            const double p = a.p ? (double)P.v[q] : 0.0;
+            sm[10] += p; sm[11] += p * p; sm[12] += w; sm[13] += w * w;
+            const double cc = a.tau * (fabs(u) * ihx + fabs(v) * ihy + fabs(w) * ihz);
+            const double cv = 4 * kv * a.tau * ((double)g.visc + nt) * lap;
+            mconv = fmax(mconv, cc);
+            mvisc = fmax(mvisc, cv);
+            mboth = fmax(mboth, cc + cv);
         }
-        const double p = a.p ? (double)a.p[id] : 0.0;
-        sm[10] += p; sm[11] += p * p; sm[12] += w; sm[13] += w * w;
-        const double cc = a.tau * (fabs(u) * ihx + fabs(v) * ihy + fabs(w) * ihz);
-        const double cv = 4 * kv * a.tau * ((double)g.visc + nt) * lap;
-        mconv = fmax(mconv, cc);
-        mvisc = fmax(mvisc, cv);
-        mboth = fmax(mboth, cc + cv);
     }
     __shared__ double sb[NDIAG + 3][8];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;

@@ -471,6 +471,277 @@ void launch_zsolve(const ZSolveArgs<T>& a, cudaStream_t s, cudaStream_t side, cu
 }
 
 // ---------------------------------------------------------------------------
+// Factored z-solve.  The z-matrix of a mode depends on the mesh and the mode only,
+// not on the time step, so its elimination (the same row order, pivots and
+// multipliers as zsolve_mode_at) is done once, in double, at solver creation and
+// stored in the working precision T as
+//   forward   z_i = F0_i r_i - F1_i z_{i-1} - F2_i z_{i-2} - F3_i z_{i-3}
+//   backward  x_i = z_i - B0_i x_{i+1} - B1_i x_{i+2} - B2_i x_{i+3}
+// (tridiagonal schemes: F0, F1, B0).  Layout: VV4 F[i][m] = {F0,F1,F2,F3} then
+// B[i][m] = {B0,B1,B2,0}; tridiagonal F[i][m] = {F0,F1} then B[i][m] = B0.  The
+// per-step solve then streams r, F, B with no divide and a one-FMA recurrence
+// chain, so many rows of loads are in flight per thread.
+// ---------------------------------------------------------------------------
+template <typename T>
+struct alignas(4 * sizeof(T)) Q4 {
+    T x, y, z, w;
+};
+template <typename T>
+struct alignas(2 * sizeof(T)) Q2 {
+    T x, y;
+};
+
+size_t zfactor_bytes(const Geom& g, int elem_bytes) {
+    const size_t per = g.scheme == TC_SCHEME_VV4 ? 8 : 3;
+    return (size_t)g.NXH * g.NY * g.NZ * per * elem_bytes;
+}
+
+template <typename T, int SCHEME>
+__global__ void __launch_bounds__(128) k_zfactor(ZSolveArgs<T> a) {
+    const Geom& g = a.g;
+    const size_t M = (size_t)g.NXH * g.NY;
+    const size_t m = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= M) return;
+    const int kx = (int)(m / g.NY), ky = (int)(m - (size_t)kx * g.NY);
+    const int NZ = g.NZ;
+    const bool pin = (kx == 0 && ky == 0);
+    const double* MA = a.m.dMAT_A;
+    const double* DZ = a.m.dDZ;
+    const double* DZW = a.m.dDZW;
+    if (SCHEME == TC_SCHEME_HW2 || SCHEME == TC_SCHEME_COLLOC) {
+        Q2<T>* F = reinterpret_cast<Q2<T>*>(a.fac);
+        T* B = reinterpret_cast<T*>(F + (size_t)NZ * M);
+        double MM;
+        if (SCHEME == TC_SCHEME_HW2)
+            MM = 2 * ((1 - a.tabs.cosx[kx]) * g.inv_hx * g.inv_hx + (1 - a.tabs.cosy[ky]) * g.inv_hy * g.inv_hy);
+        else
+            MM = (1 - a.tabs.cosx[kx]) * g.hy / g.hx + (1 - a.tabs.cosy[ky]) * g.hx / g.hy;
+        double b0;
+        if (SCHEME == TC_SCHEME_HW2) b0 = -DZ[0] * MM - MA[1];
+        else {
+            b0 = -MA[1];
+            if (!g.fd_mode) b0 += DZ[0] * MM;
+        }
+        if (pin) b0 *= 2;
+        const double ib0 = 1 / b0;
+        double pp = MA[1] * ib0;
+        F[m] = {(T)ib0, (T)0};
+        B[m] = (T)pp;
+        for (int i = 1; i <= NZ - 1; i++) {
+            double d;
+            if (SCHEME == TC_SCHEME_HW2) {
+                d = -MA[i] - DZ[i] * MM;
+                if (i != NZ - 1) d -= MA[i + 1];
+            } else {
+                const double mm = (g.fd_mode && (i == NZ - 1)) ? 0.0 : MM;
+                d = 0;
+                d -= MA[i] + DZ[i - 1] * mm;
+                if (i != NZ - 1) d -= MA[i + 1] + DZ[i] * mm;
+            }
+            d -= MA[i] * pp;
+            d = 1 / d;
+            pp = i != NZ - 1 ? MA[i + 1] * d : 0.0;
+            F[(size_t)i * M + m] = {(T)d, (T)(MA[i] * d)};
+            B[(size_t)i * M + m] = (T)pp;
+        }
+    } else {
+        Q4<T>* F = reinterpret_cast<Q4<T>*>(a.fac);
+        Q4<T>* B = F + (size_t)NZ * M;
+        const double C27 = 0.03703703703703703703, C9 = 0.11111111111111111111;
+        const double sx = a.tabs.sinx[kx], sy = a.tabs.siny[ky];
+        const double s3x = 3 * sx - 4 * sx * sx * sx, s3y = 3 * sy - 4 * sy * sy * sy;
+        const double ihx = g.inv_hx, ihy = g.inv_hy;
+        double b[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        for (int i = 0; i < NZ; i++) {
+            double row[7] = {0, 0, 0, 0, 0, 0, 0};
+            double sum = 0;
+            for (int k = 0; k < 3; k++) {
+                if (i + k - 3 < 0 || i + k - 3 >= NZ) continue;
+                row[k] = MA[i * 3 + k];
+                sum += MA[i * 3 + k];
+            }
+            for (int k = 1; k <= 3; k++) {
+                if (i + k >= NZ) continue;
+                row[3 + k] = MA[(i + k) * 3 + 3 - k];
+                sum += MA[(i + k) * 3 + 3 - k];
+            }
+            if (i <= 2) row[3] = a.m.MAT_D[i];
+            else if (i >= NZ - 3) row[3] = a.m.MAT_D[i - (NZ - 3) + 3];
+            else row[3] = -sum;
+            if (pin && i == 0) row[3] *= 2;
+            {
+                double ci = DZ[i] * sx - C27 * DZW[i] * s3x;
+                row[3] -= 4 * ihx * ihx * ci * ci / (DZ[i] - C9 * DZW[i]);
+                ci = DZ[i] * sy - C27 * DZW[i] * s3y;
+                row[3] -= 4 * ihy * ihy * ci * ci / (DZ[i] - C9 * DZW[i]);
+            }
+            double used[3] = {0, 0, 0};  // row entry eliminated against z_{i-3}, z_{i-2}, z_{i-1}
+            for (int j = -3; j < 0; j++) {
+                if (i + j < 0) continue;
+                used[3 + j] = row[3 + j];
+                const double mult = -row[3 + j];
+                for (int k = 1; k <= 3; k++) {
+                    if (i + j + k >= NZ) continue;
+                    row[3 + j + k] += mult * b[3 + j][k - 1];
+                }
+            }
+            if (fabs(row[3]) < 1e-30) {
+                if (a.err_flag) atomicExch(a.err_flag, 1);
+                return;
+            }
+            const double inv = 1.0 / row[3];
+            double nb[3];
+            for (int k = 1; k <= 3; k++) nb[k - 1] = (i + k >= NZ) ? 0.0 : row[3 + k] * inv;
+            F[(size_t)i * M + m] = {(T)inv, (T)(used[2] * inv), (T)(used[1] * inv), (T)(used[0] * inv)};
+            B[(size_t)i * M + m] = {(T)nb[0], (T)nb[1], (T)nb[2], (T)0};
+            for (int j = 0; j < 2; j++)
+                for (int k = 0; k < 3; k++) b[j][k] = b[j + 1][k];
+            for (int k = 0; k < 3; k++) b[2][k] = nb[k];
+        }
+    }
+}
+
+template <typename T>
+void launch_zfactor(const ZSolveArgs<T>& a, cudaStream_t s) {
+    const size_t M = (size_t)a.g.NXH * a.g.NY;
+    const unsigned nb = (unsigned)((M + 127) / 128);
+    if (a.g.scheme == TC_SCHEME_VV4) k_zfactor<T, TC_SCHEME_VV4><<<nb, 128, 0, s>>>(a);
+    else if (a.g.scheme == TC_SCHEME_HW2) k_zfactor<T, TC_SCHEME_HW2><<<nb, 128, 0, s>>>(a);
+    else k_zfactor<T, TC_SCHEME_COLLOC><<<nb, 128, 0, s>>>(a);
+}
+
+// One thread per mode outside the low set.  Rows are moved R at a time through two
+// register batches: the loads of batch b+1 are issued before batch b is consumed.
+template <typename T, int SCHEME>
+__global__ void __launch_bounds__(128) k_zsolve_fac(ZSolveArgs<T> a) {
+    constexpr bool VV = SCHEME == TC_SCHEME_VV4;
+    constexpr int R = sizeof(T) == 4 ? 8 : 4;
+    using FQ = typename std::conditional<VV, Q4<T>, Q2<T>>::type;
+    using BQ = typename std::conditional<VV, Q4<T>, T>::type;
+    const Geom& g = a.g;
+    const size_t M = (size_t)g.NXH * g.NY;
+    const size_t m = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= M) return;
+    const int kx = (int)(m / g.NY), ky = (int)(m - (size_t)kx * g.NY);
+    const int LM = g.low_modes;
+    if (kx < LM && (ky < LM || ky > g.NY - LM)) return;
+    const int NZ = g.NZ;
+    const FQ* F = reinterpret_cast<const FQ*>(a.fac) + m;
+    const BQ* B = reinterpret_cast<const BQ*>(reinterpret_cast<const FQ*>(a.fac) + (size_t)NZ * M) + m;
+    cplx<T>* x = a.spec + m;
+
+    // forward
+    {
+        cplx<T> z1 = {0, 0}, z2 = {0, 0}, z3 = {0, 0};
+        cplx<T> ra[R], rb[R];
+        FQ fa[R], fb[R];
+        auto load = [&](int i0, cplx<T>(&r)[R], FQ(&f)[R]) {
+#pragma unroll
+            for (int k = 0; k < R; k++)
+                if (i0 + k < NZ) {
+                    r[k] = x[(size_t)(i0 + k) * M];
+                    f[k] = F[(size_t)(i0 + k) * M];
+                }
+        };
+        auto run = [&](int i0, const cplx<T>(&r)[R], const FQ(&f)[R]) {
+#pragma unroll
+            for (int k = 0; k < R; k++) {
+                if (i0 + k >= NZ) break;
+                cplx<T> z;
+                if constexpr (VV) {
+                    z.x = r[k].x * f[k].x - f[k].w * z3.x - f[k].z * z2.x;
+                    z.y = r[k].y * f[k].x - f[k].w * z3.y - f[k].z * z2.y;
+                } else {
+                    z.x = r[k].x * f[k].x;
+                    z.y = r[k].y * f[k].x;
+                }
+                z.x -= f[k].y * z1.x;
+                z.y -= f[k].y * z1.y;
+                x[(size_t)(i0 + k) * M] = z;
+                z3 = z2;
+                z2 = z1;
+                z1 = z;
+            }
+        };
+        load(0, ra, fa);
+        for (int i0 = 0; i0 < NZ; i0 += 2 * R) {
+            load(i0 + R, rb, fb);
+            run(i0, ra, fa);
+            load(i0 + 2 * R, ra, fa);
+            run(i0 + R, rb, fb);
+        }
+    }
+    // backward (row NZ-1 first)
+    {
+        cplx<T> x1 = {0, 0}, x2 = {0, 0}, x3 = {0, 0};
+        cplx<T> za[R], zb[R];
+        BQ ba[R], bb[R];
+        auto load = [&](int i0, cplx<T>(&zz)[R], BQ(&bq)[R]) {
+#pragma unroll
+            for (int k = 0; k < R; k++)
+                if (i0 - k >= 0) {
+                    zz[k] = x[(size_t)(i0 - k) * M];
+                    bq[k] = B[(size_t)(i0 - k) * M];
+                }
+        };
+        auto run = [&](int i0, const cplx<T>(&zz)[R], const BQ(&bq)[R]) {
+#pragma unroll
+            for (int k = 0; k < R; k++) {
+                if (i0 - k < 0) break;
+                cplx<T> v;
+                if constexpr (VV) {
+                    v.x = zz[k].x - bq[k].z * x3.x - bq[k].y * x2.x;
+                    v.y = zz[k].y - bq[k].z * x3.y - bq[k].y * x2.y;
+                    v.x -= bq[k].x * x1.x;
+                    v.y -= bq[k].x * x1.y;
+                } else {
+                    v.x = zz[k].x - bq[k] * x1.x;
+                    v.y = zz[k].y - bq[k] * x1.y;
+                }
+                x[(size_t)(i0 - k) * M] = v;
+                x3 = x2;
+                x2 = x1;
+                x1 = v;
+            }
+        };
+        load(NZ - 1, za, ba);
+        for (int i0 = NZ - 1; i0 >= 0; i0 -= 2 * R) {
+            load(i0 - R, zb, bb);
+            run(i0, za, ba);
+            load(i0 - 2 * R, za, ba);
+            run(i0 - R, zb, bb);
+        }
+    }
+}
+
+template <typename T, int SCHEME>
+static void zsolve_fac_scheme(const ZSolveArgs<T>& a, cudaStream_t s, cudaStream_t side, cudaEvent_t fork,
+                              cudaEvent_t join) {
+    const size_t M = (size_t)a.g.NXH * a.g.NY;
+    // the low modes (exact elimination in double, mode (0,0) normalised) on a side
+    // stream next to the factored solve of all other modes; the two sets are disjoint
+    cudaEventRecord(fork, s);
+    cudaStreamWaitEvent(side, fork, 0);
+    const int nlow = a.g.low_modes * (2 * a.g.low_modes - 1);
+    const int nc = SCHEME == TC_SCHEME_VV4 ? 3 : 1;
+    const int nma = SCHEME == TC_SCHEME_VV4 ? 3 * a.g.NZ : a.g.NZ;
+    const size_t smem = (size_t)a.g.NZ * (sizeof(cplx<double>) + nc * sizeof(double)) + (size_t)(nma + 2 * a.g.NZ) * sizeof(double);
+    auto k = k_zsolve_low<T, SCHEME>;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k<<<nlow, 128, smem, side>>>(a);
+    cudaEventRecord(join, side);
+    k_zsolve_fac<T, SCHEME><<<(unsigned)((M + 127) / 128), 128, 0, s>>>(a);
+    cudaStreamWaitEvent(s, join, 0);
+}
+
+template <typename T>
+void launch_zsolve_fac(const ZSolveArgs<T>& a, cudaStream_t s, cudaStream_t side, cudaEvent_t fork, cudaEvent_t join) {
+    if (a.g.scheme == TC_SCHEME_VV4) zsolve_fac_scheme<T, TC_SCHEME_VV4>(a, s, side, fork, join);
+    else if (a.g.scheme == TC_SCHEME_HW2) zsolve_fac_scheme<T, TC_SCHEME_HW2>(a, s, side, fork, join);
+    else zsolve_fac_scheme<T, TC_SCHEME_COLLOC>(a, s, side, fork, join);
+}
+
+// ---------------------------------------------------------------------------
 // inverse x-FFT (complex-to-real, two rows per complex FFT) and scaling
 // ---------------------------------------------------------------------------
 template <typename T, int ROWS>
@@ -534,6 +805,10 @@ template void launch_yfft<double>(const YFftArgs<double>&, cudaStream_t);
 template void launch_yfft<float>(const YFftArgs<float>&, cudaStream_t);
 template void launch_zsolve<double>(const ZSolveArgs<double>&, cudaStream_t, cudaStream_t, cudaEvent_t, cudaEvent_t);
 template void launch_zsolve<float>(const ZSolveArgs<float>&, cudaStream_t, cudaStream_t, cudaEvent_t, cudaEvent_t);
+template void launch_zsolve_fac<double>(const ZSolveArgs<double>&, cudaStream_t, cudaStream_t, cudaEvent_t, cudaEvent_t);
+template void launch_zsolve_fac<float>(const ZSolveArgs<float>&, cudaStream_t, cudaStream_t, cudaEvent_t, cudaEvent_t);
+template void launch_zfactor<double>(const ZSolveArgs<double>&, cudaStream_t);
+template void launch_zfactor<float>(const ZSolveArgs<float>&, cudaStream_t);
 template void launch_ixfft<double>(const IxFftArgs<double>&, cudaStream_t);
 template void launch_ixfft<float>(const IxFftArgs<float>&, cudaStream_t);
 

@@ -70,6 +70,7 @@ struct ZSolveArgs {
     cplx<T>* spec;
     void* scratch;  // per-mode elimination coefficients
     int* err_flag;  // set when a pivot underflows (the reference writes -1e50)
+    void* fac = nullptr;  // precomputed factors (k_zfactor layout), zfactor_bytes()
 };
 
 // Inverse real FFT along x: p = scale * C2R(spec) (+ dest layout [z][y][x]).
@@ -140,6 +141,10 @@ template <typename T> void launch_div_xfft(const DivFftArgs<T>& a, cudaStream_t 
 template <typename T> void launch_yfft(const YFftArgs<T>& a, cudaStream_t s);
 template <typename T> void launch_zsolve(const ZSolveArgs<T>& a, cudaStream_t s, cudaStream_t side, cudaEvent_t fork,
                                        cudaEvent_t join);
+// factored solve (step path): launch_zfactor once at creation, then launch_zsolve_fac
+template <typename T> void launch_zfactor(const ZSolveArgs<T>& a, cudaStream_t s);
+template <typename T> void launch_zsolve_fac(const ZSolveArgs<T>& a, cudaStream_t s, cudaStream_t side,
+                                           cudaEvent_t fork, cudaEvent_t join);
 template <typename T> void launch_ixfft(const IxFftArgs<T>& a, cudaStream_t s);
 template <typename T> void launch_correct(const CorrArgs<T>& a, cudaStream_t s);
 template <typename T> void launch_turb(const TurbArgs<T>& a, cudaStream_t s);
@@ -153,6 +158,7 @@ template <typename T> void launch_d2t(const double* src, T* dst, long long n, cu
 template <typename T> void launch_t2d(const T* src, double* dst, long long n, cudaStream_t s);
 
 size_t zsolve_scratch_bytes(const Geom& g, int elem_bytes);
+size_t zfactor_bytes(const Geom& g, int elem_bytes);
 int diag_chunks(const Geom& g);
 int flux_grid_blocks(const Geom& g);
 

@@ -192,7 +192,7 @@ struct tc_handle {
     void* nu_t = nullptr;
     void* ptmp = nullptr;
     void* spec = nullptr;
-    void* zscr = nullptr;
+    void* zfac = nullptr;  // time-independent factors of the z-matrices (k_zfactor)
     void* mesh_t = nullptr;     // mesh arrays in T
     double* mesh_d = nullptr;   // mesh arrays in double
     double* tabs = nullptr;     // cos/sin tables
@@ -276,7 +276,7 @@ template <typename T>
 static const cplx<T>* twy(const tc_handle* h) { return (const cplx<T>*)h->tw + h->g.NX; }
 
 static void free_all(tc_handle* h) {
-    void* ptrs[] = {h->nu_t, h->ptmp, h->spec, h->zscr, h->mesh_t, h->mesh_d, h->tabs, h->tw, h->red, h->ticket,
+    void* ptrs[] = {h->nu_t, h->ptmp, h->spec, h->zfac, h->mesh_t, h->mesh_d, h->tabs, h->tw, h->red, h->ticket,
                     h->err_flag, h->planes, h->diag_part, h->stage, h->opv, h->opf, h->ops};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -381,7 +381,7 @@ extern "C" int tc_create(const tc_params* prm, const double* zz, tc_handle** out
     if (p.turb_model != TC_TURB_NONE) TC_ALLOC(h->nu_t, N * E);
     TC_ALLOC(h->ptmp, N * E);
     TC_ALLOC(h->spec, (size_t)g.NXH * g.NY * g.NZ * 2 * E);
-    TC_ALLOC(h->zscr, zsolve_scratch_bytes(g, (int)E));
+    TC_ALLOC(h->zfac, zfactor_bytes(g, (int)E));
     // mesh arrays, 9 slots of NZ+2 (the last one holds MAT_A, up to 3 NZ entries)
     const int L = g.NZ + 2;
     const size_t mlen = (size_t)8 * L + 3 * (size_t)L;
@@ -458,6 +458,14 @@ extern "C" int tc_create(const tc_params* prm, const double* zz, tc_handle** out
         cudaMemsetAsync(h->pres[l], 0, N * E, h->st);
     }
     if (h->nu_t) cudaMemsetAsync(h->nu_t, 0, N * E, h->st);
+    cudaMemsetAsync(h->zfac, 0, zfactor_bytes(g, (int)E), h->st);
+    if (h->fp64) {
+        ZSolveArgs<double> za{g, mesh_dev<double>(h), mode_tabs(h), (cplx<double>*)h->spec, nullptr, h->err_flag, h->zfac};
+        launch_zfactor<double>(za, h->st);
+    } else {
+        ZSolveArgs<float> za{g, mesh_dev<float>(h), mode_tabs(h), (cplx<float>*)h->spec, nullptr, h->err_flag, h->zfac};
+        launch_zfactor<float>(za, h->st);
+    }
     cudaError_t e = cudaStreamSynchronize(h->st);
     if (e != cudaSuccess) {
         free_all(h); delete h;
@@ -622,8 +630,8 @@ static void poisson(tc_handle* h, const void* rhs_vec, const void* rhs_scalar, v
     YFftArgs<T> ya{g, (cplx<T>*)h->spec, h->py, twy<T>(h), -1};
     launch_yfft<T>(ya, h->st);
     if (mk) mark(h, 4, eb);
-    ZSolveArgs<T> za{g, mesh_dev<T>(h), mode_tabs(h), (cplx<T>*)h->spec, h->zscr, h->err_flag};
-    launch_zsolve<T>(za, h->st, h->side, h->ev_fork, h->ev_join);
+    ZSolveArgs<T> za{g, mesh_dev<T>(h), mode_tabs(h), (cplx<T>*)h->spec, nullptr, h->err_flag, h->zfac};
+    launch_zsolve_fac<T>(za, h->st, h->side, h->ev_fork, h->ev_join);
     if (mk) mark(h, 5, eb);
     ya.sign = +1;
     launch_yfft<T>(ya, h->st);
@@ -631,7 +639,7 @@ static void poisson(tc_handle* h, const void* rhs_vec, const void* rhs_scalar, v
     IxFftArgs<T> ia{g, (const cplx<T>*)h->spec, (T*)p_out, h->px, twx<T>(h), (T)(1.0 / ((double)g.NX * g.NY))};
     launch_ixfft<T>(ia, h->st);
     if (mk) mark(h, 7, eb);
-    h->launches += 5 + (sizeof(T) == 4 ? 1 : 0);
+    h->launches += 6;
 }
 
 template <typename T>
@@ -1057,9 +1065,10 @@ extern "C" int tc_init_channel(tc_handle* h, int level, unsigned long long seed,
 // has no device memory left for a library to allocate, and a latency-critical time
 // loop cannot take cudaMalloc's implicit device-wide synchronisation.  This variant
 // takes the right-hand side and the result as device pointers in the handle's working
-// precision and runs the same launches as the step's pressure solve, with one change:
-// the z-solve's elimination coefficients live in a file-scope static device array
-// (below) instead of the handle's scratch buffer.
+// precision and runs the pressure solve's FFT launches around the z-solve that
+// eliminates every mode on the fly (launch_zsolve; the step path uses the factors
+// precomputed at creation instead); that elimination's coefficients live in a
+// file-scope static device array (below), not in a buffer of the handle.
 //
 // * Setup: the first call on a device looks the array up with cudaGetSymbolAddress
 //   (which may load this module into the context), so it should come before any

@@ -44,8 +44,9 @@ struct FftPlan {
     int fac[FFT_MAXF];
 };
 
+// aligned to its size so that loads and stores are single 8/16-byte accesses
 template <typename T>
-struct cplx {
+struct alignas(2 * sizeof(T)) cplx {
     T x, y;
 };
 
