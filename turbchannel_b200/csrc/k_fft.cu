@@ -1,0 +1,383 @@
+// k_fft.cu -- the pressure solve's FFT kernels for the lengths that have a compiled
+// two-pass register transform (fft_reg.cuh: 16 ... 1024 = 2^a 3^b); other lengths
+// keep the Stockham kernels of k_poisson.cu.  Same data layouts and results:
+//   k_div_quad     : divergence of the vector RHS (streaming, 16-byte row loads)
+//                    into a scratch real field;
+//   k_xfft_reg     : forward x-FFT of `rows` y-rows of a real field (the divergence
+//                    or the scalar RHS), two rows packed as one complex line,
+//                    unpacked to spec[z][kx][y] (kx = 0..NX/2);
+//   k_yfft_reg     : complex FFT of contiguous y-lines of spec, in place, straight
+//                    from and back to global memory;
+//   k_ixfft_reg    : Hermitian-extended half spectrum of two rows packed as one
+//                    complex line, inverse x-FFT, scaled real rows into p.
+#include <algorithm>
+
+#include "fft_reg.cuh"
+#include "kernels.cuh"
+#include "stencil_div.cuh"
+
+namespace tc {
+
+// ---------------------------------------------------------------------------
+// y-FFT
+// ---------------------------------------------------------------------------
+template <typename T, int N>
+constexpr int yfft_reg_lines() {
+    const int l = (512 / FftSplit<N>::N1) / (sizeof(T) == 8 ? 2 : 1);
+    return l < 1 ? 1 : l;
+}
+
+template <typename T, int N, int SIGN>
+__global__ void __launch_bounds__(256) k_yfft_reg(cplx<T>* spec, long long nlines, const cplx<T>* __restrict__ tw) {
+    constexpr int N1 = FftSplit<N>::N1, N2 = FftSplit<N>::N2, YL = FftSplit<N>::YL;
+    constexpr int LINES = yfft_reg_lines<T, N>();
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cplx<T>* Y = reinterpret_cast<cplx<T>*>(smraw);
+    const long long L0 = (long long)blockIdx.x * LINES;
+    const int nl = (int)min((long long)LINES, nlines - L0);
+    cplx<T>* base = spec + L0 * N;
+    for (int it = threadIdx.x; it < nl * N2; it += blockDim.x) {
+        const int l = it / N2, n2 = it - l * N2;
+        const cplx<T>* src = base + (size_t)l * N + n2;
+        cplx<T> v[N1];
+#pragma unroll
+        for (int n1 = 0; n1 < N1; n1++) v[n1] = src[n1 * N2];
+        fft_pass_a<T, N, SIGN>(v, n2, tw, Y + l * YL);
+    }
+    __syncthreads();
+    for (int it = threadIdx.x; it < nl * N1; it += blockDim.x) {
+        const int l = it / N1, k1 = it - l * N1;
+        cplx<T> v[N2];
+        fft_pass_b<T, N, SIGN>(v, k1, Y + l * YL);
+        cplx<T>* dst = base + (size_t)l * N + k1;
+#pragma unroll
+        for (int k2 = 0; k2 < N2; k2++) dst[k2 * N1] = v[k2];
+    }
+}
+
+template <typename T, int N>
+static void yfft_reg_launch(const YFftArgs<T>& a, cudaStream_t s) {
+    constexpr int LINES = yfft_reg_lines<T, N>();
+    const long long total = (long long)a.g.NZ * a.g.NXH;
+    const size_t smem = (size_t)LINES * FftSplit<N>::YL * sizeof(cplx<T>);
+    auto k = a.sign < 0 ? k_yfft_reg<T, N, -1> : k_yfft_reg<T, N, +1>;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k<<<(unsigned)((total + LINES - 1) / LINES), 256, smem, s>>>(a.spec, total, a.twy);
+}
+
+// ---------------------------------------------------------------------------
+// divergence of the vector RHS (streaming, 4 cells of a row per thread) and the
+// forward x-FFT of a real field
+// ---------------------------------------------------------------------------
+// Same expressions as div_at (stencil_div.cuh), evaluated for x..x+3 from 16-byte
+// row loads; NX % 4 == 0 (the periodic wrap then moves whole 4-cell chunks).
+template <typename T, int SCHEME>
+__global__ void __launch_bounds__(256) k_div_quad(DivFftArgs<T> a, T* __restrict__ out) {
+    const Geom& g = a.g;
+    const int NX = g.NX, NY = g.NY, NZ = g.NZ, NQ = NX >> 2;
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= (int)(g.N >> 2)) return;
+    const int row = q / NQ, x = (q - row * NQ) * 4;
+    const int y = row % NY, z = row / NY;
+    const size_t NXY = (size_t)NX * NY, pl = (size_t)z * NXY, rb = pl + (size_t)y * NX, id = rb + x;
+    const T *u = a.v.c[0], *v = a.v.c[1], *w = a.v.c[2];
+    const T ihx = (T)g.inv_hx, ihy = (T)g.inv_hy;
+    const int xq = x + 4 == NX ? 0 : x + 4, xm = x == 0 ? NX - 1 : x - 1;
+    const int yp = y + 1 == NY ? 0 : y + 1, ym = y == 0 ? NY - 1 : y - 1;
+    T e[9];  // u at x-1 .. x+7
+    {
+        const Acc4<T> U0 = ld4(u + id), U1 = ld4(u + rb + xq);
+        e[0] = __ldg(u + rb + xm);
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            e[1 + k] = U0.v[k];
+            e[5 + k] = U1.v[k];
+        }
+    }
+    T d[4];
+    if constexpr (SCHEME == TC_SCHEME_VV4) {
+        const T C27 = T(0.03703703703703703703);
+        const int ypp = yp + 1 == NY ? 0 : yp + 1;
+        const T dz = a.m.DZ[z], dzw = a.m.DZW[z];
+        const Acc4<T> V0 = ld4(v + id), Vp = ld4(v + pl + (size_t)yp * NX + x), Vpp = ld4(v + pl + (size_t)ypp * NX + x),
+                      Vm = ld4(v + pl + (size_t)ym * NX + x);
+        const Acc4<T> W0 = ld4(w + id);
+        Acc4<T> Wr, Wrr, Wll;
+        if (z == NZ - 1) {
+#pragma unroll
+            for (int k = 0; k < 4; k++) Wr.v[k] = T(0);
+            Wrr = W0;
+        } else {
+            Wr = ld4(w + id + NXY);
+            if (z == NZ - 2) {
+#pragma unroll
+                for (int k = 0; k < 4; k++) Wrr.v[k] = T(0);
+            } else {
+                Wrr = ld4(w + id + 2 * NXY);
+            }
+        }
+        if (z == 0) Wll = ld4(w + id + NXY);
+        else if (z == 1) {
+#pragma unroll
+            for (int k = 0; k < 4; k++) Wll.v[k] = T(0);
+        } else {
+            Wll = ld4(w + id - NXY);
+        }
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const T dudx = ihx * (dz * (e[k + 2] - e[k + 1]) - C27 * dzw * (e[k + 3] - e[k]));
+            const T dvdy = ihy * (dz * (Vp.v[k] - V0.v[k]) - C27 * dzw * (Vpp.v[k] - Vm.v[k]));
+            d[k] = dudx + dvdy + (Wr.v[k] - W0.v[k]) - C27 * (Wrr.v[k] - Wll.v[k]);
+        }
+    } else if constexpr (SCHEME == TC_SCHEME_HW2) {
+        const T hz = a.m.DZ[z];
+        const Acc4<T> V0 = ld4(v + id), Vp = ld4(v + pl + (size_t)yp * NX + x), W0 = ld4(w + id);
+        Acc4<T> Wr;
+        if (z < NZ - 1) Wr = ld4(w + id + NXY);
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+            d[k] = (e[k + 2] - e[k + 1]) * ihx * hz + (Vp.v[k] - V0.v[k]) * ihy * hz +
+                   ((z < NZ - 1) ? (Wr.v[k] - W0.v[k]) : (-W0.v[k]));
+    } else {
+        const T hz = a.m.cellh[z], hx = (T)g.hx, hy = (T)g.hy;
+        const Acc4<T> Vp = ld4(v + pl + (size_t)yp * NX + x), Vm = ld4(v + pl + (size_t)ym * NX + x);
+        Acc4<T> Wa, Wb;  // the two w planes of the z-difference
+        if (z == 0) {
+            Wa = ld4(w + id + NXY);
+            Wb = ld4(w + id);
+        } else if (z == NZ - 1) {
+            Wa = ld4(w + id);
+            Wb = ld4(w + id - NXY);
+        } else {
+            Wa = ld4(w + id + NXY);
+            Wb = ld4(w + id - NXY);
+        }
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            T dd = 0;
+            dd += T(0.5) * (e[k + 2] - e[k]) * hy * hz;
+            dd += T(0.5) * (Vp.v[k] - Vm.v[k]) * hx * hz;
+            dd += T(0.5) * (Wa.v[k] - Wb.v[k]) * hx * hy;
+            d[k] = dd;
+        }
+    }
+    if constexpr (sizeof(T) == 4) {
+        *reinterpret_cast<float4*>(out + id) = make_float4(d[0], d[1], d[2], d[3]);
+    } else {
+        reinterpret_cast<double2*>(out + id)[0] = make_double2(d[0], d[1]);
+        reinterpret_cast<double2*>(out + id)[1] = make_double2(d[2], d[3]);
+    }
+}
+
+template <typename T, int N>
+__global__ void __launch_bounds__(256, 2) k_xfft_reg(DivFftArgs<T> a, const T* __restrict__ src, int rows, int lrows) {
+    constexpr int N1 = FftSplit<N>::N1, N2 = FftSplit<N>::N2, YL = FftSplit<N>::YL, ZS = N + 1;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const Geom& g = a.g;
+    const int NY = g.NY, NXH = N / 2 + 1, nl = rows >> 1;
+    cplx<T>* Y = reinterpret_cast<cplx<T>*>(smraw);
+    cplx<T>* Zs = Y + nl * YL;  // transformed lines, stride N+1
+    const int z = blockIdx.y, y0 = blockIdx.x * rows;
+    const T* plane = src + ((size_t)z * NY + y0) * N;
+    for (int it = threadIdx.x; it < nl * N2; it += blockDim.x) {
+        const int l = it / N2, n2 = it - l * N2;
+        const T* d0 = plane + (size_t)(2 * l) * N + n2;
+        cplx<T> v[N1];
+#pragma unroll
+        for (int n1 = 0; n1 < N1; n1++) v[n1] = {__ldg(d0 + n1 * N2), __ldg(d0 + N + n1 * N2)};
+        fft_pass_a<T, N, -1>(v, n2, a.twx, Y + l * YL);
+    }
+    __syncthreads();
+    for (int it = threadIdx.x; it < nl * N1; it += blockDim.x) {
+        const int l = it / N1, k1 = it - l * N1;
+        cplx<T> v[N2];
+        fft_pass_b<T, N, -1>(v, k1, Y + l * YL);
+        cplx<T>* zl = Zs + l * ZS + k1;
+#pragma unroll
+        for (int k2 = 0; k2 < N2; k2++) zl[k2 * N1] = v[k2];
+    }
+    __syncthreads();
+    // unpack the two real rows of each line: X_a = (Z_k + conj Z_{N-k}) / 2, X_b = (Z_k - conj Z_{N-k}) / 2i
+    for (int e = threadIdx.x; e < NXH * rows; e += blockDim.x) {
+        const int kx = e >> lrows, r = e & (rows - 1), l = r >> 1;
+        const cplx<T> Zk = Zs[l * ZS + kx], Zm = Zs[l * ZS + (kx == 0 ? 0 : N - kx)];
+        cplx<T> val;
+        if ((r & 1) == 0) val = {T(0.5) * (Zk.x + Zm.x), T(0.5) * (Zk.y - Zm.y)};
+        else val = {T(0.5) * (Zk.y + Zm.y), -T(0.5) * (Zk.x - Zm.x)};
+        a.spec[((size_t)z * NXH + kx) * NY + y0 + r] = val;
+    }
+}
+
+template <typename T, int N>
+static size_t div_xfft_reg_smem(int rows) {
+    return (size_t)(rows / 2) * (FftSplit<N>::YL + N + 1) * sizeof(cplx<T>);
+}
+
+template <typename T, int N>
+static void xfft_reg_launch(const DivFftArgs<T>& a, const T* src, int rows, cudaStream_t s) {
+    const size_t smem = div_xfft_reg_smem<T, N>(rows);
+    int lr = 0;
+    while ((1 << lr) < rows) lr++;
+    auto k = k_xfft_reg<T, N>;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k<<<dim3(a.g.NY / rows, a.g.NZ), 256, smem, s>>>(a, src, rows, lr);
+}
+
+template <typename T>
+static void div_quad_launch(const DivFftArgs<T>& a, T* out, cudaStream_t s) {
+    const unsigned nb = (unsigned)(((a.g.N >> 2) + 255) / 256);
+    if (a.g.scheme == TC_SCHEME_VV4) k_div_quad<T, TC_SCHEME_VV4><<<nb, 256, 0, s>>>(a, out);
+    else if (a.g.scheme == TC_SCHEME_HW2) k_div_quad<T, TC_SCHEME_HW2><<<nb, 256, 0, s>>>(a, out);
+    else k_div_quad<T, TC_SCHEME_COLLOC><<<nb, 256, 0, s>>>(a, out);
+}
+
+// ---------------------------------------------------------------------------
+// inverse x-FFT
+// ---------------------------------------------------------------------------
+template <typename T, int N>
+__global__ void __launch_bounds__(256) k_ixfft_reg(IxFftArgs<T> a, int rows, int lrows) {
+    constexpr int N1 = FftSplit<N>::N1, N2 = FftSplit<N>::N2, YL = FftSplit<N>::YL, NH = N / 2, NXH = NH + 1;
+    constexpr int PC = 16 / sizeof(cplx<T>);  // complex values per 16-byte chunk
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const Geom& g = a.g;
+    const int NY = g.NY, nl = rows >> 1, TS = rows + 2;
+    cplx<T>* tile = reinterpret_cast<cplx<T>*>(smraw);  // tile[kx * TS + r]
+    cplx<T>* Y = tile + NXH * TS;
+    const int z = blockIdx.y, y0 = blockIdx.x * rows;
+    {
+        const int cpr = rows / PC, lc = lrows - (PC == 2 ? 1 : 0);
+        for (int e = threadIdx.x; e < NXH * cpr; e += blockDim.x) {
+            const int kx = e >> lc, c = e & (cpr - 1);
+            cp_async<16>(tile + kx * TS + c * PC, a.spec + ((size_t)z * NXH + kx) * NY + y0 + c * PC);
+        }
+        cp_async_commit();
+        cp_async_wait<0>();
+    }
+    __syncthreads();
+    for (int it = threadIdx.x; it < nl * N2; it += blockDim.x) {
+        const int l = it / N2, n2 = it - l * N2;
+        cplx<T> v[N1];
+#pragma unroll
+        for (int n1 = 0; n1 < N1; n1++) {
+            const int k = N2 * n1 + n2;
+            const bool up = k > NH;
+            const cplx<T>* t = tile + (up ? N - k : k) * TS + 2 * l;
+            cplx<T> av = t[0], bv = t[1];
+            if (up) {
+                av.y = -av.y;
+                bv.y = -bv.y;
+            }
+            if (k == 0 || k == NH) {
+                av.y = 0;
+                bv.y = 0;
+            }
+            v[n1] = {av.x - bv.y, av.y + bv.x};
+        }
+        fft_pass_a<T, N, +1>(v, n2, a.twx, Y + l * YL);
+    }
+    __syncthreads();
+    const T sc = a.scale;
+    for (int it = threadIdx.x; it < nl * N1; it += blockDim.x) {
+        const int l = it / N1, k1 = it - l * N1;
+        cplx<T> v[N2];
+        fft_pass_b<T, N, +1>(v, k1, Y + l * YL);
+        T* pa = a.p + ((size_t)z * NY + y0 + 2 * l) * N + k1;
+        T* pb = pa + N;
+#pragma unroll
+        for (int k2 = 0; k2 < N2; k2++) {
+            pa[k2 * N1] = v[k2].x * sc;
+            pb[k2 * N1] = v[k2].y * sc;
+        }
+    }
+}
+
+template <typename T, int N>
+static size_t ixfft_reg_smem(int rows) {
+    return ((size_t)(N / 2 + 1) * (rows + 2) + (size_t)(rows / 2) * FftSplit<N>::YL) * sizeof(cplx<T>);
+}
+
+template <typename T, int N>
+static void ixfft_reg_launch(const IxFftArgs<T>& a, int rows, cudaStream_t s) {
+    const size_t smem = ixfft_reg_smem<T, N>(rows);
+    int lr = 0;
+    while ((1 << lr) < rows) lr++;
+    auto k = k_ixfft_reg<T, N>;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k<<<dim3(a.g.NY / rows, a.g.NZ), 256, smem, s>>>(a, rows, lr);
+}
+
+// ---------------------------------------------------------------------------
+// dispatch on the transform length
+// ---------------------------------------------------------------------------
+// Rows per CTA of the x-FFT kernels: the largest of 32, 16, 8 that divides NY and
+// whose shared memory stays within 110 KB (two CTAs per SM); 0 if none.
+template <typename T, int N>
+static int xfft_reg_rows(int NY, bool inverse) {
+    for (int r : {32, 16, 8}) {
+        if (NY % r) continue;
+        const size_t sm = inverse ? ixfft_reg_smem<T, N>(r) : div_xfft_reg_smem<T, N>(r);
+        if (sm <= 110 * 1024) return r;
+    }
+    return 0;
+}
+
+#define TC_FFT_SIZES(X) X(16) X(24) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(384) X(512) X(768) X(1024)
+
+template <typename T>
+bool launch_yfft_reg(const YFftArgs<T>& a, cudaStream_t s) {
+    switch (a.g.NY) {
+#define TC_CASE(n)                  \
+    case n:                         \
+        yfft_reg_launch<T, n>(a, s); \
+        return true;
+        TC_FFT_SIZES(TC_CASE)
+#undef TC_CASE
+        default: return false;
+    }
+}
+
+// The vector RHS first goes through k_div_quad into a.dtmp (needs NX % 4 == 0 and a
+// scratch buffer), then the real field is transformed.
+template <typename T>
+int launch_div_xfft_reg(const DivFftArgs<T>& a, cudaStream_t s) {
+    const bool vec = a.src_scalar == nullptr;
+    if (vec && (a.dtmp == nullptr || a.g.NX % 4 != 0)) return 0;
+    switch (a.g.NX) {
+#define TC_CASE(n)                                           \
+    case n: {                                                \
+        const int rows = xfft_reg_rows<T, n>(a.g.NY, false); \
+        if (!rows) return 0;                                 \
+        if (vec) div_quad_launch<T>(a, a.dtmp, s);           \
+        xfft_reg_launch<T, n>(a, vec ? a.dtmp : a.src_scalar, rows, s); \
+        return vec ? 2 : 1;                                  \
+    }
+        TC_FFT_SIZES(TC_CASE)
+#undef TC_CASE
+        default: return 0;
+    }
+}
+
+template <typename T>
+bool launch_ixfft_reg(const IxFftArgs<T>& a, cudaStream_t s) {
+    switch (a.g.NX) {
+#define TC_CASE(n)                                          \
+    case n: {                                               \
+        const int rows = xfft_reg_rows<T, n>(a.g.NY, true); \
+        if (!rows) return false;                            \
+        ixfft_reg_launch<T, n>(a, rows, s);                 \
+        return true;                                        \
+    }
+        TC_FFT_SIZES(TC_CASE)
+#undef TC_CASE
+        default: return false;
+    }
+}
+
+template bool launch_yfft_reg<double>(const YFftArgs<double>&, cudaStream_t);
+template bool launch_yfft_reg<float>(const YFftArgs<float>&, cudaStream_t);
+template int launch_div_xfft_reg<double>(const DivFftArgs<double>&, cudaStream_t);
+template int launch_div_xfft_reg<float>(const DivFftArgs<float>&, cudaStream_t);
+template bool launch_ixfft_reg<double>(const IxFftArgs<double>&, cudaStream_t);
+template bool launch_ixfft_reg<float>(const IxFftArgs<float>&, cudaStream_t);
+
+}  // namespace tc

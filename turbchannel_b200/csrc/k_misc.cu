@@ -254,24 +254,6 @@ static_assert(NDIAG + 3 == TC_DIAG_STRIDE, "diagnostics layout");
 // are multiples of 4 cells (NX*NY is), read as 16-byte vectors of 4 cells, so each
 // thread keeps 5-6 vector loads in flight per iteration.
 template <typename T>
-struct Acc4 {
-    T v[4];
-};
-template <typename T>
-__device__ __forceinline__ Acc4<T> ld4(const T* p) {
-    Acc4<T> r;
-    if constexpr (sizeof(T) == 4) {
-        const float4 q = __ldg(reinterpret_cast<const float4*>(p));
-        r.v[0] = q.x; r.v[1] = q.y; r.v[2] = q.z; r.v[3] = q.w;
-    } else {
-        const double2 q0 = __ldg(reinterpret_cast<const double2*>(p));
-        const double2 q1 = __ldg(reinterpret_cast<const double2*>(p) + 1);
-        r.v[0] = q0.x; r.v[1] = q0.y; r.v[2] = q1.x; r.v[3] = q1.y;
-    }
-    return r;
-}
-
-template <typename T>
 __global__ void __launch_bounds__(256) k_diag(DiagArgs<T> a, double* part, int S) {
     const Geom& g = a.g;
     const int z = blockIdx.x, s = blockIdx.y;

@@ -61,7 +61,8 @@ static int pick_rows(int NX, int NY, size_t cbytes) {
 }
 
 template <typename T>
-void launch_div_xfft(const DivFftArgs<T>& a, cudaStream_t s) {
+int launch_div_xfft(const DivFftArgs<T>& a, cudaStream_t s) {
+    if (const int n = launch_div_xfft_reg<T>(a, s)) return n;
     const int rows = pick_rows(a.g.NX, a.g.NY, sizeof(cplx<T>));
     const size_t smem = (size_t)rows * a.g.NX * sizeof(cplx<T>);
     dim3 grid(a.g.NY / rows, a.g.NZ);
@@ -76,6 +77,7 @@ void launch_div_xfft(const DivFftArgs<T>& a, cudaStream_t s) {
     else if (a.g.scheme == TC_SCHEME_VV4) TC_LDX(TC_SCHEME_VV4, false)
     else TC_LDX(TC_SCHEME_COLLOC, false)
 #undef TC_LDX
+    return 1;
 }
 
 // ---------------------------------------------------------------------------
@@ -105,6 +107,7 @@ __global__ void __launch_bounds__(256) k_yfft(YFftArgs<T> a, int lines) {
 
 template <typename T>
 void launch_yfft(const YFftArgs<T>& a, cudaStream_t s) {
+    if (launch_yfft_reg<T>(a, s)) return;
     int lines = std::max(1, std::min(16, 4096 / a.g.NY));
     while (lines > 1 && (size_t)2 * lines * a.g.NY * sizeof(cplx<T>) > 96 * 1024) lines >>= 1;
     const size_t smem = (size_t)2 * lines * a.g.NY * sizeof(cplx<T>);
@@ -791,6 +794,7 @@ __global__ void __launch_bounds__(256) k_ixfft(IxFftArgs<T> a) {
 
 template <typename T>
 void launch_ixfft(const IxFftArgs<T>& a, cudaStream_t s) {
+    if (launch_ixfft_reg<T>(a, s)) return;
     const int rows = pick_rows(a.g.NX, a.g.NY, sizeof(cplx<T>));
     const size_t nl = rows / 2;
     const size_t smem = (nl * a.g.NX + std::max(nl * a.g.NX, (size_t)rows * a.g.NXH)) * sizeof(cplx<T>);
@@ -799,8 +803,8 @@ void launch_ixfft(const IxFftArgs<T>& a, cudaStream_t s) {
     k<<<dim3(a.g.NY / rows, a.g.NZ), 256, smem, s>>>(a);
 }
 
-template void launch_div_xfft<double>(const DivFftArgs<double>&, cudaStream_t);
-template void launch_div_xfft<float>(const DivFftArgs<float>&, cudaStream_t);
+template int launch_div_xfft<double>(const DivFftArgs<double>&, cudaStream_t);
+template int launch_div_xfft<float>(const DivFftArgs<float>&, cudaStream_t);
 template void launch_yfft<double>(const YFftArgs<double>&, cudaStream_t);
 template void launch_yfft<float>(const YFftArgs<float>&, cudaStream_t);
 template void launch_zsolve<double>(const ZSolveArgs<double>&, cudaStream_t, cudaStream_t, cudaEvent_t, cudaEvent_t);

@@ -48,6 +48,7 @@ struct DivFftArgs {
     cplx<T>* spec;
     FftPlan px;
     const cplx<T>* twx;
+    T* dtmp = nullptr;  // N-cell scratch for the divergence (the pressure output, free until the inverse FFT)
 };
 
 // In-place complex FFT along y of the lines spec[z][kx][0..NY).
@@ -137,7 +138,7 @@ constexpr int TC_DIAG_STRIDE = 19;
 
 template <typename T> void launch_flux_stag(const FluxArgs<T>& a, cudaStream_t s);
 template <typename T> void launch_flux_coll(const FluxArgs<T>& a, cudaStream_t s);
-template <typename T> void launch_div_xfft(const DivFftArgs<T>& a, cudaStream_t s);
+template <typename T> int launch_div_xfft(const DivFftArgs<T>& a, cudaStream_t s);  // returns launches
 template <typename T> void launch_yfft(const YFftArgs<T>& a, cudaStream_t s);
 template <typename T> void launch_zsolve(const ZSolveArgs<T>& a, cudaStream_t s, cudaStream_t side, cudaEvent_t fork,
                                        cudaEvent_t join);
@@ -146,6 +147,10 @@ template <typename T> void launch_zfactor(const ZSolveArgs<T>& a, cudaStream_t s
 template <typename T> void launch_zsolve_fac(const ZSolveArgs<T>& a, cudaStream_t s, cudaStream_t side,
                                            cudaEvent_t fork, cudaEvent_t join);
 template <typename T> void launch_ixfft(const IxFftArgs<T>& a, cudaStream_t s);
+// two-pass register FFT versions (k_fft.cu); false when the length has none
+template <typename T> int launch_div_xfft_reg(const DivFftArgs<T>& a, cudaStream_t s);  // 0: no such path
+template <typename T> bool launch_yfft_reg(const YFftArgs<T>& a, cudaStream_t s);
+template <typename T> bool launch_ixfft_reg(const IxFftArgs<T>& a, cudaStream_t s);
 template <typename T> void launch_correct(const CorrArgs<T>& a, cudaStream_t s);
 template <typename T> void launch_turb(const TurbArgs<T>& a, cudaStream_t s);
 template <typename T> void launch_divergence(const DivArgs<T>& a, cudaStream_t s);

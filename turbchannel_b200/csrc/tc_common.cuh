@@ -50,6 +50,26 @@ struct alignas(2 * sizeof(T)) cplx {
     T x, y;
 };
 
+// four consecutive elements as one (float) or two (double) 16-byte read-only loads;
+// the address must be 16-byte aligned
+template <typename T>
+struct Acc4 {
+    T v[4];
+};
+template <typename T>
+__device__ __forceinline__ Acc4<T> ld4(const T* p) {
+    Acc4<T> r;
+    if constexpr (sizeof(T) == 4) {
+        const float4 q = __ldg(reinterpret_cast<const float4*>(p));
+        r.v[0] = q.x; r.v[1] = q.y; r.v[2] = q.z; r.v[3] = q.w;
+    } else {
+        const double2 q0 = __ldg(reinterpret_cast<const double2*>(p));
+        const double2 q1 = __ldg(reinterpret_cast<const double2*>(p) + 1);
+        r.v[0] = q0.x; r.v[1] = q0.y; r.v[2] = q1.x; r.v[3] = q1.y;
+    }
+    return r;
+}
+
 template <typename T>
 __host__ __device__ __forceinline__ cplx<T> cmul(cplx<T> a, cplx<T> b) {
     return {a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
