@@ -116,6 +116,99 @@ __global__ void __launch_bounds__(KX* KY) k_correct(CorrArgs<T> a, int tz) {
     }
 }
 
+// The step's correction with four x-adjacent cells per thread (NX % 4 == 0): the
+// pressure row x-4..x+7, the y-neighbour rows and the RHS are read as 16-byte
+// vectors (the periodic wrap moves whole 4-cell chunks), so a thread issues about a
+// quarter of the load instructions of k_correct.  Same expressions as k_correct.
+constexpr int QX = 32, QY = 8;  // quads x rows per CTA
+template <typename T>
+__device__ __forceinline__ void st4(T* p, const T v[4]) {
+    if constexpr (sizeof(T) == 4) {
+        *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+    } else {
+        reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
+        reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
+    }
+}
+
+// ZN planes per thread: 2 for float, 1 for double (register budget).
+template <typename T>
+constexpr int correct_quad_planes() { return sizeof(T) == 4 ? 2 : 1; }
+
+template <typename T, int SCHEME, bool STAB1>
+__global__ void __launch_bounds__(QX* QY) k_correct_quad(CorrArgs<T> a) {
+    constexpr int ZN = correct_quad_planes<T>();
+    const Geom& g = a.g;
+    const int NX = g.NX, NY = g.NY, NZ = g.NZ, NQ = NX >> 2;
+    const size_t NXY = (size_t)NX * NY;
+    const int xq = blockIdx.x * QX + threadIdx.x % QX, iy = blockIdx.y * QY + threadIdx.x / QX;
+    if (xq >= NQ || iy >= NY) return;
+    const int x = 4 * xq, zb = blockIdx.z * ZN;
+    const int xl = x == 0 ? NX - 4 : x - 4, xr = x + 4 == NX ? 0 : x + 4;
+    const int ym = wrapi(iy - 1, NY), ymm = wrapi(iy - 2, NY), yp = wrapi(iy + 1, NY);
+    const T* __restrict__ p = a.p;
+    T du = 0;
+    if (a.cfr) {
+        const double ub = (*a.ub_sum) * a.cfr_scale * (double)a.tob;
+        const double d = (a.cfr_target - ub) * a.cfr_volfac;
+        du = (T)d;
+        if (blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0) *a.du_out = d;
+    }
+    const size_t row = (size_t)iy * NX;
+    Acc4<T> col[ZN + 3];  // p(zb-2 .. zb+ZN) at x..x+3; zero outside the domain (never used there)
+#pragma unroll
+    for (int k = 0; k < ZN + 3; k++) {
+        const int z = zb - 2 + k;
+        if (z >= 0 && z < NZ) col[k] = ld4(p + (size_t)z * NXY + row + x);
+        else {
+#pragma unroll
+            for (int j = 0; j < 4; j++) col[k].v[j] = T(0);
+        }
+    }
+    Acc4<T> pl4[ZN], pr4[ZN], pym[ZN], pymm[ZN], pyp[ZN], rh[ZN][3], pc[ZN];
+#pragma unroll
+    for (int k = 0; k < ZN; k++) {
+        const int z = zb + k;
+        if (z >= NZ) break;
+        const size_t pl = (size_t)z * NXY;
+        pl4[k] = ld4(p + pl + row + xl);
+        pr4[k] = ld4(p + pl + row + xr);
+        pym[k] = ld4(p + pl + (size_t)ym * NX + x);
+        pymm[k] = ld4(p + pl + (size_t)ymm * NX + x);
+        pyp[k] = ld4(p + pl + (size_t)yp * NX + x);
+#pragma unroll
+        for (int c = 0; c < 3; c++) rh[k][c] = ld4(a.rhs.c[c] + pl + row + x);
+        if (STAB1) pc[k] = ld4(a.pcur + pl + row + x);
+    }
+#pragma unroll
+    for (int k = 0; k < ZN; k++) {
+        const int z = zb + k;
+        if (z >= NZ) break;
+        const size_t id = (size_t)z * NXY + row + x;
+        T e[12];  // p at x-4 .. x+7 on plane z
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            e[j] = pl4[k].v[j];
+            e[4 + j] = col[k + 2].v[j];
+            e[8 + j] = pr4[k].v[j];
+        }
+        T o[3][4], pn[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            T gp[3];
+            grad_at<T, SCHEME>(a, z, NZ, e[4 + j], e[3 + j], e[2 + j], e[5 + j], pym[k].v[j], pymm[k].v[j], pyp[k].v[j],
+                               col[k + 1].v[j], col[k].v[j], col[k + 3].v[j], gp);
+#pragma unroll
+            for (int c = 0; c < 3; c++) o[c][j] = (rh[k][c].v[j] - gp[c]) * a.tob;
+            if (a.cfr && !(SCHEME == TC_SCHEME_COLLOC && (z == 0 || z == NZ - 1))) o[0][j] += du;
+            if (STAB1) pn[j] = col[k + 2].v[j] + pc[k].v[j];
+        }
+#pragma unroll
+        for (int c = 0; c < 3; c++) st4(a.vout.c[c] + id, o[c]);
+        if (STAB1) st4(a.pnext + id, pn);
+    }
+}
+
 static void column_shape(const Geom& g, dim3& grid, int& tz) {
     tz = ZC;
     grid = dim3((g.NX + KX - 1) / KX, (g.NY + KY - 1) / KY, (g.NZ + tz - 1) / tz);
@@ -123,6 +216,13 @@ static void column_shape(const Geom& g, dim3& grid, int& tz) {
 
 template <typename T, int SCHEME>
 static void correct_scheme(const CorrArgs<T>& a, cudaStream_t s) {
+    if (!a.grad_only && a.g.NX % 4 == 0) {
+        constexpr int ZN = correct_quad_planes<T>();
+        const dim3 gq((a.g.NX / 4 + QX - 1) / QX, (a.g.NY + QY - 1) / QY, (a.g.NZ + ZN - 1) / ZN);
+        if (a.pnext) k_correct_quad<T, SCHEME, true><<<gq, QX * QY, 0, s>>>(a);
+        else k_correct_quad<T, SCHEME, false><<<gq, QX * QY, 0, s>>>(a);
+        return;
+    }
     dim3 grid;
     int tz;
     column_shape(a.g, grid, tz);

@@ -480,10 +480,12 @@ void launch_zsolve(const ZSolveArgs<T>& a, cudaStream_t s, cudaStream_t side, cu
 // stored in the working precision T as
 //   forward   z_i = F0_i r_i - F1_i z_{i-1} - F2_i z_{i-2} - F3_i z_{i-3}
 //   backward  x_i = z_i - B0_i x_{i+1} - B1_i x_{i+2} - B2_i x_{i+3}
-// (tridiagonal schemes: F0, F1, B0).  Layout: VV4 F[i][m] = {F0,F1,F2,F3} then
-// B[i][m] = {B0,B1,B2,0}; tridiagonal F[i][m] = {F0,F1} then B[i][m] = B0.  The
-// per-step solve then streams r, F, B with no divide and a one-FMA recurrence
-// chain, so many rows of loads are in flight per thread.
+// (tridiagonal schemes: F0, F1, B0).  The matrix of mode (kx, ky) depends on ky only
+// through cos(2 pi ky/NY) or sin^2(pi ky/NY), so ky and NY-ky share their factors:
+// they are stored for kh = 0..NY/2 (mode index mh = kx*(NY/2+1) + kh).  Layout: VV4
+// F[i][mh] = {F0,F1,F2,F3} then B[i][mh] = {B0,B1,B2,0}; tridiagonal F[i][mh] =
+// {F0,F1} then B[i][mh] = B0.  The per-step solve streams r, F, B with no divide and
+// a one-FMA recurrence chain, one thread per pair (ky, NY-ky) reading the factors once.
 // ---------------------------------------------------------------------------
 template <typename T>
 struct alignas(4 * sizeof(T)) Q4 {
@@ -496,16 +498,17 @@ struct alignas(2 * sizeof(T)) Q2 {
 
 size_t zfactor_bytes(const Geom& g, int elem_bytes) {
     const size_t per = g.scheme == TC_SCHEME_VV4 ? 8 : 3;
-    return (size_t)g.NXH * g.NY * g.NZ * per * elem_bytes;
+    return (size_t)g.NXH * (g.NY / 2 + 1) * g.NZ * per * elem_bytes;
 }
 
 template <typename T, int SCHEME>
 __global__ void __launch_bounds__(128) k_zfactor(ZSolveArgs<T> a) {
     const Geom& g = a.g;
-    const size_t M = (size_t)g.NXH * g.NY;
+    const int NYH1 = g.NY / 2 + 1;
+    const size_t M = (size_t)g.NXH * NYH1;  // factor modes (kx, ky <= NY/2)
     const size_t m = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= M) return;
-    const int kx = (int)(m / g.NY), ky = (int)(m - (size_t)kx * g.NY);
+    const int kx = (int)(m / NYH1), ky = (int)(m - (size_t)kx * NYH1);
     const int NZ = g.NZ;
     const bool pin = (kx == 0 && ky == 0);
     const double* MA = a.m.dMAT_A;
@@ -606,14 +609,16 @@ __global__ void __launch_bounds__(128) k_zfactor(ZSolveArgs<T> a) {
 
 template <typename T>
 void launch_zfactor(const ZSolveArgs<T>& a, cudaStream_t s) {
-    const size_t M = (size_t)a.g.NXH * a.g.NY;
+    const size_t M = (size_t)a.g.NXH * (a.g.NY / 2 + 1);
     const unsigned nb = (unsigned)((M + 127) / 128);
     if (a.g.scheme == TC_SCHEME_VV4) k_zfactor<T, TC_SCHEME_VV4><<<nb, 128, 0, s>>>(a);
     else if (a.g.scheme == TC_SCHEME_HW2) k_zfactor<T, TC_SCHEME_HW2><<<nb, 128, 0, s>>>(a);
     else k_zfactor<T, TC_SCHEME_COLLOC><<<nb, 128, 0, s>>>(a);
 }
 
-// One thread per mode outside the low set.  Rows are moved R at a time through two
+// One thread per mode outside the low set.  Adjacent lanes take the two modes
+// (kx, kh), (kx, NY-kh) that share their factors, so a warp's factor loads fetch each
+// factor row once (two lanes, one address).  Rows are moved R at a time through two
 // register batches: the loads of batch b+1 are issued before batch b is consumed.
 template <typename T, int SCHEME>
 __global__ void __launch_bounds__(128) k_zsolve_fac(ZSolveArgs<T> a) {
@@ -622,16 +627,20 @@ __global__ void __launch_bounds__(128) k_zsolve_fac(ZSolveArgs<T> a) {
     using FQ = typename std::conditional<VV, Q4<T>, Q2<T>>::type;
     using BQ = typename std::conditional<VV, Q4<T>, T>::type;
     const Geom& g = a.g;
-    const size_t M = (size_t)g.NXH * g.NY;
-    const size_t m = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (m >= M) return;
-    const int kx = (int)(m / g.NY), ky = (int)(m - (size_t)kx * g.NY);
+    const int NY = g.NY, NYH1 = NY / 2 + 1;
+    const size_t M = (size_t)g.NXH * NY, MH = (size_t)g.NXH * NYH1;
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t mh = t >> 1;
+    if (mh >= MH) return;
+    const int kx = (int)(mh / NYH1), kh = (int)(mh - (size_t)kx * NYH1);
+    if ((t & 1) && (kh == 0 || 2 * kh == NY)) return;  // no partner mode
     const int LM = g.low_modes;
-    if (kx < LM && (ky < LM || ky > g.NY - LM)) return;
+    if (kx < LM && kh < LM) return;
+    const int ky = (t & 1) ? NY - kh : kh;
     const int NZ = g.NZ;
-    const FQ* F = reinterpret_cast<const FQ*>(a.fac) + m;
-    const BQ* B = reinterpret_cast<const BQ*>(reinterpret_cast<const FQ*>(a.fac) + (size_t)NZ * M) + m;
-    cplx<T>* x = a.spec + m;
+    const FQ* F = reinterpret_cast<const FQ*>(a.fac) + mh;
+    const BQ* B = reinterpret_cast<const BQ*>(reinterpret_cast<const FQ*>(a.fac) + (size_t)NZ * MH) + mh;
+    cplx<T>* x = a.spec + (size_t)kx * NY + ky;
 
     // forward
     {
@@ -643,7 +652,7 @@ __global__ void __launch_bounds__(128) k_zsolve_fac(ZSolveArgs<T> a) {
             for (int k = 0; k < R; k++)
                 if (i0 + k < NZ) {
                     r[k] = x[(size_t)(i0 + k) * M];
-                    f[k] = F[(size_t)(i0 + k) * M];
+                    f[k] = F[(size_t)(i0 + k) * MH];
                 }
         };
         auto run = [&](int i0, const cplx<T>(&r)[R], const FQ(&f)[R]) {
@@ -684,7 +693,7 @@ __global__ void __launch_bounds__(128) k_zsolve_fac(ZSolveArgs<T> a) {
             for (int k = 0; k < R; k++)
                 if (i0 - k >= 0) {
                     zz[k] = x[(size_t)(i0 - k) * M];
-                    bq[k] = B[(size_t)(i0 - k) * M];
+                    bq[k] = B[(size_t)(i0 - k) * MH];
                 }
         };
         auto run = [&](int i0, const cplx<T>(&zz)[R], const BQ(&bq)[R]) {
@@ -720,8 +729,7 @@ __global__ void __launch_bounds__(128) k_zsolve_fac(ZSolveArgs<T> a) {
 template <typename T, int SCHEME>
 static void zsolve_fac_scheme(const ZSolveArgs<T>& a, cudaStream_t s, cudaStream_t side, cudaEvent_t fork,
                               cudaEvent_t join) {
-    const size_t M = (size_t)a.g.NXH * a.g.NY;
-    // the low modes (exact elimination in double, mode (0,0) normalised) on a side
+        // the low modes (exact elimination in double, mode (0,0) normalised) on a side
     // stream next to the factored solve of all other modes; the two sets are disjoint
     cudaEventRecord(fork, s);
     cudaStreamWaitEvent(side, fork, 0);
@@ -733,7 +741,8 @@ static void zsolve_fac_scheme(const ZSolveArgs<T>& a, cudaStream_t s, cudaStream
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k<<<nlow, 128, smem, side>>>(a);
     cudaEventRecord(join, side);
-    k_zsolve_fac<T, SCHEME><<<(unsigned)((M + 127) / 128), 128, 0, s>>>(a);
+    const size_t MH = (size_t)a.g.NXH * (a.g.NY / 2 + 1);
+    k_zsolve_fac<T, SCHEME><<<(unsigned)((2 * MH + 127) / 128), 128, 0, s>>>(a);
     cudaStreamWaitEvent(s, join, 0);
 }
 
