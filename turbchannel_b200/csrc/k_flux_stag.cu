@@ -157,6 +157,7 @@ __global__ void __launch_bounds__(STX* STY, 2) k_flux_stag(FluxArgs<T> a, int tz
         cp_async_wait<1>();
         __syncthreads();
         mz.iz = z;
+        mz.pc = a.m.PC + TC_PC * z;
         const T gcz = SCHEME == TC_SCHEME_VV4 ? a.m.GCZ[z] : T(0);
         const bool inner = z >= zlo && z <= zhi;
 #pragma unroll

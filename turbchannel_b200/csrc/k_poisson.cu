@@ -496,6 +496,11 @@ struct alignas(2 * sizeof(T)) Q2 {
     T x, y;
 };
 
+size_t zfactor_low_bytes(const Geom& g) {
+    const size_t per = g.scheme == TC_SCHEME_VV4 ? 8 : 3;
+    return (size_t)g.low_modes * g.low_modes * g.NZ * per * sizeof(double);
+}
+
 size_t zfactor_bytes(const Geom& g, int elem_bytes) {
     const size_t per = g.scheme == TC_SCHEME_VV4 ? 8 : 3;
     return (size_t)g.NXH * (g.NY / 2 + 1) * g.NZ * per * elem_bytes;
@@ -511,6 +516,10 @@ __global__ void __launch_bounds__(128) k_zfactor(ZSolveArgs<T> a) {
     const int kx = (int)(m / NYH1), ky = (int)(m - (size_t)kx * NYH1);
     const int NZ = g.NZ;
     const bool pin = (kx == 0 && ky == 0);
+    // low modes (kx, ky < LM): a double copy, mode-major [jl][row], for k_zsolve_low
+    const int LM = g.low_modes;
+    const bool low = a.fac_low != nullptr && kx < LM && ky < LM;
+    const size_t jl = (size_t)kx * LM + ky;
     const double* MA = a.m.dMAT_A;
     const double* DZ = a.m.dDZ;
     const double* DZW = a.m.dDZW;
@@ -533,6 +542,12 @@ __global__ void __launch_bounds__(128) k_zfactor(ZSolveArgs<T> a) {
         double pp = MA[1] * ib0;
         F[m] = {(T)ib0, (T)0};
         B[m] = (T)pp;
+        Q2<double>* FL = reinterpret_cast<Q2<double>*>(a.fac_low) + jl * NZ;
+        double* BL = reinterpret_cast<double*>(reinterpret_cast<Q2<double>*>(a.fac_low) + (size_t)LM * LM * NZ) + jl * NZ;
+        if (low) {
+            FL[0] = {ib0, 0.0};
+            BL[0] = pp;
+        }
         for (int i = 1; i <= NZ - 1; i++) {
             double d;
             if (SCHEME == TC_SCHEME_HW2) {
@@ -549,10 +564,16 @@ __global__ void __launch_bounds__(128) k_zfactor(ZSolveArgs<T> a) {
             pp = i != NZ - 1 ? MA[i + 1] * d : 0.0;
             F[(size_t)i * M + m] = {(T)d, (T)(MA[i] * d)};
             B[(size_t)i * M + m] = (T)pp;
+            if (low) {
+                FL[i] = {d, MA[i] * d};
+                BL[i] = pp;
+            }
         }
     } else {
         Q4<T>* F = reinterpret_cast<Q4<T>*>(a.fac);
         Q4<T>* B = F + (size_t)NZ * M;
+        Q4<double>* FL = reinterpret_cast<Q4<double>*>(a.fac_low) + jl * NZ;
+        Q4<double>* BL = reinterpret_cast<Q4<double>*>(a.fac_low) + (size_t)LM * LM * NZ + jl * NZ;
         const double C27 = 0.03703703703703703703, C9 = 0.11111111111111111111;
         const double sx = a.tabs.sinx[kx], sy = a.tabs.siny[ky];
         const double s3x = 3 * sx - 4 * sx * sx * sx, s3y = 3 * sy - 4 * sy * sy * sy;
@@ -600,6 +621,10 @@ __global__ void __launch_bounds__(128) k_zfactor(ZSolveArgs<T> a) {
             for (int k = 1; k <= 3; k++) nb[k - 1] = (i + k >= NZ) ? 0.0 : row[3 + k] * inv;
             F[(size_t)i * M + m] = {(T)inv, (T)(used[2] * inv), (T)(used[1] * inv), (T)(used[0] * inv)};
             B[(size_t)i * M + m] = {(T)nb[0], (T)nb[1], (T)nb[2], (T)0};
+            if (low) {
+                FL[i] = {inv, used[2] * inv, used[1] * inv, used[0] * inv};
+                BL[i] = {nb[0], nb[1], nb[2], 0.0};
+            }
             for (int j = 0; j < 2; j++)
                 for (int k = 0; k < 3; k++) b[j][k] = b[j + 1][k];
             for (int k = 0; k < 3; k++) b[2][k] = nb[k];
@@ -726,6 +751,98 @@ __global__ void __launch_bounds__(128) k_zsolve_fac(ZSolveArgs<T> a) {
     }
 }
 
+// The low-|k| modes (kx < LM, |ky| < LM) in double from their double factors; mode
+// (0,0) also normalised.  One CTA per mode: the column and its factors are staged into
+// shared memory by all threads, one thread runs the two sweeps there (shared-memory
+// latency per row), all threads write the column back.
+template <typename T, int SCHEME>
+__global__ void __launch_bounds__(128) k_zsolve_low_fac(ZSolveArgs<T> a) {
+    constexpr bool VV = SCHEME == TC_SCHEME_VV4;
+    using FQ = typename std::conditional<VV, Q4<double>, Q2<double>>::type;
+    using BQ = typename std::conditional<VV, Q4<double>, double>::type;
+    extern __shared__ __align__(32) unsigned char smraw[];
+    const Geom& g = a.g;
+    const int LM = g.low_modes, nky = 2 * LM - 1;
+    const int idx = blockIdx.x;
+    const int kx = idx / nky, j = idx - kx * nky;
+    const int ky = j < LM ? j : g.NY - (j - LM + 1);
+    if (kx >= g.NXH || ky < 0 || ky >= g.NY) return;
+    const int kh = j < LM ? j : j - LM + 1;  // min(ky, NY - ky)
+    const int NZ = g.NZ;
+    const size_t M = (size_t)g.NXH * g.NY;
+    const size_t m = (size_t)kx * g.NY + ky;
+    const size_t jl = (size_t)kx * LM + kh;
+    // shared layout: F rows, B rows, then the column at a 32-byte boundary
+    FQ* sF = reinterpret_cast<FQ*>(smraw);
+    BQ* sB = reinterpret_cast<BQ*>(sF + NZ);
+    const size_t xo = ((size_t)NZ * (sizeof(FQ) + sizeof(BQ)) + 31) & ~(size_t)31;
+    cplx<double>* xs = reinterpret_cast<cplx<double>*>(smraw + xo);
+    const FQ* F = reinterpret_cast<const FQ*>(a.fac_low) + jl * NZ;
+    const BQ* B = reinterpret_cast<const BQ*>(reinterpret_cast<const FQ*>(a.fac_low) + (size_t)LM * LM * NZ) + jl * NZ;
+    for (int i = threadIdx.x; i < NZ; i += blockDim.x) {
+        const cplx<T> v = a.spec[(size_t)i * M + m];
+        xs[i] = {(double)v.x, (double)v.y};
+        sF[i] = F[i];
+        sB[i] = B[i];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        cplx<double> z1 = {0, 0}, z2 = {0, 0}, z3 = {0, 0};
+        for (int i = 0; i < NZ; i++) {
+            const FQ f = sF[i];
+            const cplx<double> r = xs[i];
+            cplx<double> z;
+            if constexpr (VV) {
+                z.x = r.x * f.x - f.w * z3.x - f.z * z2.x;
+                z.y = r.y * f.x - f.w * z3.y - f.z * z2.y;
+            } else {
+                z.x = r.x * f.x;
+                z.y = r.y * f.x;
+            }
+            z.x -= f.y * z1.x;
+            z.y -= f.y * z1.y;
+            xs[i] = z;
+            z3 = z2;
+            z2 = z1;
+            z1 = z;
+        }
+        cplx<double> x1 = {0, 0}, x2 = {0, 0}, x3 = {0, 0};
+        for (int i = NZ - 1; i >= 0; i--) {
+            const BQ b = sB[i];
+            const cplx<double> zz = xs[i];
+            cplx<double> v;
+            if constexpr (VV) {
+                v.x = zz.x - b.z * x3.x - b.y * x2.x;
+                v.y = zz.y - b.z * x3.y - b.y * x2.y;
+                v.x -= b.x * x1.x;
+                v.y -= b.x * x1.y;
+            } else {
+                v.x = zz.x - b * x1.x;
+                v.y = zz.y - b * x1.y;
+            }
+            xs[i] = v;
+            x3 = x2;
+            x2 = x1;
+            x1 = v;
+        }
+        if (m == 0) {
+            ZSolveArgs<double> b;
+            b.g = g;
+            b.g.NXH = 1;
+            b.g.NY = 1;  // a single column: stride 1 between z
+            b.m.dDZ = a.m.dDZ; b.m.dKERG = a.m.dKERG; b.m.dcellh = a.m.dcellh; b.m.dZZ = a.m.dZZ;
+            b.m.KERG_norm2 = a.m.KERG_norm2;
+            b.spec = xs;
+            normalize_mean_mode(b);
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < NZ; i += blockDim.x) {
+        const cplx<double> v = xs[i];
+        a.spec[(size_t)i * M + m] = {(T)v.x, (T)v.y};
+    }
+}
+
 template <typename T, int SCHEME>
 static void zsolve_fac_scheme(const ZSolveArgs<T>& a, cudaStream_t s, cudaStream_t side, cudaEvent_t fork,
                               cudaEvent_t join) {
@@ -734,10 +851,9 @@ static void zsolve_fac_scheme(const ZSolveArgs<T>& a, cudaStream_t s, cudaStream
     cudaEventRecord(fork, s);
     cudaStreamWaitEvent(side, fork, 0);
     const int nlow = a.g.low_modes * (2 * a.g.low_modes - 1);
-    const int nc = SCHEME == TC_SCHEME_VV4 ? 3 : 1;
-    const int nma = SCHEME == TC_SCHEME_VV4 ? 3 * a.g.NZ : a.g.NZ;
-    const size_t smem = (size_t)a.g.NZ * (sizeof(cplx<double>) + nc * sizeof(double)) + (size_t)(nma + 2 * a.g.NZ) * sizeof(double);
-    auto k = k_zsolve_low<T, SCHEME>;
+    const size_t smem = (((size_t)a.g.NZ * (SCHEME == TC_SCHEME_VV4 ? 64 : 24) + 31) & ~(size_t)31) +
+                        (size_t)a.g.NZ * sizeof(cplx<double>);
+    auto k = k_zsolve_low_fac<T, SCHEME>;
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k<<<nlow, 128, smem, side>>>(a);
     cudaEventRecord(join, side);

@@ -72,6 +72,7 @@ struct ZSolveArgs {
     void* scratch;  // per-mode elimination coefficients
     int* err_flag;  // set when a pivot underflows (the reference writes -1e50)
     void* fac = nullptr;  // precomputed factors (k_zfactor layout), zfactor_bytes()
+    void* fac_low = nullptr;  // double factors of the low modes, zfactor_low_bytes()
 };
 
 // Inverse real FFT along x: p = scale * C2R(spec) (+ dest layout [z][y][x]).
@@ -164,6 +165,7 @@ template <typename T> void launch_t2d(const T* src, double* dst, long long n, cu
 
 size_t zsolve_scratch_bytes(const Geom& g, int elem_bytes);
 size_t zfactor_bytes(const Geom& g, int elem_bytes);
+size_t zfactor_low_bytes(const Geom& g);
 int diag_chunks(const Geom& g);
 int flux_grid_blocks(const Geom& g);
 

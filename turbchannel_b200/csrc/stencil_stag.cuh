@@ -24,6 +24,7 @@ struct StagZ {  // wall-normal metric at the current plane
     const T* DZ;
     const T* DZW;
     T hx, hy, ihx, ihy, visc;
+    const T* pc;  // MeshDev::PC + TC_PC * iz
 };
 
 template <typename T, typename ACC, bool INT = false>
@@ -33,8 +34,8 @@ __device__ __forceinline__ void conv_hw2(const ACC& A, const StagZ<T>& m, T s[3]
 #define W(a, b, c) A(2, a, b, c)
     const int iz = m.iz, NZ = m.NZ;
     const T* DZ = m.DZ;
-    const T inv_hz = T(1) / DZ[iz];
-    const T inv_hz_alt = T(2) / (DZ[iz] + ((!INT && iz == 0) ? T(0) : DZ[iz - 1]));
+    const T inv_hz = m.pc[0];
+    const T inv_hz_alt = m.pc[1];
     const T U0 = U(0, 0, 0), V0 = V(0, 0, 0), W0 = W(0, 0, 0);
     s[0] = s[1] = s[2] = 0;
     T a = U0 + U(1, 0, 0), c = U0 + U(-1, 0, 0);
@@ -198,18 +199,18 @@ __device__ __forceinline__ void conv_vv4(const ACC& A, const StagZ<T>& m, T gcz,
             else s[2] += C27 * bbl * (W(0, 0, 1) + W0);
         }
     }
-    const T miv = T(-1) / (32 * (dz - C9 * dzw) * hx * hy);
+    const T miv = m.pc[4];
     s[0] *= miv;
     s[1] *= miv;
-    s[2] *= (-T(1. / 32.) * m.ihx * m.ihy * gcz);
+    s[2] *= m.pc[5];
 }
 
 template <typename T, typename ACC, bool INT = false>
 __device__ __forceinline__ void visc_cross(const ACC& A, const StagZ<T>& m, T s[3]) {
     const int iz = m.iz, NZ = m.NZ;
     const T* DZ = m.DZ;
-    const T inv_hz = T(1) / DZ[iz];
-    const T inv_hz_alt = T(2) / (DZ[iz] + ((!INT && iz == 0) ? T(0) : DZ[iz - 1]));
+    const T inv_hz = m.pc[0];
+    const T inv_hz_alt = m.pc[1];
 #pragma unroll
     for (int c = 0; c < 3; c++) {
         const T v0 = A(c, 0, 0, 0);
@@ -218,12 +219,12 @@ __device__ __forceinline__ void visc_cross(const ACC& A, const StagZ<T>& m, T s[
     }
     const T U0 = U(0, 0, 0), V0 = V(0, 0, 0), W0 = W(0, 0, 0);
     if ((INT || iz != NZ - 1)) {
-        const T up = T(2) / (DZ[iz] + DZ[iz + 1]);
+        const T up = m.pc[2];
         s[0] += (U(0, 0, 1) - U0) * up * inv_hz;
         s[1] += (V(0, 0, 1) - V0) * up * inv_hz;
         s[2] += (W(0, 0, 1) - W0) * inv_hz * inv_hz_alt;
     } else {
-        const T up = T(2) / (DZ[iz]);
+        const T up = m.pc[2];
         s[0] += (-U0) * up * inv_hz;
         s[1] += (-V0) * up * inv_hz;
         s[2] += (-W0) * inv_hz * inv_hz_alt;
@@ -231,7 +232,7 @@ __device__ __forceinline__ void visc_cross(const ACC& A, const StagZ<T>& m, T s[
     if ((INT || iz != 0)) {
         s[0] += (U(0, 0, -1) - U0) * inv_hz_alt * inv_hz;
         s[1] += (V(0, 0, -1) - V0) * inv_hz_alt * inv_hz;
-        s[2] += (W(0, 0, -1) - W0) * (T(1) / DZ[iz - 1]) * inv_hz_alt;
+        s[2] += (W(0, 0, -1) - W0) * m.pc[3] * inv_hz_alt;
     } else {
         s[0] += (-U0) * inv_hz_alt * inv_hz;
         s[1] += (-V0) * inv_hz_alt * inv_hz;
@@ -246,9 +247,9 @@ template <typename T, typename ACC, typename MUF, bool INT = false>
 __device__ __forceinline__ void visc_naive(const ACC& A, const MUF& MU, const StagZ<T>& m, T s[3]) {
     const int iz = m.iz, NZ = m.NZ;
     const T *DZ = m.DZ, ihx = m.ihx, ihy = m.ihy, visc = m.visc;
-    const T inv_hz = T(1) / DZ[iz];
-    const T up = 2 / (DZ[iz] + ((!INT && iz == NZ - 1) ? T(0) : DZ[iz + 1]));
-    const T dn = 2 / (DZ[iz] + ((!INT && iz == 0) ? T(0) : DZ[iz - 1]));
+    const T inv_hz = m.pc[0];
+    const T up = m.pc[2];
+    const T dn = m.pc[1];
     const T U0 = U(0, 0, 0), V0 = V(0, 0, 0), W0 = W(0, 0, 0);
     const T q = T(0.25);
     const T mu0 = MU(0, 0, 0), muxl = MU(-1, 0, 0), muyl = MU(0, -1, 0);
@@ -290,9 +291,9 @@ template <typename T, typename ACC>
 __device__ __forceinline__ T abs_strain(const ACC& A, const StagZ<T>& m) {
     const int iz = m.iz, NZ = m.NZ;
     const T *DZ = m.DZ, ihx = m.ihx, ihy = m.ihy;
-    const T inv_hz = T(1) / DZ[iz];
-    const T up = 2 / (DZ[iz] + (iz == NZ - 1 ? T(0) : DZ[iz + 1]));
-    const T dn = 2 / (DZ[iz] + (iz == 0 ? T(0) : DZ[iz - 1]));
+    const T inv_hz = m.pc[0];
+    const T up = m.pc[2];
+    const T dn = m.pc[1];
     const T U0 = U(0, 0, 0), V0 = V(0, 0, 0), W0 = W(0, 0, 0);
     const T sxx = (U(1, 0, 0) - U0) * ihx;
     const T syy = (V(0, 1, 0) - V0) * ihy;

@@ -193,6 +193,7 @@ struct tc_handle {
     void* ptmp = nullptr;
     void* spec = nullptr;
     void* zfac = nullptr;  // time-independent factors of the z-matrices (k_zfactor)
+    void* zfac_low = nullptr;  // double factors of the low modes
     void* mesh_t = nullptr;     // mesh arrays in T
     double* mesh_d = nullptr;   // mesh arrays in double
     double* tabs = nullptr;     // cos/sin tables
@@ -252,7 +253,7 @@ static MeshDev<T> mesh_dev(const tc_handle* h) {
     const double* d = h->mesh_d;
     MeshDev<T> m;
     m.ZZ = t + 0 * L; m.DZ = t + 1 * L; m.DZW = t + 2 * L; m.GC1 = t + 3 * L; m.GC2 = t + 4 * L;
-    m.GCZ = t + 5 * L; m.KERG = t + 6 * L; m.cellh = t + 7 * L; m.MAT_A = t + 8 * L;
+    m.GCZ = t + 5 * L; m.KERG = t + 6 * L; m.cellh = t + 7 * L; m.MAT_A = t + 8 * L; m.PC = t + 11 * L;
     m.dZZ = d + 0 * L; m.dDZ = d + 1 * L; m.dDZW = d + 2 * L; m.dKERG = d + 6 * L; m.dcellh = d + 7 * L;
     m.dMAT_A = d + 8 * L;
     for (int i = 0; i < 6; i++) m.MAT_D[i] = h->hm.MAT_D[i];
@@ -276,7 +277,7 @@ template <typename T>
 static const cplx<T>* twy(const tc_handle* h) { return (const cplx<T>*)h->tw + h->g.NX; }
 
 static void free_all(tc_handle* h) {
-    void* ptrs[] = {h->nu_t, h->ptmp, h->spec, h->zfac, h->mesh_t, h->mesh_d, h->tabs, h->tw, h->red, h->ticket,
+    void* ptrs[] = {h->nu_t, h->ptmp, h->spec, h->zfac, h->zfac_low, h->mesh_t, h->mesh_d, h->tabs, h->tw, h->red, h->ticket,
                     h->err_flag, h->planes, h->diag_part, h->stage, h->opv, h->opf, h->ops};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -310,6 +311,29 @@ static bool is_23(int n) {
             return fail(TC_E_NOMEM, "device allocation of " + std::to_string((size_t)(bytes)) + " bytes failed"); \
         }                                                                                           \
     } while (0)
+
+// Per-plane reciprocals of the staggered stencils (layout in MeshDev::PC), computed in
+// the working type T from the T-valued mesh (t: the mesh slots as uploaded).
+template <typename T>
+static void fill_plane_consts(const Geom& g, const HostMesh& hm, const T* t, T* pc) {
+    const int NZ = g.NZ, L = NZ + 2;
+    const T* DZ = t + 1 * L;
+    const T* DZW = t + 2 * L;
+    const T* GCZ = t + 5 * L;
+    const T hx = (T)g.hx, hy = (T)g.hy, ihx = (T)g.inv_hx, ihy = (T)g.inv_hy;
+    const T C9 = T(0.11111111111111111111);
+    (void)hm;
+    for (int z = 0; z < NZ; z++) {
+        T* c = pc + (size_t)TC_PC * z;
+        c[0] = T(1) / DZ[z];
+        c[1] = T(2) / (DZ[z] + (z == 0 ? T(0) : DZ[z - 1]));
+        c[2] = T(2) / (DZ[z] + (z == NZ - 1 ? T(0) : DZ[z + 1]));
+        c[3] = z == 0 ? T(0) : T(1) / DZ[z - 1];
+        c[4] = T(-1) / (32 * (DZ[z] - C9 * DZW[z]) * hx * hy);
+        c[5] = -T(1. / 32.) * ihx * ihy * GCZ[z];
+        c[6] = c[7] = T(0);
+    }
+}
 
 extern "C" int tc_create(const tc_params* prm, const double* zz, tc_handle** out) {
     if (!prm || !zz || !out) return fail(TC_E_ARG, "tc_create: null argument");
@@ -382,9 +406,11 @@ extern "C" int tc_create(const tc_params* prm, const double* zz, tc_handle** out
     TC_ALLOC(h->ptmp, N * E);
     TC_ALLOC(h->spec, (size_t)g.NXH * g.NY * g.NZ * 2 * E);
     TC_ALLOC(h->zfac, zfactor_bytes(g, (int)E));
-    // mesh arrays, 9 slots of NZ+2 (the last one holds MAT_A, up to 3 NZ entries)
+    TC_ALLOC(h->zfac_low, zfactor_low_bytes(g));
+    // mesh arrays, 9 slots of NZ+2 (the last one holds MAT_A, up to 3 NZ entries), then
+    // the per-plane reciprocals (TC_PC per plane)
     const int L = g.NZ + 2;
-    const size_t mlen = (size_t)8 * L + 3 * (size_t)L;
+    const size_t mlen = (size_t)8 * L + 3 * (size_t)L + (size_t)TC_PC * L;
     TC_ALLOC(h->mesh_t, mlen * E);
     TC_ALLOC(h->mesh_d, mlen * sizeof(double));
     {
@@ -395,6 +421,8 @@ extern "C" int tc_create(const tc_params* prm, const double* zz, tc_handle** out
         };
         put(0, hm.ZZ); put(1, hm.DZ); put(2, hm.DZW); put(3, hm.GC1); put(4, hm.GC2); put(5, hm.GCZ);
         put(6, hm.KERG); put(7, hm.cellh); put(8, hm.MAT_A);
+        const size_t pc0 = (size_t)11 * L;
+        fill_plane_consts<double>(g, hm, md.data(), md.data() + pc0);
         if (cudaMemcpy(h->mesh_d, md.data(), mlen * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) {
             free_all(h); delete h;
             return fail(TC_E_CUDA, "tc_create: mesh upload failed");
@@ -404,6 +432,7 @@ extern "C" int tc_create(const tc_params* prm, const double* zz, tc_handle** out
         } else {
             std::vector<float> mf(mlen);
             for (size_t i = 0; i < mlen; i++) mf[i] = (float)md[i];
+            fill_plane_consts<float>(g, hm, mf.data(), mf.data() + pc0);
             cudaMemcpy(h->mesh_t, mf.data(), mlen * sizeof(float), cudaMemcpyHostToDevice);
         }
     }
@@ -459,11 +488,14 @@ extern "C" int tc_create(const tc_params* prm, const double* zz, tc_handle** out
     }
     if (h->nu_t) cudaMemsetAsync(h->nu_t, 0, N * E, h->st);
     cudaMemsetAsync(h->zfac, 0, zfactor_bytes(g, (int)E), h->st);
+    cudaMemsetAsync(h->zfac_low, 0, zfactor_low_bytes(g), h->st);
     if (h->fp64) {
-        ZSolveArgs<double> za{g, mesh_dev<double>(h), mode_tabs(h), (cplx<double>*)h->spec, nullptr, h->err_flag, h->zfac};
+        ZSolveArgs<double> za{g, mesh_dev<double>(h), mode_tabs(h), (cplx<double>*)h->spec, nullptr, h->err_flag, h->zfac,
+                              h->zfac_low};
         launch_zfactor<double>(za, h->st);
     } else {
-        ZSolveArgs<float> za{g, mesh_dev<float>(h), mode_tabs(h), (cplx<float>*)h->spec, nullptr, h->err_flag, h->zfac};
+        ZSolveArgs<float> za{g, mesh_dev<float>(h), mode_tabs(h), (cplx<float>*)h->spec, nullptr, h->err_flag, h->zfac,
+                             h->zfac_low};
         launch_zfactor<float>(za, h->st);
     }
     cudaError_t e = cudaStreamSynchronize(h->st);
@@ -631,7 +663,7 @@ static void poisson(tc_handle* h, const void* rhs_vec, const void* rhs_scalar, v
     YFftArgs<T> ya{g, (cplx<T>*)h->spec, h->py, twy<T>(h), -1};
     launch_yfft<T>(ya, h->st);
     if (mk) mark(h, 4, eb);
-    ZSolveArgs<T> za{g, mesh_dev<T>(h), mode_tabs(h), (cplx<T>*)h->spec, nullptr, h->err_flag, h->zfac};
+    ZSolveArgs<T> za{g, mesh_dev<T>(h), mode_tabs(h), (cplx<T>*)h->spec, nullptr, h->err_flag, h->zfac, h->zfac_low};
     launch_zsolve_fac<T>(za, h->st, h->side, h->ev_fork, h->ev_join);
     if (mk) mark(h, 5, eb);
     ya.sign = +1;

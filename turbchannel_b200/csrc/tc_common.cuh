@@ -23,9 +23,14 @@ struct Geom {
 // follow struct main_params (staggered/config.h:58-72) in the working type T;
 // collocated ones follow collocated_AB3/data_global.h:113-116 (double).  The
 // double copies serve the double-precision banded solves of the mixed mode.
+// PC: per-plane reciprocals of the staggered stencils, 8 per plane (precomputed on
+// the host so the per-cell code has no division): [0] 1/DZ[z], [1] 2/(DZ[z]+DZ[z-1])
+// (DZ[-1] = 0), [2] 2/(DZ[z]+DZ[z+1]) (DZ[NZ] = 0), [3] 1/DZ[z-1] (0 at z = 0),
+// [4] VV4 convective scale -1/(32 (DZ-DZW/9) hx hy), [5] VV4 w scale -GCZ/(32 hx hy).
+constexpr int TC_PC = 8;
 template <typename T>
 struct MeshDev {
-    const T *ZZ, *DZ, *DZW, *GC1, *GC2, *GCZ, *KERG, *MAT_A, *cellh;
+    const T *ZZ, *DZ, *DZW, *GC1, *GC2, *GCZ, *KERG, *MAT_A, *cellh, *PC;
     const double *dZZ, *dDZ, *dDZW, *dKERG, *dMAT_A, *dcellh;
     double MAT_D[6];
     double KERG_norm2;
