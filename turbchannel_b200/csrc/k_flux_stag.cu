@@ -20,14 +20,24 @@ constexpr int STX = 32, STY = 8;  // threads per CTA: 32 x 8
 constexpr int SG = 4;              // x-halo of the shared tile (a whole 16-byte chunk for float and double)
 
 // CY: cells per thread along y (the tile is 32 x 8*CY cells).
+// The offsets of the 2H+1 planes around the current one are computed once per plane,
+// so every stencil access is one of them plus a compile-time displacement.
 template <typename T, int H, int CY>
 struct RingAcc {
     static constexpr int PW = STX + 2 * SG, PH = STY * CY + 2 * H, PL = PW * PH, RS = 2 * H + 2;
     const T* ring;
-    int zs, tx, ty;  // ty: cell row inside the tile
+    int o[2 * H + 1];  // element offset of (slot of plane z+dz, component 0, this cell)
+    __device__ __forceinline__ void set(const T* r, int zs, int tx, int ty) {  // ty: cell row inside the tile
+        ring = r;
+#pragma unroll
+        for (int dz = -H; dz <= H; dz++) o[dz + H] = ((zs + dz) & (RS - 1)) * 3 * PL + (ty + H) * PW + tx + SG;
+    }
+    __device__ __forceinline__ void shift_rows(int q) {
+#pragma unroll
+        for (int k = 0; k < 2 * H + 1; k++) o[k] += q * PW;
+    }
     __device__ __forceinline__ T operator()(int c, int dx, int dy, int dz) const {
-        const int slot = (zs + dz) & (RS - 1);
-        return ring[((slot * 3 + c) * PH + ty + H + dy) * PW + tx + SG + dx];
+        return ring[o[dz + H] + c * PL + dy * PW + dx];
     }
 };
 
@@ -160,12 +170,15 @@ __global__ void __launch_bounds__(STX* STY, 2) k_flux_stag(FluxArgs<T> a, int tz
         mz.pc = a.m.PC + TC_PC * z;
         const T gcz = SCHEME == TC_SCHEME_VV4 ? a.m.GCZ[z] : T(0);
         const bool inner = z >= zlo && z <= zhi;
+        ACC A0;
+        A0.set(ring, z & (RS - 1), tx, tyt * CY);
 #pragma unroll
         for (int q = 0; q < CY; q++) {
             const int ty = tyt * CY + q, iy = y0 + ty;
             if (ix >= NX || iy >= NY) continue;
             const int ym = wrapi(iy - 1, NY), yp = wrapi(iy + 1, NY);
-            const ACC A{ring, z & (RS - 1), tx, ty};
+            ACC A = A0;
+            A.shift_rows(q);
             T f[3];
             if (inner) flux_cell<T, SCHEME, VISC, LES, true, CY>(A, mz, gcz, a, ix, iy, xm, xp, ym, yp, NXY, f);
             else flux_cell<T, SCHEME, VISC, LES, false, CY>(A, mz, gcz, a, ix, iy, xm, xp, ym, yp, NXY, f);
