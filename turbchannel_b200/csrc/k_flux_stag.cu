@@ -25,19 +25,18 @@ constexpr int SG = 4;              // x-halo of the shared tile (a whole 16-byte
 template <typename T, int H, int CY>
 struct RingAcc {
     static constexpr int PW = STX + 2 * SG, PH = STY * CY + 2 * H, PL = PW * PH, RS = 2 * H + 2;
-    const T* ring;
-    int o[2 * H + 1];  // element offset of (slot of plane z+dz, component 0, this cell)
+    const T* p[2 * H + 1];  // (slot of plane z+dz, component 0, this cell)
     __device__ __forceinline__ void set(const T* r, int zs, int tx, int ty) {  // ty: cell row inside the tile
-        ring = r;
+        const T* c = r + (ty + H) * PW + tx + SG;
 #pragma unroll
-        for (int dz = -H; dz <= H; dz++) o[dz + H] = ((zs + dz) & (RS - 1)) * 3 * PL + (ty + H) * PW + tx + SG;
+        for (int dz = -H; dz <= H; dz++) p[dz + H] = c + ((zs + dz) & (RS - 1)) * 3 * PL;
     }
     __device__ __forceinline__ void shift_rows(int q) {
 #pragma unroll
-        for (int k = 0; k < 2 * H + 1; k++) o[k] += q * PW;
+        for (int k = 0; k < 2 * H + 1; k++) p[k] += q * PW;
     }
     __device__ __forceinline__ T operator()(int c, int dx, int dy, int dz) const {
-        return ring[o[dz + H] + c * PL + dy * PW + dx];
+        return p[dz + H][c * PL + dy * PW + dx];
     }
 };
 
@@ -167,7 +166,8 @@ __global__ void __launch_bounds__(STX* STY, 2) k_flux_stag(FluxArgs<T> a, int tz
         cp_async_wait<1>();
         __syncthreads();
         mz.iz = z;
-        mz.pc = a.m.PC + TC_PC * z;
+#pragma unroll
+        for (int k = 0; k < 6; k++) mz.pc[k] = a.m.PC[TC_PC * z + k];
         const T gcz = SCHEME == TC_SCHEME_VV4 ? a.m.GCZ[z] : T(0);
         const bool inner = z >= zlo && z <= zhi;
         ACC A0;
@@ -264,6 +264,9 @@ static void run_visc(const FluxArgs<T>& a, cudaStream_t s) {
 
 template <typename T>
 void launch_flux_stag(const FluxArgs<T>& a, cudaStream_t s) {
+    if constexpr (sizeof(T) == 4) {
+        if (launch_flux_stag_pair(a, s)) return;
+    }
     if (a.g.scheme == TC_SCHEME_VV4) run_visc<T, TC_SCHEME_VV4>(a, s);
     else run_visc<T, TC_SCHEME_HW2>(a, s);
 }

@@ -271,7 +271,9 @@ __global__ void __launch_bounds__(256) k_turb_stag(TurbArgs<T> a) {
     if (in >= g.N) return;
     const int ix = (int)(in % g.NX), iy = (int)((in / g.NX) % g.NY), iz = (int)(in / g.NXY);
     GAcc<T> A{{a.v.c[0], a.v.c[1], a.v.c[2]}, ix, iy, iz, g.NX, g.NY, (size_t)g.NXY};
-    StagZ<T> mz{iz, g.NZ, a.m.DZ, a.m.DZW, (T)g.hx, (T)g.hy, (T)g.inv_hx, (T)g.inv_hy, (T)g.visc, a.m.PC + TC_PC * iz};
+    StagZ<T> mz{iz, g.NZ, a.m.DZ, a.m.DZW, (T)g.hx, (T)g.hy, (T)g.inv_hx, (T)g.inv_hy, (T)g.visc, {}};
+#pragma unroll
+    for (int k = 0; k < 6; k++) mz.pc[k] = a.m.PC[TC_PC * iz + k];
     const T S = abs_strain(A, mz);
     const T* ZZ = a.m.ZZ;
     const T H = T(0.5) * (ZZ[g.NZ] - ZZ[0]);

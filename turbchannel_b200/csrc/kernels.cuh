@@ -139,6 +139,7 @@ constexpr int TC_DIAG_STRIDE = 19;
 
 template <typename T> void launch_flux_stag(const FluxArgs<T>& a, cudaStream_t s);
 template <typename T> void launch_flux_coll(const FluxArgs<T>& a, cudaStream_t s);
+bool launch_flux_stag_pair(const FluxArgs<float>& a, cudaStream_t s);  // k_flux_pair.cu; false: not covered
 template <typename T> int launch_div_xfft(const DivFftArgs<T>& a, cudaStream_t s);  // returns launches
 template <typename T> void launch_yfft(const YFftArgs<T>& a, cudaStream_t s);
 template <typename T> void launch_zsolve(const ZSolveArgs<T>& a, cudaStream_t s, cudaStream_t side, cudaEvent_t fork,

@@ -24,11 +24,11 @@ struct StagZ {  // wall-normal metric at the current plane
     const T* DZ;
     const T* DZW;
     T hx, hy, ihx, ihy, visc;
-    const T* pc;  // MeshDev::PC + TC_PC * iz
+    T pc[6];  // MeshDev::PC[TC_PC * iz + 0..5], loaded once per plane
 };
 
-template <typename T, typename ACC, bool INT = false>
-__device__ __forceinline__ void conv_hw2(const ACC& A, const StagZ<T>& m, T s[3]) {
+template <typename T, typename ACC, bool INT = false, typename VT = T>
+__device__ __forceinline__ void conv_hw2(const ACC& A, const StagZ<T>& m, VT s[3]) {
 #define U(a, b, c) A(0, a, b, c)
 #define V(a, b, c) A(1, a, b, c)
 #define W(a, b, c) A(2, a, b, c)
@@ -36,9 +36,9 @@ __device__ __forceinline__ void conv_hw2(const ACC& A, const StagZ<T>& m, T s[3]
     const T* DZ = m.DZ;
     const T inv_hz = m.pc[0];
     const T inv_hz_alt = m.pc[1];
-    const T U0 = U(0, 0, 0), V0 = V(0, 0, 0), W0 = W(0, 0, 0);
+    const VT U0 = U(0, 0, 0), V0 = V(0, 0, 0), W0 = W(0, 0, 0);
     s[0] = s[1] = s[2] = 0;
-    T a = U0 + U(1, 0, 0), c = U0 + U(-1, 0, 0);
+    VT a = U0 + U(1, 0, 0), c = U0 + U(-1, 0, 0);
     s[0] -= (a * a - c * c) * m.ihx;
     s[0] -= ((U0 + U(0, 1, 0)) * (V(0, 1, 0) + V(-1, 1, 0)) - (U0 + U(0, -1, 0)) * (V0 + V(-1, 0, 0))) * m.ihy;
     if ((INT || iz != NZ - 1)) s[0] -= (U0 + U(0, 0, 1)) * (W(0, 0, 1) + W(-1, 0, 1)) * inv_hz;
@@ -56,7 +56,7 @@ __device__ __forceinline__ void conv_hw2(const ACC& A, const StagZ<T>& m, T s[3]
                  (W0 + W(-1, 0, 0)) * (U0 * DZ[iz] + U(0, 0, -1) * DZ[iz - 1])) * m.ihx * inv_hz_alt;
         s[2] -= ((W0 + W(0, 1, 0)) * (V(0, 1, 0) * DZ[iz] + V(0, 1, -1) * DZ[iz - 1]) -
                  (W0 + W(0, -1, 0)) * (V0 * DZ[iz] + V(0, 0, -1) * DZ[iz - 1])) * m.ihy * inv_hz_alt;
-        a = W0 + ((!INT && iz == NZ - 1) ? T(0) : W(0, 0, 1));
+        a = W0 + ((!INT && iz == NZ - 1) ? VT(0) : W(0, 0, 1));
         s[2] -= a * a * inv_hz_alt;
         a = W0 + W(0, 0, -1);
         s[2] += a * a * inv_hz_alt;
@@ -66,30 +66,30 @@ __device__ __forceinline__ void conv_hw2(const ACC& A, const StagZ<T>& m, T s[3]
     s[2] *= T(0.25);
 }
 
-template <typename T, typename ACC, bool INT = false>
-__device__ __forceinline__ void conv_vv4(const ACC& A, const StagZ<T>& m, T gcz, T s[3]) {
+template <typename T, typename ACC, bool INT = false, typename VT = T>
+__device__ __forceinline__ void conv_vv4(const ACC& A, const StagZ<T>& m, T gcz, VT s[3]) {
     const int iz = m.iz, NZ = m.NZ;
     const T *DZ = m.DZ, *DZW = m.DZW;
     const T hx = m.hx, hy = m.hy, dz = DZ[iz], dzw = DZW[iz], hxhy = hx * hy;
     const T C27 = T(0.03703703703703703703), C9 = T(0.11111111111111111111);
-    const T U0 = U(0, 0, 0), V0 = V(0, 0, 0), W0 = W(0, 0, 0);
+    const VT U0 = U(0, 0, 0), V0 = V(0, 0, 0), W0 = W(0, 0, 0);
     s[0] = s[1] = s[2] = 0;
     {  // u: x-faces
-        T br = dz * hy * (9 * (U0 + U(1, 0, 0)) - (U(-1, 0, 0) + U(2, 0, 0)));
-        T bl = dz * hy * (9 * (U(-1, 0, 0) + U0) - (U(-2, 0, 0) + U(1, 0, 0)));
-        T bbr = dzw * hy * (9 * (U(1, 0, 0) + U(2, 0, 0)) - (U0 + U(3, 0, 0)));
-        T bbl = dzw * hy * (9 * (U(-2, 0, 0) + U(-1, 0, 0)) - (U(-3, 0, 0) + U0));
+        VT br = dz * hy * (9 * (U0 + U(1, 0, 0)) - (U(-1, 0, 0) + U(2, 0, 0)));
+        VT bl = dz * hy * (9 * (U(-1, 0, 0) + U0) - (U(-2, 0, 0) + U(1, 0, 0)));
+        VT bbr = dzw * hy * (9 * (U(1, 0, 0) + U(2, 0, 0)) - (U0 + U(3, 0, 0)));
+        VT bbl = dzw * hy * (9 * (U(-2, 0, 0) + U(-1, 0, 0)) - (U(-3, 0, 0) + U0));
         s[0] += br * (U0 + U(1, 0, 0)) - C27 * bbr * (U0 + U(3, 0, 0)) - bl * (U(-1, 0, 0) + U0) + C27 * bbl * (U(-3, 0, 0) + U0);
     }
     {  // u: y-faces
-        T br = dz * hx * (9 * (V(0, 1, 0) + V(-1, 1, 0)) - (V(-2, 1, 0) + V(1, 1, 0)));
-        T bl = dz * hx * (9 * (V0 + V(-1, 0, 0)) - (V(-2, 0, 0) + V(1, 0, 0)));
-        T bbr = dzw * hx * (9 * (V(0, 2, 0) + V(-1, 2, 0)) - (V(-2, 2, 0) + V(1, 2, 0)));
-        T bbl = dzw * hx * (9 * (V(0, -1, 0) + V(-1, -1, 0)) - (V(-2, -1, 0) + V(1, -1, 0)));
+        VT br = dz * hx * (9 * (V(0, 1, 0) + V(-1, 1, 0)) - (V(-2, 1, 0) + V(1, 1, 0)));
+        VT bl = dz * hx * (9 * (V0 + V(-1, 0, 0)) - (V(-2, 0, 0) + V(1, 0, 0)));
+        VT bbr = dzw * hx * (9 * (V(0, 2, 0) + V(-1, 2, 0)) - (V(-2, 2, 0) + V(1, 2, 0)));
+        VT bbl = dzw * hx * (9 * (V(0, -1, 0) + V(-1, -1, 0)) - (V(-2, -1, 0) + V(1, -1, 0)));
         s[0] += br * (U0 + U(0, 1, 0)) - C27 * bbr * (U0 + U(0, 3, 0)) - bl * (U(0, -1, 0) + U0) + C27 * bbl * (U(0, -3, 0) + U0);
     }
     {  // u: z-faces
-        T wzl, wzr, wbzl, wbzr;
+        VT wzl, wzr, wbzl, wbzr;
         if ((!INT && iz == 0)) wzl = 0;
         else wzl = hxhy * (9 * (W0 + W(-1, 0, 0)) - (W(-2, 0, 0) + W(1, 0, 0)));
         if ((!INT && iz == NZ - 1)) wzr = 0;
@@ -100,28 +100,28 @@ __device__ __forceinline__ void conv_vv4(const ACC& A, const StagZ<T>& m, T gcz,
         if ((!INT && iz == NZ - 2)) wbzr = 0;
         else if ((!INT && iz == NZ - 1)) wbzr = wzl;
         else wbzr = hxhy * (9 * (W(0, 0, 2) + W(-1, 0, 2)) - (W(-2, 0, 2) + W(1, 0, 2)));
-        T uzr = (!INT && iz == NZ - 1) ? T(0) : U0 + U(0, 0, 1);
-        T uzrr = U0 + ((!INT && iz == NZ - 3) ? -U(0, 0, 2) : (!INT && iz == NZ - 2) ? T(0) : (!INT && iz == NZ - 1) ? U(0, 0, -2) : U(0, 0, 3));
-        T uzl = (!INT && iz == 0) ? T(0) : U(0, 0, -1) + U0;
-        T uzll = U0 + ((!INT && iz == 2) ? -U(0, 0, -2) : (!INT && iz == 1) ? T(0) : (!INT && iz == 0) ? U(0, 0, 2) : U(0, 0, -3));
+        VT uzr = (!INT && iz == NZ - 1) ? VT(0) : U0 + U(0, 0, 1);
+        VT uzrr = U0 + ((!INT && iz == NZ - 3) ? -U(0, 0, 2) : (!INT && iz == NZ - 2) ? VT(0) : (!INT && iz == NZ - 1) ? U(0, 0, -2) : U(0, 0, 3));
+        VT uzl = (!INT && iz == 0) ? VT(0) : U(0, 0, -1) + U0;
+        VT uzll = U0 + ((!INT && iz == 2) ? -U(0, 0, -2) : (!INT && iz == 1) ? VT(0) : (!INT && iz == 0) ? U(0, 0, 2) : U(0, 0, -3));
         s[0] += wzr * uzr - C27 * wbzr * uzrr - wzl * uzl + C27 * wbzl * uzll;
     }
     {  // v: x-faces
-        T br = dz * hy * (9 * (U(1, 0, 0) + U(1, -1, 0)) - (U(1, -2, 0) + U(1, 1, 0)));
-        T bl = dz * hy * (9 * (U0 + U(0, -1, 0)) - (U(0, -2, 0) + U(0, 1, 0)));
-        T bbr = dzw * hy * (9 * (U(2, 0, 0) + U(2, -1, 0)) - (U(2, -2, 0) + U(2, 1, 0)));
-        T bbl = dzw * hy * (9 * (U(-1, 0, 0) + U(-1, -1, 0)) - (U(-1, -2, 0) + U(-1, 1, 0)));
+        VT br = dz * hy * (9 * (U(1, 0, 0) + U(1, -1, 0)) - (U(1, -2, 0) + U(1, 1, 0)));
+        VT bl = dz * hy * (9 * (U0 + U(0, -1, 0)) - (U(0, -2, 0) + U(0, 1, 0)));
+        VT bbr = dzw * hy * (9 * (U(2, 0, 0) + U(2, -1, 0)) - (U(2, -2, 0) + U(2, 1, 0)));
+        VT bbl = dzw * hy * (9 * (U(-1, 0, 0) + U(-1, -1, 0)) - (U(-1, -2, 0) + U(-1, 1, 0)));
         s[1] += br * (V0 + V(1, 0, 0)) - C27 * bbr * (V0 + V(3, 0, 0)) - bl * (V(-1, 0, 0) + V0) + C27 * bbl * (V(-3, 0, 0) + V0);
     }
     {  // v: y-faces
-        T br = dz * hx * (9 * (V0 + V(0, 1, 0)) - (V(0, -1, 0) + V(0, 2, 0)));
-        T bl = dz * hx * (9 * (V(0, -1, 0) + V0) - (V(0, -2, 0) + V(0, 1, 0)));
-        T bbr = dzw * hx * (9 * (V(0, 1, 0) + V(0, 2, 0)) - (V0 + V(0, 3, 0)));
-        T bbl = dzw * hx * (9 * (V(0, -2, 0) + V(0, -1, 0)) - (V(0, -3, 0) + V0));
+        VT br = dz * hx * (9 * (V0 + V(0, 1, 0)) - (V(0, -1, 0) + V(0, 2, 0)));
+        VT bl = dz * hx * (9 * (V(0, -1, 0) + V0) - (V(0, -2, 0) + V(0, 1, 0)));
+        VT bbr = dzw * hx * (9 * (V(0, 1, 0) + V(0, 2, 0)) - (V0 + V(0, 3, 0)));
+        VT bbl = dzw * hx * (9 * (V(0, -2, 0) + V(0, -1, 0)) - (V(0, -3, 0) + V0));
         s[1] += br * (V0 + V(0, 1, 0)) - C27 * bbr * (V0 + V(0, 3, 0)) - bl * (V(0, -1, 0) + V0) + C27 * bbl * (V(0, -3, 0) + V0);
     }
     {  // v: z-faces
-        T wzl, wzr, wbzl, wbzr;
+        VT wzl, wzr, wbzl, wbzr;
         if ((!INT && iz == 0)) wzl = 0;
         else wzl = hxhy * (9 * (W0 + W(0, -1, 0)) - (W(0, -2, 0) + W(0, 1, 0)));
         if ((!INT && iz == NZ - 1)) wzr = 0;
@@ -132,15 +132,15 @@ __device__ __forceinline__ void conv_vv4(const ACC& A, const StagZ<T>& m, T gcz,
         if ((!INT && iz == NZ - 2)) wbzr = 0;
         else if ((!INT && iz == NZ - 1)) wbzr = wzl;
         else wbzr = hxhy * (9 * (W(0, 0, 2) + W(0, -1, 2)) - (W(0, -2, 2) + W(0, 1, 2)));
-        T vzr = (!INT && iz == NZ - 1) ? T(0) : V0 + V(0, 0, 1);
-        T vzrr = V0 + ((!INT && iz == NZ - 3) ? -V(0, 0, 2) : (!INT && iz == NZ - 2) ? T(0) : (!INT && iz == NZ - 1) ? V(0, 0, -2) : V(0, 0, 3));
-        T vzl = (!INT && iz == 0) ? T(0) : V(0, 0, -1) + V0;
-        T vzll = V0 + ((!INT && iz == 2) ? -V(0, 0, -2) : (!INT && iz == 1) ? T(0) : (!INT && iz == 0) ? V(0, 0, 2) : V(0, 0, -3));
+        VT vzr = (!INT && iz == NZ - 1) ? VT(0) : V0 + V(0, 0, 1);
+        VT vzrr = V0 + ((!INT && iz == NZ - 3) ? -V(0, 0, 2) : (!INT && iz == NZ - 2) ? VT(0) : (!INT && iz == NZ - 1) ? V(0, 0, -2) : V(0, 0, 3));
+        VT vzl = (!INT && iz == 0) ? VT(0) : V(0, 0, -1) + V0;
+        VT vzll = V0 + ((!INT && iz == 2) ? -V(0, 0, -2) : (!INT && iz == 1) ? VT(0) : (!INT && iz == 0) ? V(0, 0, 2) : V(0, 0, -3));
         s[1] += wzr * vzr - C27 * wbzr * vzrr - wzl * vzl + C27 * wbzl * vzll;
     }
     if ((INT || iz != 0)) {
         {  // w: x-faces, mass flux averaged to the w-face in z
-            T br, bl, bbr, bbl;
+            VT br, bl, bbr, bbl;
             br = 9 * (U(1, 0, 0) * DZ[iz] + U(1, 0, -1) * DZ[iz - 1]);
             br -= ((!INT && iz == 1)) ? -U(1, 0, -1) * DZ[0] : U(1, 0, -2) * DZ[iz - 2];
             br -= ((!INT && iz == NZ - 1)) ? -U(1, 0, 0) * DZ[NZ - 1] : U(1, 0, 1) * DZ[iz + 1];
@@ -160,7 +160,7 @@ __device__ __forceinline__ void conv_vv4(const ACC& A, const StagZ<T>& m, T gcz,
             s[2] += br * (W0 + W(1, 0, 0)) - C27 * bbr * (W0 + W(3, 0, 0)) - bl * (W(-1, 0, 0) + W0) + C27 * bbl * (W(-3, 0, 0) + W0);
         }
         {  // w: y-faces (scaled by hy as in staggered/func_global.h:475-487)
-            T br, bl, bbr, bbl;
+            VT br, bl, bbr, bbl;
             br = 9 * (V(0, 1, 0) * DZ[iz] + V(0, 1, -1) * DZ[iz - 1]);
             br -= ((!INT && iz == 1)) ? -V(0, 1, -1) * DZ[0] : V(0, 1, -2) * DZ[iz - 2];
             br -= ((!INT && iz == NZ - 1)) ? -V(0, 1, 0) * DZ[NZ - 1] : V(0, 1, 1) * DZ[iz + 1];
@@ -180,16 +180,16 @@ __device__ __forceinline__ void conv_vv4(const ACC& A, const StagZ<T>& m, T gcz,
             s[2] += br * (W0 + W(0, 1, 0)) - C27 * bbr * (W0 + W(0, 3, 0)) - bl * (W(0, -1, 0) + W0) + C27 * bbl * (W(0, -3, 0) + W0);
         }
         {  // w: z-faces
-            T wzl = W(0, 0, -1);
-            T wzr = (!INT && iz == NZ - 1) ? T(0) : W(0, 0, 1);
-            T wzll = (!INT && iz == 1) ? W0 : W(0, 0, -2);
-            T wzrr = (!INT && iz == NZ - 2) ? T(0) : (!INT && iz == NZ - 1) ? W0 : W(0, 0, 2);
-            T wzlll = (!INT && iz == 1) ? W(0, 0, 1) : (!INT && iz == 2) ? W(0, 0, -1) : W(0, 0, -3);
-            T wzrrr = (!INT && iz == NZ - 3) ? T(0) : (!INT && iz == NZ - 2) ? W(0, 0, 1) : (!INT && iz == NZ - 1) ? W(0, 0, -1) : W(0, 0, 3);
-            T bl = hxhy * (9 * (wzl + W0) - (wzll + wzr));
-            T br = hxhy * (9 * (W0 + wzr) - (wzl + wzrr));
-            T bbl = hxhy * (9 * (wzll + wzl) - (wzlll + W0));
-            T bbr = hxhy * (9 * (wzr + wzrr) - (W0 + wzrrr));
+            VT wzl = W(0, 0, -1);
+            VT wzr = (!INT && iz == NZ - 1) ? VT(0) : W(0, 0, 1);
+            VT wzll = (!INT && iz == 1) ? W0 : W(0, 0, -2);
+            VT wzrr = (!INT && iz == NZ - 2) ? VT(0) : (!INT && iz == NZ - 1) ? W0 : W(0, 0, 2);
+            VT wzlll = (!INT && iz == 1) ? W(0, 0, 1) : (!INT && iz == 2) ? W(0, 0, -1) : W(0, 0, -3);
+            VT wzrrr = (!INT && iz == NZ - 3) ? VT(0) : (!INT && iz == NZ - 2) ? W(0, 0, 1) : (!INT && iz == NZ - 1) ? W(0, 0, -1) : W(0, 0, 3);
+            VT bl = hxhy * (9 * (wzl + W0) - (wzll + wzr));
+            VT br = hxhy * (9 * (W0 + wzr) - (wzl + wzrr));
+            VT bbl = hxhy * (9 * (wzll + wzl) - (wzlll + W0));
+            VT bbr = hxhy * (9 * (wzr + wzrr) - (W0 + wzrrr));
             s[2] += br * (W0 + wzr) - bl * (wzl + W0);
             if ((INT || iz < NZ - 2)) s[2] -= C27 * bbr * (W0 + wzrrr);
             else if ((!INT && iz == NZ - 2)) s[2] -= C27 * bbr * (-W(0, 0, 1) + W0);
@@ -205,19 +205,19 @@ __device__ __forceinline__ void conv_vv4(const ACC& A, const StagZ<T>& m, T gcz,
     s[2] *= m.pc[5];
 }
 
-template <typename T, typename ACC, bool INT = false>
-__device__ __forceinline__ void visc_cross(const ACC& A, const StagZ<T>& m, T s[3]) {
+template <typename T, typename ACC, bool INT = false, typename VT = T>
+__device__ __forceinline__ void visc_cross(const ACC& A, const StagZ<T>& m, VT s[3]) {
     const int iz = m.iz, NZ = m.NZ;
     const T* DZ = m.DZ;
     const T inv_hz = m.pc[0];
     const T inv_hz_alt = m.pc[1];
 #pragma unroll
     for (int c = 0; c < 3; c++) {
-        const T v0 = A(c, 0, 0, 0);
+        const VT v0 = A(c, 0, 0, 0);
         s[c] = m.ihx * m.ihx * (A(c, 1, 0, 0) + A(c, -1, 0, 0) - T(2.) * v0);
         s[c] += m.ihy * m.ihy * (A(c, 0, 1, 0) + A(c, 0, -1, 0) - T(2.) * v0);
     }
-    const T U0 = U(0, 0, 0), V0 = V(0, 0, 0), W0 = W(0, 0, 0);
+    const VT U0 = U(0, 0, 0), V0 = V(0, 0, 0), W0 = W(0, 0, 0);
     if ((INT || iz != NZ - 1)) {
         const T up = m.pc[2];
         s[0] += (U(0, 0, 1) - U0) * up * inv_hz;
