@@ -46,7 +46,7 @@ FALLBACK_HBM_GBS = 6650.0
 # DRAM bytes per cell of one launch (dram__bytes_read.sum + dram__bytes_write.sum) from
 # the ncu capture summarised in profiles/flux_vv4_192x128x192.md (4.7 M cells, inputs
 # larger than L2); traffic grows with the cell count, so it is scaled to the grid.
-TRAFFIC_BYTES_PER_CELL = {("flux", 4): 376.33e6 / 4718592, ("flux", 8): 798.1e6 / 4718592}
+TRAFFIC_BYTES_PER_CELL = {("flux", 4): (284.9e6 + 90.76e6) / 4718592, ("flux", 8): (591.3e6 + 208.6e6) / 4718592}
 
 
 def peaks():
