@@ -11,8 +11,11 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 HEADER = os.path.join(ROOT, "include", "turbch.h")
 
 
-def _declared():
-    src = open(HEADER).read()
+HEADER_LES = os.path.join(ROOT, "include", "turbch_les.h")
+
+
+def _declared(path=HEADER):
+    src = open(path).read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
     return sorted(set(re.findall(r"\b(tc_[a-z0-9_]+)\s*\(", src)))
 
@@ -34,6 +37,10 @@ def test_exports_every_declared_symbol(lib):
     for n in names:
         assert hasattr(lib, n), n
     assert sorted(tb.EXPORTS) == names
+    les = _declared(HEADER_LES)
+    for n in les:
+        assert hasattr(lib, n), n
+    assert sorted(tb.EXPORTS_LES) == les
 
 
 def test_version_and_error_strings(lib):

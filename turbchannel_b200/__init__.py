@@ -44,6 +44,12 @@ EXPORTS = [
     "tc_init_channel", "tc_mesh_tanh", "tc_phase_timing", "tc_phase_times", "tc_launch_count",
     "tc_op_pressure_solve_static",
 ]
+# Every entry point declared in include/turbch_les.h (learned LES closure).
+EXPORTS_LES = [
+    "tc_les_filter", "tc_les_samples", "tc_mlp_create", "tc_mlp_destroy", "tc_mlp_get_params", "tc_mlp_set_params",
+    "tc_mlp_set_data", "tc_mlp_train", "tc_mlp_grad", "tc_mlp_forward",
+]
+MLP_NPAR = 4673
 NPHASE = 8
 PHASES = ["turb", "flux", "div_xfft", "yfft", "zsolve", "iyfft", "ixfft", "correct"]
 
@@ -93,6 +99,17 @@ def load_library(path: str = LIB_PATH):
     L.tc_phase_timing.argtypes = [vp, ip]
     L.tc_phase_times.argtypes = [vp, vp, C.POINTER(C.c_int)]
     L.tc_launch_count.argtypes = [vp, C.POINTER(C.c_ulonglong)]
+    ll = C.c_longlong
+    L.tc_les_filter.argtypes = [vp, ip, ip, vp]
+    L.tc_les_samples.argtypes = [vp, ip, ip, vp, vp]
+    L.tc_mlp_create.argtypes = [ip, C.c_ulonglong, C.POINTER(vp)]
+    L.tc_mlp_destroy.argtypes = [vp]
+    L.tc_mlp_get_params.argtypes = [vp, vp]
+    L.tc_mlp_set_params.argtypes = [vp, vp]
+    L.tc_mlp_set_data.argtypes = [vp, vp, vp, ll]
+    L.tc_mlp_train.argtypes = [vp, ip, ll, C.c_float, vp]
+    L.tc_mlp_grad.argtypes = [vp, vp, vp, ll, vp, C.POINTER(C.c_float)]
+    L.tc_mlp_forward.argtypes = [vp, vp, ll, vp]
     _lib = L
     return L
 
@@ -186,7 +203,25 @@ class Solver:
         return d.value
 
     def set_turb_model(self, kind: int, weights=None):
-        self._check(self.L.tc_set_turb_model(self.h, kind, None if weights is None else _ptr(weights)))
+        """kind TURB_NONE / TURB_SMAGORINSKY / TURB_MLP (weights: MLP_NPAR float parameters)."""
+        w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float32)
+        self._check(self.L.tc_set_turb_model(self.h, kind, None if w is None else _ptr(w)))
+
+    # ---- learned closure: training data ----
+    def les_filter(self, level: int, width: int = 4):
+        """Box filter (width in x and y): 10 fields [k][z][Y][X] (u, v, w, p, uu, vv, ww, uv, uw, vw)."""
+        M = (self.NX // width) * (self.NY // width) * self.NZ
+        out = np.zeros(10 * M, dtype=np.float32)
+        self._check(self.L.tc_les_filter(self.h, level, width, _ptr(out)))
+        return out.reshape(10, self.NZ, self.NY // width, self.NX // width)
+
+    def les_samples(self, level: int, width: int = 4):
+        """Closure training samples of the filtered level: features (M, 6), targets nu*/nu (M,)."""
+        M = (self.NX // width) * (self.NY // width) * self.NZ
+        X = np.zeros((M, 6), dtype=np.float32)
+        Y = np.zeros(M, dtype=np.float32)
+        self._check(self.L.tc_les_samples(self.h, level, width, _ptr(X), _ptr(Y)))
+        return X, Y
 
     # ---- diagnostics ----
     def CalcIntegral(self, level: int):
@@ -266,6 +301,68 @@ class Solver:
 
     def init_channel(self, level: int, seed: int = 12345, amp: float = 0.1, project: bool = True):
         self._check(self.L.tc_init_channel(self.h, level, seed, amp, 1 if project else 0))
+
+
+class Mlp:
+    """The learned closure's network on one GPU (include/turbch_les.h): BF16 tensor-core
+    training (Adam) and inference kernels of the library."""
+
+    def __init__(self, seed: int = 12345, device: int = 0):
+        self.L = load_library()
+        h = C.c_void_p()
+        self._check(self.L.tc_mlp_create(device, seed, C.byref(h)))
+        self.h = h
+
+    def _check(self, rc: int):
+        if rc != 0:
+            raise TcError(f"turbch error {rc}: {self.L.tc_last_error().decode()}")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.tc_mlp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def params(self) -> np.ndarray:
+        p = np.zeros(MLP_NPAR, dtype=np.float32)
+        self._check(self.L.tc_mlp_get_params(self.h, _ptr(p)))
+        return p
+
+    @params.setter
+    def params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        assert p.size == MLP_NPAR
+        self._check(self.L.tc_mlp_set_params(self.h, _ptr(p)))
+
+    def set_data(self, X, Y):
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        Y = np.ascontiguousarray(Y, dtype=np.float32)
+        self._check(self.L.tc_mlp_set_data(self.h, _ptr(X), _ptr(Y), len(Y)))
+
+    def train(self, epochs: int, batch: int, lr: float) -> np.ndarray:
+        loss = np.zeros(epochs, dtype=np.float32)
+        self._check(self.L.tc_mlp_train(self.h, epochs, batch, lr, _ptr(loss)))
+        return loss
+
+    def grad(self, X, Y):
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        Y = np.ascontiguousarray(Y, dtype=np.float32)
+        g = np.zeros(MLP_NPAR, dtype=np.float32)
+        loss = C.c_float()
+        self._check(self.L.tc_mlp_grad(self.h, _ptr(X), _ptr(Y), len(Y), _ptr(g), C.byref(loss)))
+        return g, loss.value
+
+    def forward(self, X):
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        out = np.zeros(len(X), dtype=np.float32)
+        self._check(self.L.tc_mlp_forward(self.h, _ptr(X), len(X), _ptr(out)))
+        return out
 
 
 def channel_params(scheme: int, NX: int, NY: int, NZ: int, Lx: float, Ly: float, Re_b: float, gamma: float,

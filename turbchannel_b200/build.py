@@ -37,7 +37,7 @@ def build(verbose: bool = False, jobs: int | None = None) -> str:
     os.makedirs(BUILD, exist_ok=True)
     sources = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
     headers = sorted(glob.glob(os.path.join(CSRC, "*.cuh"))) + [
-        os.path.join(HERE, "..", "include", "turbch.h")]
+        os.path.join(HERE, "..", "include", "turbch.h"), os.path.join(HERE, "..", "include", "turbch_les.h")]
     objs = []
     cmds = []
     for s in sources:

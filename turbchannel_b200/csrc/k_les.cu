@@ -1,0 +1,232 @@
+// k_les.cu -- data for the learned LES closure and its use in a run (staggered grids).
+//
+//   k_les_filter    box filter of width fw in x and y (the periodic directions) of one
+//                   ring level: per coarse cell the cell-centred means of u, v, w, p and
+//                   of the six products u_i u_j (10 fields) -- the snapshot and the
+//                   sub-filter stresses tau_ij = <u_i u_j> - <u_i><u_j>;
+//   k_les_features  per coarse cell the closure's 6 inputs (les_features) from the
+//                   filtered gradient, and its training target nu*/nu, the
+//                   least-squares eddy viscosity -tau^d_ij S_ij / (2 S_kl S_kl) >= 0;
+//   k_turb_mlp      a run's nu_t = nu * MLP(features of the resolved field), one warp
+//                   per 16 cells on the tensor cores (inference of mlp.cuh).
+// Cell-centred velocities: u_c = (u_x + u_{x+1})/2 etc. (u on the lower x-face,
+// v on the lower y-face, w on the lower z-face, w = 0 on the top wall).  Gradients:
+// central differences; at the walls the no-slip value 0 at the wall plane is the
+// missing neighbour.
+#include "kernels.cuh"
+#include "mlp.cuh"
+
+namespace tc {
+
+// The closure's inputs from the velocity gradient G[i][j] = du_i/dx_j: with S, O the
+// symmetric and antisymmetric parts in wall units (times nu/u_tau^2), asinh of
+// tr(S^2), tr(O^2), tr(S^3), tr(O^2 S), tr(O^2 S^2), and log(1 + y+)/4.
+__device__ __forceinline__ void les_features(const double G[3][3], double nu, double utau, double d, float f[6]) {
+    const double sc = nu / (utau * utau);
+    double S[3][3], O[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            S[i][j] = 0.5 * (G[i][j] + G[j][i]) * sc;
+            O[i][j] = 0.5 * (G[i][j] - G[j][i]) * sc;
+        }
+    double S2[3][3], O2[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            S2[i][j] = S[i][0] * S[0][j] + S[i][1] * S[1][j] + S[i][2] * S[2][j];
+            O2[i][j] = O[i][0] * O[0][j] + O[i][1] * O[1][j] + O[i][2] * O[2][j];
+        }
+    double l1 = 0, l2 = 0, l3 = 0, l4 = 0, l5 = 0;
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            l1 += S[i][j] * S[j][i];
+            l2 += O[i][j] * O[j][i];
+            l3 += S2[i][j] * S[j][i];
+            l4 += O2[i][j] * S[j][i];
+            l5 += O2[i][j] * S2[j][i];
+        }
+    f[0] = (float)asinh(l1);
+    f[1] = (float)asinh(l2);
+    f[2] = (float)asinh(l3);
+    f[3] = (float)asinh(l4);
+    f[4] = (float)asinh(l5);
+    f[5] = (float)(0.25 * log1p(d * utau / nu));
+}
+
+// z-derivative of a cell-centred column value at plane z from the values at z-1, z,
+// z+1 (the wall value 0 replaces a missing neighbour).
+__device__ __forceinline__ double ddz(const double* ZZ, int NZ, int z, double qm, double qp) {
+    const double zc = 0.5 * (ZZ[z] + ZZ[z + 1]);
+    const double zm = z > 0 ? 0.5 * (ZZ[z - 1] + ZZ[z]) : ZZ[0];
+    const double zp = z < NZ - 1 ? 0.5 * (ZZ[z + 1] + ZZ[z + 2]) : ZZ[NZ];
+    (void)zc;
+    return ((z < NZ - 1 ? qp : 0.0) - (z > 0 ? qm : 0.0)) / (zp - zm);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_les_filter(const T* __restrict__ u, const T* __restrict__ v,
+                                                    const T* __restrict__ w, const T* __restrict__ p, int NX, int NY,
+                                                    int NZ, int fw, float* __restrict__ F) {
+    const int NXc = NX / fw, NYc = NY / fw;
+    const long long M = (long long)NXc * NYc * NZ;
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= M) return;
+    const int X = (int)(c % NXc), Y = (int)((c / NXc) % NYc), z = (int)(c / ((long long)NXc * NYc));
+    const size_t NXY = (size_t)NX * NY, pl = (size_t)z * NXY;
+    double s[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int dy = 0; dy < fw; dy++) {
+        const int iy = fw * Y + dy, iyp = iy + 1 == NY ? 0 : iy + 1;
+        for (int dx = 0; dx < fw; dx++) {
+            const int ix = fw * X + dx, ixp = ix + 1 == NX ? 0 : ix + 1;
+            const size_t id = pl + (size_t)iy * NX + ix;
+            const double uc = 0.5 * ((double)u[id] + (double)u[pl + (size_t)iy * NX + ixp]);
+            const double vc = 0.5 * ((double)v[id] + (double)v[pl + (size_t)iyp * NX + ix]);
+            const double wc = 0.5 * ((double)w[id] + (z + 1 < NZ ? (double)w[id + NXY] : 0.0));
+            s[0] += uc; s[1] += vc; s[2] += wc; s[3] += p ? (double)p[id] : 0.0;
+            s[4] += uc * uc; s[5] += vc * vc; s[6] += wc * wc;
+            s[7] += uc * vc; s[8] += uc * wc; s[9] += vc * wc;
+        }
+    }
+    const double inv = 1.0 / (fw * fw);
+#pragma unroll
+    for (int k = 0; k < 10; k++) F[k * M + c] = (float)(s[k] * inv);
+}
+
+// F: the 10 filtered fields of k_les_filter (layout [k][z][Y][X]).  X: M x 6, Y: M.
+__global__ void __launch_bounds__(256) k_les_features(const float* __restrict__ F, int NXc, int NYc, int NZ, double dxc,
+                                                      double dyc, const double* __restrict__ ZZ, double nu, double utau,
+                                                      float* __restrict__ Xo, float* __restrict__ Yo) {
+    const long long M = (long long)NXc * NYc * NZ;
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= M) return;
+    const int X = (int)(c % NXc), Y = (int)((c / NXc) % NYc), z = (int)(c / ((long long)NXc * NYc));
+    const long long pl = (long long)NXc * NYc;
+    const int Xp = X + 1 == NXc ? 0 : X + 1, Xm = X == 0 ? NXc - 1 : X - 1;
+    const int Yp = Y + 1 == NYc ? 0 : Y + 1, Ym = Y == 0 ? NYc - 1 : Y - 1;
+    auto at = [&](int k, int xx, int yy, int zz) -> double {
+        return (double)F[k * M + (long long)zz * pl + (long long)yy * NXc + xx];
+    };
+    double G[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        G[i][0] = (at(i, Xp, Y, z) - at(i, Xm, Y, z)) / (2 * dxc);
+        G[i][1] = (at(i, X, Yp, z) - at(i, X, Ym, z)) / (2 * dyc);
+        G[i][2] = ddz(ZZ, NZ, z, z > 0 ? at(i, X, Y, z - 1) : 0.0, z < NZ - 1 ? at(i, X, Y, z + 1) : 0.0);
+    }
+    const double zc = 0.5 * (ZZ[z] + ZZ[z + 1]);
+    const double d = fmin(zc - ZZ[0], ZZ[NZ] - zc);
+    float f[6];
+    les_features(G, nu, utau, d, f);
+#pragma unroll
+    for (int k = 0; k < 6; k++) Xo[c * 6 + k] = f[k];
+    // target: least-squares eddy viscosity of the sub-filter stress
+    const double ub[3] = {at(0, X, Y, z), at(1, X, Y, z), at(2, X, Y, z)};
+    double tau[3][3];
+    tau[0][0] = at(4, X, Y, z) - ub[0] * ub[0];
+    tau[1][1] = at(5, X, Y, z) - ub[1] * ub[1];
+    tau[2][2] = at(6, X, Y, z) - ub[2] * ub[2];
+    tau[0][1] = tau[1][0] = at(7, X, Y, z) - ub[0] * ub[1];
+    tau[0][2] = tau[2][0] = at(8, X, Y, z) - ub[0] * ub[2];
+    tau[1][2] = tau[2][1] = at(9, X, Y, z) - ub[1] * ub[2];
+    const double tr = (tau[0][0] + tau[1][1] + tau[2][2]) / 3.0;
+    double num = 0, den = 0;
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            const double Sij = 0.5 * (G[i][j] + G[j][i]);
+            num -= (tau[i][j] - (i == j ? tr : 0.0)) * Sij;
+            den += 2 * Sij * Sij;
+        }
+    const double nus = den > 1e-300 ? fmax(0.0, num / den) : 0.0;
+    Yo[c] = (float)(nus / nu);
+}
+
+// nu_t of a staggered run from the learned closure.  P: packed FP32 parameters.
+template <typename T>
+__global__ void __launch_bounds__(128) k_turb_mlp(TurbArgs<T> a, const float* __restrict__ P) {
+    __shared__ MlpSmem S;
+    __shared__ float Xs[4][16][MLP_IN];
+    mlp_load_smem(S, P);
+    __syncthreads();
+    const Geom& g = a.g;
+    const int NX = g.NX, NY = g.NY, NZ = g.NZ;
+    const size_t NXY = (size_t)NX * NY;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, gq = lane >> 2, t = lane & 3;
+    const double nu = g.visc, utau = g.inv_ls * g.visc;
+    const long long N = g.N, ntile = (N + 15) / 16;
+    for (long long tile = (long long)blockIdx.x * 4 + wid; tile < ntile; tile += (long long)gridDim.x * 4) {
+        const long long c0 = tile * 16;
+        const int nrow = (int)min(16LL, N - c0);
+        if (lane < nrow) {
+            const long long c = c0 + lane;
+            const int ix = (int)(c % NX), iy = (int)((c / NX) % NY), iz = (int)(c / NXY);
+            // cell-centred value of component k at the cell displaced by (dx, dy, dz)
+            auto cc = [&](int k, int dx, int dy, int dz) -> double {
+                const int x = ix + dx < 0 ? NX - 1 : (ix + dx >= NX ? 0 : ix + dx);
+                const int y = iy + dy < 0 ? NY - 1 : (iy + dy >= NY ? 0 : iy + dy);
+                const int zz = iz + dz;
+                const size_t id = (size_t)zz * NXY + (size_t)y * NX + x;
+                if (k == 0) return 0.5 * ((double)a.v.c[0][id] + (double)a.v.c[0][(size_t)zz * NXY + (size_t)y * NX + (x + 1 == NX ? 0 : x + 1)]);
+                if (k == 1) return 0.5 * ((double)a.v.c[1][id] + (double)a.v.c[1][(size_t)zz * NXY + (size_t)(y + 1 == NY ? 0 : y + 1) * NX + x]);
+                return 0.5 * ((double)a.v.c[2][id] + (zz + 1 < NZ ? (double)a.v.c[2][id + NXY] : 0.0));
+            };
+            double G[3][3];
+#pragma unroll
+            for (int i = 0; i < 3; i++) {
+                G[i][0] = (cc(i, 1, 0, 0) - cc(i, -1, 0, 0)) * (0.5 * g.inv_hx);
+                G[i][1] = (cc(i, 0, 1, 0) - cc(i, 0, -1, 0)) * (0.5 * g.inv_hy);
+                G[i][2] = ddz(a.m.dZZ, NZ, iz, iz > 0 ? cc(i, 0, 0, -1) : 0.0, iz < NZ - 1 ? cc(i, 0, 0, 1) : 0.0);
+            }
+            const double zc = 0.5 * (a.m.dZZ[iz] + a.m.dZZ[iz + 1]);
+            const double d = fmin(zc - a.m.dZZ[0], a.m.dZZ[NZ] - zc);
+            les_features(G, nu, utau, d, Xs[wid][lane]);
+        }
+        __syncwarp();
+        unsigned ax[4];
+        feature_fragment(&Xs[wid][0][0], MLP_IN, nrow, ax);
+        Acc64 z1, z2;
+        unsigned h1a[4][4];
+        float z3[2];
+        mlp_forward_tile(S, ax, z1, z2, h1a, z3);
+        if (t == 0) {
+            if (gq < nrow) a.nu_t[c0 + gq] = (T)(nu * softplus(z3[0]));
+            if (gq + 8 < nrow) a.nu_t[c0 + gq + 8] = (T)(nu * softplus(z3[1]));
+        }
+        __syncwarp();
+    }
+}
+
+template <typename T>
+void launch_les_filter(const T* u, const T* v, const T* w, const T* p, const Geom& g, int fw, float* F, cudaStream_t s) {
+    const long long M = (long long)(g.NX / fw) * (g.NY / fw) * g.NZ;
+    k_les_filter<T><<<(unsigned)((M + 255) / 256), 256, 0, s>>>(u, v, w, p, g.NX, g.NY, g.NZ, fw, F);
+}
+
+void launch_les_features(const float* F, const Geom& g, int fw, const double* ZZ, float* X, float* Y, cudaStream_t s) {
+    const int NXc = g.NX / fw, NYc = g.NY / fw;
+    const long long M = (long long)NXc * NYc * g.NZ;
+    k_les_features<<<(unsigned)((M + 255) / 256), 256, 0, s>>>(F, NXc, NYc, g.NZ, fw * g.hx, fw * g.hy, ZZ, g.visc,
+                                                              g.inv_ls * g.visc, X, Y);
+}
+
+template <typename T>
+void launch_turb_mlp(const TurbArgs<T>& a, const float* P, cudaStream_t s) {
+    const long long ntile = (a.g.N + 15) / 16;
+    const int nb = (int)std::max<long long>(1, std::min<long long>((ntile + 3) / 4, 148 * 8));
+    k_turb_mlp<T><<<nb, 128, 0, s>>>(a, P);
+}
+
+template void launch_les_filter<double>(const double*, const double*, const double*, const double*, const Geom&, int,
+                                        float*, cudaStream_t);
+template void launch_les_filter<float>(const float*, const float*, const float*, const float*, const Geom&, int,
+                                       float*, cudaStream_t);
+template void launch_turb_mlp<double>(const TurbArgs<double>&, const float*, cudaStream_t);
+template void launch_turb_mlp<float>(const TurbArgs<float>&, const float*, cudaStream_t);
+
+}  // namespace tc

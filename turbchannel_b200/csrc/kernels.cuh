@@ -164,6 +164,18 @@ template <typename T> void launch_soa_to_aos(CV3<T> src, double* dst, long long 
 template <typename T> void launch_d2t(const double* src, T* dst, long long n, cudaStream_t s);
 template <typename T> void launch_t2d(const T* src, double* dst, long long n, cudaStream_t s);
 
+// learned LES closure (k_les.cu, k_mlp.cu)
+template <typename T>
+void launch_les_filter(const T* u, const T* v, const T* w, const T* p, const Geom& g, int fw, float* F, cudaStream_t s);
+void launch_les_features(const float* F, const Geom& g, int fw, const double* ZZ, float* X, float* Y, cudaStream_t s);
+template <typename T> void launch_turb_mlp(const TurbArgs<T>& a, const float* P, cudaStream_t s);
+void launch_mlp_grad(const float* P, const float* X, const float* Y, long long n, float* part, float* grad,
+                     cudaStream_t s);
+void launch_mlp_adam(float* P, float* M, float* V, const float* grad, float lr, int step, cudaStream_t s);
+void launch_mlp_forward(const float* P, const float* X, long long n, float* out, cudaStream_t s);
+int mlp_grad_blocks(long long n);
+void launch_mlp_loss_acc(float* acc, const float* grad, cudaStream_t s);  // acc += loss sum in grad
+
 size_t zsolve_scratch_bytes(const Geom& g, int elem_bytes);
 size_t zfactor_bytes(const Geom& g, int elem_bytes);
 size_t zfactor_low_bytes(const Geom& g);

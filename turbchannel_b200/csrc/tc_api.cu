@@ -18,7 +18,9 @@
 #include <string>
 #include <vector>
 
+#include "../../include/turbch_les.h"
 #include "kernels.cuh"
+#include "mlp.cuh"
 
 using namespace tc;
 
@@ -214,6 +216,9 @@ struct tc_handle {
     double forcing_value = 0;
     double last_tau = 0, last_bd0 = 1;
     int turb_kind = TC_TURB_NONE;
+    float* mlp_params = nullptr;  // learned closure (TC_TURB_MLP): packed FP32 parameters
+    float* les_buf = nullptr;     // box-filter / feature scratch (tc_les_*), grown on demand
+    size_t les_bytes = 0;
     // instrumentation
     unsigned long long launches = 0;
     bool timing = false;
@@ -278,7 +283,7 @@ static const cplx<T>* twy(const tc_handle* h) { return (const cplx<T>*)h->tw + h
 
 static void free_all(tc_handle* h) {
     void* ptrs[] = {h->nu_t, h->ptmp, h->spec, h->zfac, h->zfac_low, h->mesh_t, h->mesh_d, h->tabs, h->tw, h->red, h->ticket,
-                    h->err_flag, h->planes, h->diag_part, h->stage, h->opv, h->opf, h->ops};
+                    h->err_flag, h->planes, h->diag_part, h->stage, h->opv, h->opf, h->ops, h->mlp_params, h->les_buf};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (int l = 0; l < 4; l++) {
@@ -678,7 +683,8 @@ static void poisson(tc_handle* h, const void* rhs_vec, const void* rhs_scalar, v
 template <typename T>
 static void turb_visc(tc_handle* h, const void* v) {
     TurbArgs<T> ta{h->g, mesh_dev<T>(h), cvec<T>((void*)v, h->g.N), (T*)h->nu_t};
-    launch_turb<T>(ta, h->st);
+    if (h->turb_kind == TC_TURB_MLP) launch_turb_mlp<T>(ta, h->mlp_params, h->st);
+    else launch_turb<T>(ta, h->st);
 }
 
 template <typename T>
@@ -691,7 +697,7 @@ static int step_impl(tc_handle* h, double tau, int cur, int order) {
     const T tob = (T)(tau / bd0);
     const bool coll = g.scheme == TC_SCHEME_COLLOC;
     const bool stab1 = coll && g.stab_type == 1;
-    const bool les = h->nu_t && h->turb_kind == TC_TURB_SMAGORINSKY;
+    const bool les = h->nu_t && (h->turb_kind == TC_TURB_SMAGORINSKY || h->turb_kind == TC_TURB_MLP);
     const size_t eb = h->ev_used;
     mark(h, 0, eb);
     if (les) {
@@ -820,15 +826,21 @@ extern "C" int tc_last_dpdx(tc_handle* h, double* dpdx) {
 }
 
 extern "C" int tc_set_turb_model(tc_handle* h, int kind, const void* weights) {
-    (void)weights;
     if (!h) return fail(TC_E_ARG, "tc_set_turb_model: null handle");
     if (kind == TC_TURB_NONE) {
         h->turb_kind = kind;
         return TC_OK;
     }
-    if (kind != TC_TURB_SMAGORINSKY) return fail(TC_E_ARG, "tc_set_turb_model: unknown model");
+    if (kind != TC_TURB_SMAGORINSKY && kind != TC_TURB_MLP) return fail(TC_E_ARG, "tc_set_turb_model: unknown model");
     if (h->g.visc_type == TC_VISC_CROSS) return fail(TC_E_ARG, "tc_set_turb_model: CROSS viscosity has no nu_t");
     cudaSetDevice(h->prm.device);
+    if (kind == TC_TURB_MLP) {
+        if (h->g.scheme == TC_SCHEME_COLLOC) return fail(TC_E_ARG, "tc_set_turb_model: the learned closure is for the staggered schemes");
+        if (!weights) return fail(TC_E_ARG, "tc_set_turb_model: TC_TURB_MLP needs TC_MLP_NPAR float parameters");
+        if (!h->mlp_params && cudaMalloc(&h->mlp_params, MLP_NPAR * sizeof(float)) != cudaSuccess)
+            return fail(TC_E_NOMEM, "closure parameters");
+        TC_CUDA(cudaMemcpy(h->mlp_params, weights, MLP_NPAR * sizeof(float), cudaMemcpyHostToDevice));
+    }
     if (!h->nu_t) {
         if (cudaMalloc(&h->nu_t, (size_t)h->g.N * h->esz) != cudaSuccess) return fail(TC_E_NOMEM, "nu_t allocation");
         cudaMemsetAsync(h->nu_t, 0, (size_t)h->g.N * h->esz, h->st);
@@ -1172,4 +1184,257 @@ extern "C" int tc_op_pressure_solve_static(tc_handle* h, const void* rhs, void* 
     const int rc = static_zscr(h->prm.device, &scr);
     if (rc) return rc;
     return TC_DISPATCH(h, poisson_static, h, rhs, p, scr);
+}
+
+// ---------------------------------------------------------------------------
+// Learned LES closure: training data from a run (box filter), the network's training
+// and inference, its parameters.  (include/turbch_les.h)
+// ---------------------------------------------------------------------------
+static_assert(MLP_NPAR == TC_MLP_NPAR, "parameter count of the closure");
+
+static int les_scratch(tc_handle* h, size_t bytes) {
+    if (h->les_bytes >= bytes) return TC_OK;
+    if (h->les_buf) cudaFree(h->les_buf);
+    h->les_buf = nullptr;
+    h->les_bytes = 0;
+    if (cudaMalloc((void**)&h->les_buf, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(TC_E_NOMEM, "tc_les: scratch allocation failed");
+    }
+    h->les_bytes = bytes;
+    return TC_OK;
+}
+
+static int les_check(tc_handle* h, int level, int width, const char* who) {
+    if (!h || level < 0 || level > 3) return fail(TC_E_ARG, std::string(who) + ": bad handle or level");
+    if (h->g.scheme == TC_SCHEME_COLLOC) return fail(TC_E_ARG, std::string(who) + ": staggered schemes only");
+    if (width < 1 || h->g.NX % width || h->g.NY % width)
+        return fail(TC_E_ARG, std::string(who) + ": the filter width must divide NX and NY");
+    return TC_OK;
+}
+
+template <typename T>
+static void les_filter_run(tc_handle* h, int level, int width, float* F) {
+    const size_t N = (size_t)h->g.N;
+    const T* v = (const T*)h->vel[level];
+    launch_les_filter<T>(v, v + N, v + 2 * N, (const T*)h->pres[level], h->g, width, F, h->st);
+}
+
+extern "C" int tc_les_filter(tc_handle* h, int level, int width, float* fields) {
+    int rc = les_check(h, level, width, "tc_les_filter");
+    if (rc) return rc;
+    if (!fields) return fail(TC_E_ARG, "tc_les_filter: null output");
+    cudaSetDevice(h->prm.device);
+    const size_t M = (size_t)(h->g.NX / width) * (h->g.NY / width) * h->g.NZ;
+    if ((rc = les_scratch(h, 10 * M * sizeof(float)))) return rc;
+    TC_DISPATCH(h, les_filter_run, h, level, width, h->les_buf);
+    if ((rc = check_launch("tc_les_filter"))) return rc;
+    TC_CUDA(cudaMemcpyAsync(fields, h->les_buf, 10 * M * sizeof(float), cudaMemcpyDeviceToHost, h->st));
+    TC_CUDA(cudaStreamSynchronize(h->st));
+    return TC_OK;
+}
+
+extern "C" int tc_les_samples(tc_handle* h, int level, int width, float* features, float* targets) {
+    int rc = les_check(h, level, width, "tc_les_samples");
+    if (rc) return rc;
+    if (!features || !targets) return fail(TC_E_ARG, "tc_les_samples: null output");
+    cudaSetDevice(h->prm.device);
+    const size_t M = (size_t)(h->g.NX / width) * (h->g.NY / width) * h->g.NZ;
+    if ((rc = les_scratch(h, 17 * M * sizeof(float)))) return rc;
+    float* F = h->les_buf;
+    float* X = F + 10 * M;
+    float* Y = X + 6 * M;
+    TC_DISPATCH(h, les_filter_run, h, level, width, F);
+    launch_les_features(F, h->g, width, h->mesh_d, X, Y, h->st);
+    if ((rc = check_launch("tc_les_samples"))) return rc;
+    TC_CUDA(cudaMemcpyAsync(features, X, 6 * M * sizeof(float), cudaMemcpyDeviceToHost, h->st));
+    TC_CUDA(cudaMemcpyAsync(targets, Y, M * sizeof(float), cudaMemcpyDeviceToHost, h->st));
+    TC_CUDA(cudaStreamSynchronize(h->st));
+    return TC_OK;
+}
+
+struct tc_mlp {
+    int device = 0;
+    cudaStream_t st = nullptr;
+    float *P = nullptr, *M = nullptr, *V = nullptr, *grad = nullptr, *part = nullptr, *loss = nullptr;
+    float *X = nullptr, *Y = nullptr;  // training data on the device
+    long long n = 0, part_blocks = 0, loss_cap = 0;
+    int step = 0;
+};
+
+static void mlp_free(tc_mlp* m) {
+    float* ptrs[] = {m->P, m->M, m->V, m->grad, m->part, m->loss, m->X, m->Y};
+    for (float* p : ptrs)
+        if (p) cudaFree(p);
+    if (m->st) cudaStreamDestroy(m->st);
+}
+
+// partial-gradient buffer for batches of up to n samples
+static int mlp_parts(tc_mlp* m, long long n) {
+    const long long nb = mlp_grad_blocks(n);
+    if (nb <= m->part_blocks) return TC_OK;
+    if (m->part) cudaFree(m->part);
+    m->part = nullptr;
+    m->part_blocks = 0;
+    if (cudaMalloc((void**)&m->part, (size_t)nb * (MLP_NPAR + 1) * sizeof(float)) != cudaSuccess)
+        return fail(TC_E_NOMEM, "tc_mlp: partial-gradient buffer");
+    m->part_blocks = nb;
+    return TC_OK;
+}
+
+extern "C" int tc_mlp_create(int device, unsigned long long seed, tc_mlp** out) {
+    if (!out) return fail(TC_E_ARG, "tc_mlp_create: null output");
+    *out = nullptr;
+    TC_CUDA(cudaSetDevice(device));
+    tc_mlp* m = new tc_mlp;
+    m->device = device;
+    bool ok = cudaStreamCreateWithFlags(&m->st, cudaStreamNonBlocking) == cudaSuccess;
+    for (float** p : {&m->P, &m->M, &m->V, &m->grad})
+        ok = ok && cudaMalloc((void**)p, (MLP_NPAR + 1) * sizeof(float)) == cudaSuccess;
+    if (!ok) {
+        cudaGetLastError();
+        mlp_free(m);
+        delete m;
+        return fail(TC_E_NOMEM, "tc_mlp_create: allocation failed");
+    }
+    // seeded initialisation: weights uniform in +-1/sqrt(fan_in), biases zero, b3 = -2
+    std::vector<float> P(MLP_NPAR, 0.f);
+    std::mt19937_64 gen(seed);
+    auto uni = [&](double bound) { return (float)(bound * (2.0 * (double)(gen() >> 11) * (1.0 / 9007199254740992.0) - 1.0)); };
+    for (int i = 0; i < MLP_IN * MLP_H; i++) P[MLP_OW1 + i] = uni(1.0 / std::sqrt((double)MLP_IN));
+    for (int i = 0; i < MLP_H * MLP_H; i++) P[MLP_OW2 + i] = uni(1.0 / std::sqrt((double)MLP_H));
+    for (int i = 0; i < MLP_H; i++) P[MLP_OW3 + i] = uni(1.0 / std::sqrt((double)MLP_H));
+    P[MLP_OB3] = -2.f;
+    cudaMemcpy(m->P, P.data(), MLP_NPAR * sizeof(float), cudaMemcpyHostToDevice);
+    cudaMemset(m->M, 0, (MLP_NPAR + 1) * sizeof(float));
+    cudaMemset(m->V, 0, (MLP_NPAR + 1) * sizeof(float));
+    *out = m;
+    return TC_OK;
+}
+
+extern "C" int tc_mlp_destroy(tc_mlp* m) {
+    if (!m) return TC_OK;
+    cudaSetDevice(m->device);
+    mlp_free(m);
+    delete m;
+    return TC_OK;
+}
+
+extern "C" int tc_mlp_get_params(tc_mlp* m, float* params) {
+    if (!m || !params) return fail(TC_E_ARG, "tc_mlp_get_params: null argument");
+    cudaSetDevice(m->device);
+    TC_CUDA(cudaStreamSynchronize(m->st));
+    TC_CUDA(cudaMemcpy(params, m->P, MLP_NPAR * sizeof(float), cudaMemcpyDeviceToHost));
+    return TC_OK;
+}
+
+extern "C" int tc_mlp_set_params(tc_mlp* m, const float* params) {
+    if (!m || !params) return fail(TC_E_ARG, "tc_mlp_set_params: null argument");
+    cudaSetDevice(m->device);
+    TC_CUDA(cudaStreamSynchronize(m->st));
+    TC_CUDA(cudaMemcpy(m->P, params, MLP_NPAR * sizeof(float), cudaMemcpyHostToDevice));
+    TC_CUDA(cudaMemset(m->M, 0, (MLP_NPAR + 1) * sizeof(float)));
+    TC_CUDA(cudaMemset(m->V, 0, (MLP_NPAR + 1) * sizeof(float)));
+    m->step = 0;
+    return TC_OK;
+}
+
+extern "C" int tc_mlp_set_data(tc_mlp* m, const float* features, const float* targets, long long n) {
+    if (!m || !features || !targets || n <= 0) return fail(TC_E_ARG, "tc_mlp_set_data: bad argument");
+    cudaSetDevice(m->device);
+    TC_CUDA(cudaStreamSynchronize(m->st));
+    if (m->X) cudaFree(m->X);
+    if (m->Y) cudaFree(m->Y);
+    m->X = m->Y = nullptr;
+    m->n = 0;
+    if (cudaMalloc((void**)&m->X, (size_t)n * MLP_IN * sizeof(float)) != cudaSuccess ||
+        cudaMalloc((void**)&m->Y, (size_t)n * sizeof(float)) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(TC_E_NOMEM, "tc_mlp_set_data: allocation failed");
+    }
+    TC_CUDA(cudaMemcpy(m->X, features, (size_t)n * MLP_IN * sizeof(float), cudaMemcpyHostToDevice));
+    TC_CUDA(cudaMemcpy(m->Y, targets, (size_t)n * sizeof(float), cudaMemcpyHostToDevice));
+    m->n = n;
+    return TC_OK;
+}
+
+extern "C" int tc_mlp_train(tc_mlp* m, int epochs, long long batch, float lr, float* epoch_loss) {
+    if (!m || epochs < 1 || batch < 1 || !(lr > 0.f)) return fail(TC_E_ARG, "tc_mlp_train: bad argument");
+    if (!m->X) return fail(TC_E_STATE, "tc_mlp_train: no training data (tc_mlp_set_data)");
+    cudaSetDevice(m->device);
+    const long long bsz = std::min(batch, m->n);
+    int rc = mlp_parts(m, bsz);
+    if (rc) return rc;
+    if (m->loss_cap < epochs) {
+        if (m->loss) cudaFree(m->loss);
+        m->loss = nullptr;
+        if (cudaMalloc((void**)&m->loss, (size_t)epochs * sizeof(float)) != cudaSuccess)
+            return fail(TC_E_NOMEM, "tc_mlp_train: loss buffer");
+        m->loss_cap = epochs;
+    }
+    TC_CUDA(cudaMemsetAsync(m->loss, 0, (size_t)epochs * sizeof(float), m->st));
+    for (int e = 0; e < epochs; e++) {
+        for (long long off = 0; off < m->n; off += bsz) {
+            const long long nb = std::min(bsz, m->n - off);
+            launch_mlp_grad(m->P, m->X + off * MLP_IN, m->Y + off, nb, m->part, m->grad, m->st);
+            launch_mlp_loss_acc(m->loss + e, m->grad, m->st);
+            launch_mlp_adam(m->P, m->M, m->V, m->grad, lr, ++m->step, m->st);
+        }
+    }
+    if ((rc = check_launch("tc_mlp_train"))) return rc;
+    if (epoch_loss) {
+        std::vector<float> l(epochs);
+        TC_CUDA(cudaMemcpyAsync(l.data(), m->loss, (size_t)epochs * sizeof(float), cudaMemcpyDeviceToHost, m->st));
+        TC_CUDA(cudaStreamSynchronize(m->st));
+        for (int e = 0; e < epochs; e++) epoch_loss[e] = l[e] / (float)m->n;
+    }
+    TC_CUDA(cudaStreamSynchronize(m->st));
+    return TC_OK;
+}
+
+// one gradient evaluation on host data (no update): grad[TC_MLP_NPAR], loss = mean square error
+extern "C" int tc_mlp_grad(tc_mlp* m, const float* features, const float* targets, long long n, float* grad, float* loss) {
+    if (!m || !features || !targets || n <= 0 || !grad) return fail(TC_E_ARG, "tc_mlp_grad: bad argument");
+    cudaSetDevice(m->device);
+    int rc = mlp_parts(m, n);
+    if (rc) return rc;
+    float *X = nullptr, *Y = nullptr;
+    if (cudaMalloc((void**)&X, (size_t)n * MLP_IN * sizeof(float)) != cudaSuccess ||
+        cudaMalloc((void**)&Y, (size_t)n * sizeof(float)) != cudaSuccess) {
+        cudaGetLastError();
+        if (X) cudaFree(X);
+        return fail(TC_E_NOMEM, "tc_mlp_grad: allocation failed");
+    }
+    cudaMemcpyAsync(X, features, (size_t)n * MLP_IN * sizeof(float), cudaMemcpyHostToDevice, m->st);
+    cudaMemcpyAsync(Y, targets, (size_t)n * sizeof(float), cudaMemcpyHostToDevice, m->st);
+    launch_mlp_grad(m->P, X, Y, n, m->part, m->grad, m->st);
+    std::vector<float> gbuf(MLP_NPAR + 1);
+    cudaMemcpyAsync(gbuf.data(), m->grad, (MLP_NPAR + 1) * sizeof(float), cudaMemcpyDeviceToHost, m->st);
+    const cudaError_t e = cudaStreamSynchronize(m->st);
+    cudaFree(X);
+    cudaFree(Y);
+    if (e != cudaSuccess) return fail(TC_E_CUDA, std::string("tc_mlp_grad: ") + cudaGetErrorString(e));
+    std::copy(gbuf.begin(), gbuf.begin() + MLP_NPAR, grad);
+    if (loss) *loss = gbuf[MLP_NPAR] / (float)n;
+    return TC_OK;
+}
+
+extern "C" int tc_mlp_forward(tc_mlp* m, const float* features, long long n, float* out) {
+    if (!m || !features || n <= 0 || !out) return fail(TC_E_ARG, "tc_mlp_forward: bad argument");
+    cudaSetDevice(m->device);
+    float *X = nullptr, *O = nullptr;
+    if (cudaMalloc((void**)&X, (size_t)n * MLP_IN * sizeof(float)) != cudaSuccess ||
+        cudaMalloc((void**)&O, (size_t)n * sizeof(float)) != cudaSuccess) {
+        cudaGetLastError();
+        if (X) cudaFree(X);
+        return fail(TC_E_NOMEM, "tc_mlp_forward: allocation failed");
+    }
+    cudaMemcpyAsync(X, features, (size_t)n * MLP_IN * sizeof(float), cudaMemcpyHostToDevice, m->st);
+    launch_mlp_forward(m->P, X, n, O, m->st);
+    cudaMemcpyAsync(out, O, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost, m->st);
+    const cudaError_t e = cudaStreamSynchronize(m->st);
+    cudaFree(X);
+    cudaFree(O);
+    if (e != cudaSuccess) return fail(TC_E_CUDA, std::string("tc_mlp_forward: ") + cudaGetErrorString(e));
+    return TC_OK;
 }
