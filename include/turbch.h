@@ -120,6 +120,14 @@ int tc_profiles(tc_handle* h, int level, double* out);
  * (main.cpp:313-338 calls the three separately).  Any output may be NULL. */
 int tc_diagnostics(tc_handle* h, int level, double tau, double integral[3], double* cfl, double* profiles);
 
+/* Where the diagnostics are computed (no counterpart in the reference, whose driver runs
+ * separate reduction passes after the step).  mode 0: a separate pass over the level per
+ * call (default); 1: the step's correction kernel also reduces the new level (staggered
+ * schemes, NX % 4 == 0), a diagnostics call for that level and tau only adds the planes;
+ * 2: as 1 while the caller reads the diagnostics of every step's output, as 0 otherwise.
+ * The results agree to round-off (summation order). */
+int tc_set_diag_fusion(tc_handle* h, int mode);
+
 /* Operator-level entry points on host buffers (the reference's operator methods,
  * used by its CPU/GPU self-checks, staggered/selftest.cpp:360-438). */
 int tc_op_explicit_term(tc_handle* h, const double* vel_aos, double* flux_aos);    /* ExplicitTerm    */

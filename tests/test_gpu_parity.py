@@ -147,3 +147,31 @@ def test_init_channel_matches_oracle():
         S.init_channel(2, seed=777, amp=0.1, project=True)
         O.init_channel(2, seed=777, amp=0.1, project=True)
         assert rel_err(S.download_level(2)[0], O.get_level(2)[0]) < 1e-13
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("name", ["vv4_dns", "hw2_les", "vv4_pow23"])
+def test_fused_diagnostics_match_separate_pass(name, precision):
+    """Diagnostics reduced inside the step's correction (tc_set_diag_fusion 1) agree with
+    the separate pass (mode 0) to round-off: 1e-12 (FP64) / 1e-5 (mixed) relative."""
+    import turbchannel_b200 as tb
+
+    tol = 1e-12 if precision == 0 else 1e-5
+    prod, _, zz = make_case(precision=precision, **CASES[name])
+    res = []
+    for mode in (0, 1):
+        S = tb.Solver(prod, zz)
+        S.set_diag_fusion(mode)
+        S.init_channel(0, seed=31, amp=0.2, project=True)
+        S.set_forcing(1, 1.0)
+        out = []
+        tau = 2e-3
+        for it in range(5):
+            S.Step(it * tau, tau, it % 4, min(it + 1, 3))
+            out.append(S.diagnostics((it + 1) % 4, tau))
+        res.append(out)
+        S.close()
+    for (i0, c0, p0), (i1, c1, p1) in zip(*res):
+        assert rel_err(i1, i0) < tol
+        assert abs(c1 - c0) <= tol * abs(c0)
+        assert rel_err(p1, p0) < tol

@@ -42,7 +42,7 @@ EXPORTS = [
     "tc_diagnostics", "tc_op_explicit_term", "tc_op_apply_gradient", "tc_op_apply_divergence",
     "tc_op_unapply_gradient", "tc_op_pressure_solve", "tc_op_turb_visc", "tc_set_nu_t", "tc_get_nu_t",
     "tc_init_channel", "tc_mesh_tanh", "tc_phase_timing", "tc_phase_times", "tc_launch_count",
-    "tc_op_pressure_solve_static",
+    "tc_op_pressure_solve_static", "tc_set_diag_fusion",
 ]
 # Every entry point declared in include/turbch_les.h (learned LES closure).
 EXPORTS_LES = [
@@ -99,6 +99,7 @@ def load_library(path: str = LIB_PATH):
     L.tc_phase_timing.argtypes = [vp, ip]
     L.tc_phase_times.argtypes = [vp, vp, C.POINTER(C.c_int)]
     L.tc_launch_count.argtypes = [vp, C.POINTER(C.c_ulonglong)]
+    L.tc_set_diag_fusion.argtypes = [vp, ip]
     ll = C.c_longlong
     L.tc_les_filter.argtypes = [vp, ip, ip, vp]
     L.tc_les_samples.argtypes = [vp, ip, ip, vp, vp]
@@ -284,6 +285,10 @@ class Solver:
         out = np.zeros(self.N)
         self._check(self.L.tc_get_nu_t(self.h, _ptr(out)))
         return out
+
+    def set_diag_fusion(self, mode: int):
+        """0 (default): separate diagnostics pass, 1: fused into the step, 2: fused while read every step."""
+        self._check(self.L.tc_set_diag_fusion(self.h, mode))
 
     def phase_timing(self, on: bool):
         self._check(self.L.tc_phase_timing(self.h, 1 if on else 0))

@@ -209,6 +209,9 @@ __global__ void __launch_bounds__(QX* QY) k_correct_quad(CorrArgs<T> a) {
     }
 }
 
+template <typename T, int SCHEME>
+void launch_correct_diag(const CorrArgs<T>& a, cudaStream_t s);
+
 static void column_shape(const Geom& g, dim3& grid, int& tz) {
     tz = ZC;
     grid = dim3((g.NX + KX - 1) / KX, (g.NY + KY - 1) / KY, (g.NZ + tz - 1) / tz);
@@ -216,6 +219,12 @@ static void column_shape(const Geom& g, dim3& grid, int& tz) {
 
 template <typename T, int SCHEME>
 static void correct_scheme(const CorrArgs<T>& a, cudaStream_t s) {
+    if constexpr (SCHEME != TC_SCHEME_COLLOC) {
+        if (a.dpart && !a.grad_only && !a.pnext && a.g.NX % 4 == 0) {
+            launch_correct_diag<T, SCHEME>(a, s);
+            return;
+        }
+    }
     if (!a.grad_only && a.g.NX % 4 == 0) {
         constexpr int ZN = correct_quad_planes<T>();
         const dim3 gq((a.g.NX / 4 + QX - 1) / QX, (a.g.NY + QY - 1) / QY, (a.g.NZ + ZN - 1) / ZN);
@@ -451,6 +460,167 @@ int diag_chunks(const Geom& g) {
     int S = (int)std::min<long long>(64, std::max<long long>(1, nxy / 2048));
     while (S > 1 && (long long)S * g.NZ > 148 * 32) S--;
     return S;
+}
+
+// ---------------------------------------------------------------------------
+// Correction with the diagnostics of the new level fused in (staggered schemes).
+// Same correction as k_correct_quad; each thread also corrects w on the plane above
+// its chunk (the centred w of its top plane needs it), accumulates the k_diag sums of
+// its 4 x ZN cells per plane in double, and each CTA writes one partial per plane
+// (layout of k_diag's part[z][chunk][k], chunk = the CTA's xy index) for
+// k_diag_finish.
+// ---------------------------------------------------------------------------
+int correct_diag_chunks(const Geom& g) {
+    return ((g.NX / 4 + QX - 1) / QX) * ((g.NY + QY - 1) / QY);
+}
+
+template <typename T, int SCHEME>
+__global__ void __launch_bounds__(QX* QY) k_correct_diag(CorrArgs<T> a) {
+    constexpr int ZN = correct_quad_planes<T>();
+    const Geom& g = a.g;
+    const int NX = g.NX, NY = g.NY, NZ = g.NZ, NQ = NX >> 2;
+    const size_t NXY = (size_t)NX * NY;
+    const int xq = blockIdx.x * QX + threadIdx.x % QX, iy = blockIdx.y * QY + threadIdx.x / QX;
+    const bool act = xq < NQ && iy < NY;
+    const int x = 4 * (act ? xq : 0), zb = blockIdx.z * ZN, yy = act ? iy : 0;
+    const int xl = x == 0 ? NX - 4 : x - 4, xr = x + 4 == NX ? 0 : x + 4;
+    const int ym = wrapi(yy - 1, NY), ymm = wrapi(yy - 2, NY), yp = wrapi(yy + 1, NY);
+    const T* __restrict__ p = a.p;
+    T du = 0;
+    if (a.cfr) {
+        const double ub = (*a.ub_sum) * a.cfr_scale * (double)a.tob;
+        const double d = (a.cfr_target - ub) * a.cfr_volfac;
+        du = (T)d;
+        if (blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0) *a.du_out = d;
+    }
+    const size_t row = (size_t)yy * NX;
+    Acc4<T> col[ZN + 4];  // p(zb-2 .. zb+ZN+1)
+#pragma unroll
+    for (int k = 0; k < ZN + 4; k++) {
+        const int z = zb - 2 + k;
+        if (act && z >= 0 && z < NZ) col[k] = ld4(p + (size_t)z * NXY + row + x);
+        else {
+#pragma unroll
+            for (int j = 0; j < 4; j++) col[k].v[j] = T(0);
+        }
+    }
+    T o[ZN][3][4];
+    T wtop[4] = {T(0), T(0), T(0), T(0)};  // corrected w on plane zb+ZN (0 at the top wall)
+#pragma unroll
+    for (int k = 0; k < ZN; k++) {
+        const int z = zb + k;
+        if (!act || z >= NZ) continue;
+        const size_t pl = (size_t)z * NXY;
+        const Acc4<T> pl4 = ld4(p + pl + row + xl), pr4 = ld4(p + pl + row + xr);
+        const Acc4<T> pym = ld4(p + pl + (size_t)ym * NX + x), pymm = ld4(p + pl + (size_t)ymm * NX + x),
+                      pyp = ld4(p + pl + (size_t)yp * NX + x);
+        Acc4<T> rh[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) rh[c] = ld4(a.rhs.c[c] + pl + row + x);
+        T e[12];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            e[j] = pl4.v[j];
+            e[4 + j] = col[k + 2].v[j];
+            e[8 + j] = pr4.v[j];
+        }
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            T gp[3];
+            grad_at<T, SCHEME>(a, z, NZ, e[4 + j], e[3 + j], e[2 + j], e[5 + j], pym.v[j], pymm.v[j], pyp.v[j],
+                               col[k + 1].v[j], col[k].v[j], col[k + 3].v[j], gp);
+#pragma unroll
+            for (int c = 0; c < 3; c++) o[k][c][j] = (rh[c].v[j] - gp[c]) * a.tob;
+            if (a.cfr) o[k][0][j] += du;
+        }
+#pragma unroll
+        for (int c = 0; c < 3; c++) st4(a.vout.c[c] + pl + row + x, o[k][c]);
+    }
+    if (act && zb + ZN < NZ) {  // w on the plane above: the z-component of the gradient only
+        const int z = zb + ZN;
+        const Acc4<T> rw = ld4(a.rhs.c[2] + (size_t)z * NXY + row + x);
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            T gp[3];
+            grad_at<T, SCHEME>(a, z, NZ, col[ZN + 2].v[j], T(0), T(0), T(0), T(0), T(0), T(0), col[ZN + 1].v[j],
+                               col[ZN].v[j], col[ZN + 3].v[j], gp);
+            wtop[j] = (rw.v[j] - gp[2]) * a.tob;
+        }
+    }
+    // per-plane sums (k_diag's definitions) and the CTA reduction
+    __shared__ double sb[NDIAG + 3][QX * QY / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int S = gridDim.x * gridDim.y, sidx = blockIdx.y * gridDim.x + blockIdx.x;
+    const double ihx = g.inv_hx, ihy = g.inv_hy;
+#pragma unroll
+    for (int k = 0; k < ZN; k++) {
+        const int z = zb + k;
+        if (z >= NZ) break;  // uniform over the CTA
+        // this thread's 4 cells in the working precision T (float in the mixed mode), the
+        // warp and CTA sums in double
+        T sm[NDIAG];
+#pragma unroll
+        for (int q = 0; q < NDIAG; q++) sm[q] = T(0);
+        T mconv = 0, mvisc = 0, mboth = 0;
+        const T ihz = T(1) / a.m.DZ[z], tihx = (T)ihx, tihy = (T)ihy;
+        const T lap = tihx * tihx + tihy * tihy + ihz * ihz, tau = (T)a.dtau, kv4 = (T)(4 * a.dkv);
+        if (act) {
+            const size_t id = (size_t)z * NXY + row + x;
+            Acc4<T> NT;
+            if (a.nu_t) NT = ld4(a.nu_t + id);
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const T u = o[k][0][j], v = o[k][1][j], w = o[k][2][j];
+                const T wn = k + 1 < ZN ? o[k + 1][2][j] : wtop[j];
+                const T wc = T(0.5) * (w + (z == NZ - 1 ? T(0) : wn));
+                sm[0] += u; sm[1] += v; sm[2] += wc;
+                sm[3] += u * u; sm[4] += v * v; sm[5] += wc * wc; sm[6] += u * v; sm[7] += u * wc; sm[8] += v * wc;
+                T nt = 0;
+                if (a.nu_t) {
+                    nt = NT.v[j];
+                    sm[9] += nt;
+                }
+                const T pv = col[k + 2].v[j];
+                sm[10] += pv; sm[11] += pv * pv; sm[12] += w; sm[13] += w * w;
+                const T cc = tau * (fabs(u) * tihx + fabs(v) * tihy + fabs(w) * ihz);
+                const T cv = kv4 * tau * ((T)g.visc + nt) * lap;
+                mconv = fmax(mconv, cc);
+                mvisc = fmax(mvisc, cv);
+                mboth = fmax(mboth, cc + cv);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < NDIAG; q++) {
+            const double r = warp_sum((double)sm[q]);
+            if (lane == 0) sb[q][wid] = r;
+        }
+        const double m0 = warp_max((double)mconv), m1 = warp_max((double)mvisc), m2 = warp_max((double)mboth);
+        if (lane == 0) {
+            sb[NDIAG][wid] = m0;
+            sb[NDIAG + 1][wid] = m1;
+            sb[NDIAG + 2][wid] = m2;
+        }
+        __syncthreads();
+        if (threadIdx.x < NDIAG + 3) {
+            const int q = threadIdx.x;
+            double r = sb[q][0];
+            for (int w2 = 1; w2 < QX * QY / 32; w2++) r = q < NDIAG ? r + sb[q][w2] : fmax(r, sb[q][w2]);
+            a.dpart[((size_t)z * S + sidx) * TC_DIAG_STRIDE + q] = r;
+        }
+        __syncthreads();
+    }
+}
+
+template <typename T, int SCHEME>
+void launch_correct_diag(const CorrArgs<T>& a, cudaStream_t s) {
+    constexpr int ZN = correct_quad_planes<T>();
+    const dim3 gq((a.g.NX / 4 + QX - 1) / QX, (a.g.NY + QY - 1) / QY, (a.g.NZ + ZN - 1) / ZN);
+    k_correct_diag<T, SCHEME><<<gq, QX * QY, 0, s>>>(a);
+}
+
+void launch_diag_finish(const double* part, double* planes, int NZ, int S, cudaStream_t s) {
+    const int n = NZ * TC_DIAG_STRIDE;
+    k_diag_finish<<<(n + 255) / 256, 256, 0, s>>>(part, planes, NZ, S);
 }
 
 template <typename T>

@@ -105,6 +105,12 @@ struct CorrArgs {
     const double* ub_sum;  // sum of RHS_x weights from the flux kernel
     double* du_out;        // shift applied (for tc_last_dpdx)
     int grad_only;         // operator form: vout = G p
+    // Diagnostics of the new level fused into the correction (staggered, NX % 4 == 0):
+    // per (plane, xy-CTA) partial sums in the k_diag layout; nullptr: not fused.
+    double* dpart = nullptr;
+    const T* nu_t = nullptr;  // LES eddy viscosity (diagnostics only)
+    double dtau = 0.0;        // time step of the CFL numbers
+    double dkv = 1.0;         // viscous CFL factor of the scheme's viscosity
 };
 
 template <typename T>
@@ -180,6 +186,8 @@ size_t zsolve_scratch_bytes(const Geom& g, int elem_bytes);
 size_t zfactor_bytes(const Geom& g, int elem_bytes);
 size_t zfactor_low_bytes(const Geom& g);
 int diag_chunks(const Geom& g);
+int correct_diag_chunks(const Geom& g);  // xy-CTAs per plane of the fused diagnostics
+void launch_diag_finish(const double* part, double* planes, int NZ, int S, cudaStream_t s);
 int flux_grid_blocks(const Geom& g);
 
 }  // namespace tc

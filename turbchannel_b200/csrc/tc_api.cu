@@ -217,6 +217,13 @@ struct tc_handle {
     double last_tau = 0, last_bd0 = 1;
     int turb_kind = TC_TURB_NONE;
     float* mlp_params = nullptr;  // learned closure (TC_TURB_MLP): packed FP32 parameters
+    // diagnostics fused into the step's correction (tc_set_diag_fusion)
+    int diag_fuse = 0;             // 0 off (default), 1 always, 2 when the caller reads every step's diagnostics
+    bool diag_follow = false;      // mode 2: the last step's output level was read
+    bool fused_valid = false, fused_used = false;
+    int fused_level = -1, last_out = -1;
+    double fused_tau = 0.0;
+    double* fdiag_part = nullptr;  // NZ x correct_diag_chunks x TC_DIAG_STRIDE
     float* les_buf = nullptr;     // box-filter / feature scratch (tc_les_*), grown on demand
     size_t les_bytes = 0;
     // instrumentation
@@ -283,7 +290,7 @@ static const cplx<T>* twy(const tc_handle* h) { return (const cplx<T>*)h->tw + h
 
 static void free_all(tc_handle* h) {
     void* ptrs[] = {h->nu_t, h->ptmp, h->spec, h->zfac, h->zfac_low, h->mesh_t, h->mesh_d, h->tabs, h->tw, h->red, h->ticket,
-                    h->err_flag, h->planes, h->diag_part, h->stage, h->opv, h->opf, h->ops, h->mlp_params, h->les_buf};
+                    h->err_flag, h->planes, h->diag_part, h->stage, h->opv, h->opf, h->ops, h->mlp_params, h->les_buf, h->fdiag_part};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (int l = 0; l < 4; l++) {
@@ -586,6 +593,7 @@ static int down_scal(tc_handle* h, const void* src, double* dst) {
 
 extern "C" int tc_upload_level(tc_handle* h, int level, const double* vel, const double* p) {
     if (!h || level < 0 || level > 3) return fail(TC_E_ARG, "tc_upload_level: bad handle or level");
+    if (h) h->fused_valid = false;
     cudaSetDevice(h->prm.device);
     int rc = TC_OK;
     if (vel) rc = TC_DISPATCH(h, up_vec, h, vel, h->vel[level]);
@@ -607,6 +615,7 @@ extern "C" int tc_download_flux(tc_handle* h, int level, double* f) {
     return TC_DISPATCH(h, down_vec, h, h->flux[level], f);
 }
 extern "C" int tc_device_level(tc_handle* h, int level, void** vel, void** p) {
+    if (h) h->fused_valid = false;  // the caller may write the level
     if (!h || level < 0 || level > 3) return fail(TC_E_ARG, "tc_device_level: bad handle or level");
     if (vel) *vel = h->vel[level];
     if (p) *p = h->pres[level];
@@ -630,6 +639,7 @@ extern "C" int tc_sync(tc_handle* h) {
     return TC_OK;
 }
 extern "C" int tc_set_nu_t(tc_handle* h, const double* nt) {
+    if (h) h->fused_valid = false;
     if (!h || !nt) return fail(TC_E_ARG, "tc_set_nu_t: null argument");
     if (!h->nu_t) return fail(TC_E_STATE, "tc_set_nu_t: no turbulence model configured");
     cudaSetDevice(h->prm.device);
@@ -751,8 +761,34 @@ static int step_impl(tc_handle* h, double tau, int cur, int order) {
     ca.ub_sum = h->red;
     ca.du_out = h->red + 1;
     ca.grad_only = 0;
+    // the new level's diagnostics fused into the correction: forced, or (mode 2) while the
+    // caller reads every step's diagnostics (the previous fused result was consumed)
+    if (h->fused_valid && !h->fused_used) h->diag_follow = false;
+    h->fused_valid = false;
+    bool fuse = !coll && g.NX % 4 == 0 && (h->diag_fuse == 1 || (h->diag_fuse == 2 && h->diag_follow));
+    if (fuse && !h->fdiag_part) {
+        const size_t need = (size_t)g.NZ * correct_diag_chunks(g) * TC_DIAG_STRIDE * sizeof(double);
+        if (cudaMalloc((void**)&h->fdiag_part, need) != cudaSuccess) {
+            cudaGetLastError();
+            h->fdiag_part = nullptr;
+            fuse = false;
+        }
+    }
+    if (fuse) {
+        ca.dpart = h->fdiag_part;
+        ca.nu_t = (h->nu_t && h->turb_kind != TC_TURB_NONE) ? (const T*)h->nu_t : nullptr;
+        ca.dtau = tau;
+        ca.dkv = g.visc_type != TC_VISC_CROSS ? 2.0 : 1.0;
+    }
     launch_correct<T>(ca, h->st);
     h->launches += 1;
+    if (fuse) {
+        h->fused_valid = true;
+        h->fused_used = false;
+        h->fused_level = nxt;
+        h->fused_tau = tau;
+    }
+    h->last_out = nxt;
     mark(h, 8, eb);
     if (h->timing) {
         h->ev_used += 9;
@@ -827,6 +863,7 @@ extern "C" int tc_last_dpdx(tc_handle* h, double* dpdx) {
 
 extern "C" int tc_set_turb_model(tc_handle* h, int kind, const void* weights) {
     if (!h) return fail(TC_E_ARG, "tc_set_turb_model: null handle");
+    h->fused_valid = false;
     if (kind == TC_TURB_NONE) {
         h->turb_kind = kind;
         return TC_OK;
@@ -855,6 +892,16 @@ extern "C" int tc_set_turb_model(tc_handle* h, int kind, const void* weights) {
 // ---------------------------------------------------------------------------
 template <typename T>
 static int diag_run(tc_handle* h, int level, double tau) {
+    if (h->fused_valid && level == h->fused_level && tau == h->fused_tau) {
+        launch_diag_finish(h->fdiag_part, h->planes, h->g.NZ, correct_diag_chunks(h->g), h->st);
+        h->fused_used = true;
+        TC_CUDA(cudaGetLastError());
+        TC_CUDA(cudaMemcpyAsync(h->planes_h, h->planes, (size_t)h->g.NZ * TC_DIAG_STRIDE * sizeof(double),
+                                cudaMemcpyDeviceToHost, h->st));
+        TC_CUDA(cudaStreamSynchronize(h->st));
+        return TC_OK;
+    }
+    if (h->diag_fuse == 2 && level == h->last_out) h->diag_follow = true;
     DiagArgs<T> a;
     a.g = h->g;
     a.m = mesh_dev<T>(h);
@@ -1038,6 +1085,7 @@ extern "C" int tc_op_pressure_solve(tc_handle* h, const double* rhs, double* p) 
     return TC_DISPATCH(h, op_psolve, h, rhs, p);
 }
 extern "C" int tc_op_turb_visc(tc_handle* h, const double* v, double* nt) {
+    if (h) h->fused_valid = false;
     TC_OPCHK(h, v, nt);
     if (!h->nu_t) return fail(TC_E_STATE, "tc_op_turb_visc: no turbulence model configured");
     return TC_DISPATCH(h, op_turb, h, v, nt);
@@ -1436,5 +1484,13 @@ extern "C" int tc_mlp_forward(tc_mlp* m, const float* features, long long n, flo
     cudaFree(X);
     cudaFree(O);
     if (e != cudaSuccess) return fail(TC_E_CUDA, std::string("tc_mlp_forward: ") + cudaGetErrorString(e));
+    return TC_OK;
+}
+
+extern "C" int tc_set_diag_fusion(tc_handle* h, int mode) {
+    if (!h || mode < 0 || mode > 2) return fail(TC_E_ARG, "tc_set_diag_fusion: bad handle or mode");
+    h->diag_fuse = mode;
+    h->diag_follow = false;
+    h->fused_valid = false;
     return TC_OK;
 }
