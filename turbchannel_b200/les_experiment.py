@@ -5,7 +5,9 @@ compared with the filtered-DNS mean velocity profile.
     python -m turbchannel_b200.les_experiment [--dns-steps 20000 --stat-steps 5000 ...] --out res.json
 
 1. DNS: staggered VV4, 384x256x384 cells (x, wall-normal, span), Re_b 21900, 2pi x 2 x pi,
-   tanh 2.2, dt 0.0008, constant flow rate, mixed precision, from the seeded field; spin-up,
+   tanh 2.2, dt 0.0008, constant flow rate, mixed precision, from the seeded field plus
+   large-scale vortices as a transition trigger (--vortex; the seeded noise alone decays
+   and the flow stays laminar); spin-up,
    then statistics: the mean u profile every `--stat-every` steps and, every
    `--snap-every` steps, the box-filtered snapshot (width 4 in x and span) as closure
    training samples (features, targets nu*/nu, tc_les_samples).
@@ -50,10 +52,43 @@ def restrict_to_les(vel, NX, NY, NZ, r, dz_fine):
     return out
 
 
+def add_vortices(S, p, zz, amp, seed=7):
+    """Adds large-scale vortices to ring level 0 as a transition trigger: for (kx, ky) in
+    {1, 2, 3}^2 with seeded random amplitudes and phases, u += -a cos(kx x' + f) sin(ky y' + g) G(z)
+    and v += a (Ly/Lx)(kx/ky) sin(kx x' + f) cos(ky y' + g) G(z) (x' = 2 pi x/Lx, y' = 2 pi y/Ly),
+    divergence-free mode by mode, G(z) = 1 - ((z - H)/H)^2; the total is scaled to a maximum
+    of `amp` (units of the bulk velocity).  At staggered positions; the first step's
+    projection removes the discretisation's residual divergence."""
+    NX, NY, NZ = p["NX"], p["NY"], p["NZ"]
+    v, q = S.download_level(0)
+    zc = 0.5 * (zz[:-1] + zz[1:])
+    H = 0.5 * (zz[-1] - zz[0])
+    G = (1.0 - ((zc - zz[0] - H) / H) ** 2)[:, None, None]
+    Lx, Ly = NX * p["hx"], NY * p["hy"]
+    xf, xc = np.arange(NX) * p["hx"], (np.arange(NX) + 0.5) * p["hx"]
+    yf, yc = np.arange(NY) * p["hy"], (np.arange(NY) + 0.5) * p["hy"]
+    rng = np.random.default_rng(seed)
+    du = np.zeros((NZ, NY, NX))
+    dv = np.zeros((NZ, NY, NX))
+    for kx in (1, 2, 3):
+        for ky in (1, 2, 3):
+            a, f, g = rng.uniform(0.5, 1.0), rng.uniform(0, 2 * np.pi), rng.uniform(0, 2 * np.pi)
+            ax = 2 * np.pi * kx / Lx
+            ay = 2 * np.pi * ky / Ly
+            du += -a * (np.cos(ax * xf + f)[None, None, :] * np.sin(ay * yc + g)[None, :, None]) * G
+            dv += a * (ax / ay) * (np.sin(ax * xc + f)[None, None, :] * np.cos(ay * yf + g)[None, :, None]) * G
+    sc = amp / max(np.abs(du).max(), np.abs(dv).max())
+    v[:, 0] += sc * du.reshape(-1)
+    v[:, 1] += sc * dv.reshape(-1)
+    S.upload_level(0, v, q)
+
+
 def run_dns(args, log):
     p, zz = tb.channel_params(tb.VV4, args.nx, args.ny, args.nz, LX, LY, RE_B, GAMMA, precision=tb.MIXED)
     S = tb.Solver(p, zz)
     S.init_channel(0, seed=12345, amp=0.1, project=True)
+    if args.vortex > 0:
+        add_vortices(S, p, zz, args.vortex)
     S.set_forcing(1, 1.0)
     tau, cur = args.dt, 0
     prof, nprof = np.zeros(args.nz), 0
@@ -74,7 +109,7 @@ def run_dns(args, log):
                 sel = rng.random(len(Y)) < args.sample_frac
                 Xs.append(X[sel])
                 Ys.append(Y[sel])
-        if (it + 1) % 2000 == 0:
+        if (it + 1) % 1000 == 0:
             ub = S.CalcIntegral(cur)[0] / p["area"]
             log(f"DNS step {it + 1}/{total}  Ub {ub:.5f}  dp/dx {S.last_dpdx():.5f}  {time.time() - t0:.0f} s")
     S.sync()
@@ -95,28 +130,42 @@ def run_les(args, model, params, vel0, log):
     S.upload_level(0, vel0, np.zeros(len(vel0)))
     S.set_forcing(1, 1.0)
     tau, cur = args.les_dt, 0
-    prof, nprof = np.zeros(p["NZ"]), 0
+    prof, wsum = np.zeros(p["NZ"]), 0.0
     total = args.les_steps + args.les_stat_steps
     import torch
 
     stream = torch.cuda.ExternalStream(S.stream())
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start, t, timed = 0, 0.0, False
     for it in range(total):
         if it == args.les_steps:
             e0.record(stream)
-        S.Step(it * tau, tau, cur, min(it + 1, 3))
+            timed = True
+        S.Step(t, tau, cur, min(it - start + 1, 3))
         cur = (cur + 1) % 4
+        t += tau
         if it >= args.les_steps and (it - args.les_steps) % args.stat_every == 0:
-            prof += S.CalcProfiles(cur)[:, 0]
-            nprof += 1
+            prof += tau * S.CalcProfiles(cur)[:, 0]
+            wsum += tau
+        if it % 10 == 9:  # the reference driver's CFL control (staggered/main.cpp:361-370)
+            cfl = S.CalcCFL(cur, tau, 3)
+            if not np.isfinite(cfl):
+                break
+            while cfl > args.cfl_max:
+                cfl *= 0.5
+                tau *= 0.5
+                start = it + 1
+            if cfl < args.cfl_min:
+                tau *= 1.5
+                start = it + 1
     e1.record(stream)
     e1.synchronize()
-    ms = e0.elapsed_time(e1) / max(1, args.les_stat_steps)
+    ms = e0.elapsed_time(e1) / max(1, args.les_stat_steps) if timed else float("nan")
     ub = S.CalcIntegral(cur)[0] / p["area"]
     ok = bool(np.all(np.isfinite(prof)))
     S.close()
     log(f"LES {model}: Ub {ub:.5f}, {ms:.4f} ms/step (with the per-sample profile calls)")
-    return dict(prof=prof / max(nprof, 1), ms_per_step=ms, ub=ub, finite=ok, zz=zz)
+    return dict(prof=prof / max(wsum, 1e-300), ms_per_step=ms, ub=ub, finite=ok, zz=zz, final_tau=tau)
 
 
 def main():
@@ -125,7 +174,10 @@ def main():
     ap.add_argument("--ny", type=int, default=384)
     ap.add_argument("--nz", type=int, default=256)
     ap.add_argument("--dt", type=float, default=0.0008)
-    ap.add_argument("--dns-steps", type=int, default=20000)
+    ap.add_argument("--vortex", type=float, default=0.5,
+                    help="maximum amplitude (units of the bulk velocity) of large-scale vortices added to the "
+                         "seeded field as a transition trigger; the seeded noise alone decays without transition")
+    ap.add_argument("--dns-steps", type=int, default=40000)
     ap.add_argument("--stat-steps", type=int, default=5000)
     ap.add_argument("--stat-every", type=int, default=10)
     ap.add_argument("--snap-every", type=int, default=500)
@@ -134,6 +186,8 @@ def main():
     ap.add_argument("--batch", type=int, default=4096)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--les-dt", type=float, default=0.002)
+    ap.add_argument("--cfl-min", type=float, default=0.1)
+    ap.add_argument("--cfl-max", type=float, default=0.4)
     ap.add_argument("--les-steps", type=int, default=10000)
     ap.add_argument("--les-stat-steps", type=int, default=10000)
     ap.add_argument("--out", default="les_experiment.json")
