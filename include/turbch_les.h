@@ -24,15 +24,17 @@ extern "C" {
 
 #define TC_MLP_NPAR 4673
 
-/* Box filter of width `width` in x and y (must divide NX and NY) of ring level `level`:
- * 10 fields of M = (NX/width)(NY/width)NZ floats, field-major, cells [z][Y][X]: the
- * means of the cell-centred u, v, w, p, then of uu, vv, ww, uv, uw, vw. */
-int tc_les_filter(tc_handle* h, int level, int width, float* fields);
+/* Box filter of width `width` cells in x and y (must divide NX and NY) and `width_z`
+ * cells in z (must divide NZ; volume-weighted by the cell heights, so the coarse cells are
+ * those of the grid with every width_z-th z-face) of ring level `level`: 10 fields of
+ * M = (NX/width)(NY/width)(NZ/width_z) floats, field-major, cells [Z][Y][X]: the means of
+ * the cell-centred u, v, w, p, then of uu, vv, ww, uv, uw, vw. */
+int tc_les_filter(tc_handle* h, int level, int width, int width_z, float* fields);
 
 /* Training samples of the closure from the same filter: features[M][6] (above) and
  * targets[M] = nu* / nu, nu* = max(0, -tau^d_ij S_ij / (2 S_kl S_kl)) the least-squares
  * eddy viscosity of the sub-filter stress tau_ij = <u_i u_j> - <u_i><u_j>. */
-int tc_les_samples(tc_handle* h, int level, int width, float* features, float* targets);
+int tc_les_samples(tc_handle* h, int level, int width, int width_z, float* features, float* targets);
 
 typedef struct tc_mlp tc_mlp;
 /* A network on `device` with seeded initial parameters (weights uniform in

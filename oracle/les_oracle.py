@@ -42,15 +42,19 @@ def cell_centred(vel, NX, NY, NZ):
     return np.stack([uc, vc, wc])
 
 
-def box_filter(vel, p, NX, NY, NZ, fw):
-    """The 10 filtered fields [k][z][Y][X] of k_les_filter (float64)."""
+def box_filter(vel, p, NX, NY, NZ, fw, fz=1, ZZ=None):
+    """The 10 filtered fields [k][Z][Y][X] of k_les_filter (float64): means over fw x fw
+    cells in x, y and, weighted by the cell heights ZZ[z+1] - ZZ[z], over fz cells in z."""
     c = cell_centred(vel, NX, NY, NZ)
     pp = p.reshape(NZ, NY, NX)
     q = [c[0], c[1], c[2], pp, c[0] * c[0], c[1] * c[1], c[2] * c[2], c[0] * c[1], c[0] * c[2], c[1] * c[2]]
+    hz = np.ones(NZ) if ZZ is None else np.diff(np.asarray(ZZ, dtype=np.float64))
+    wz = hz.reshape(NZ // fz, fz)
+    wz = wz / wz.sum(axis=1, keepdims=True)
     out = []
     for a in q:
-        b = a.reshape(NZ, NY // fw, fw, NX // fw, fw).mean(axis=(2, 4))
-        out.append(b)
+        b = a.reshape(NZ // fz, fz, NY // fw, fw, NX // fw, fw).mean(axis=(3, 5))
+        out.append(np.einsum("zkyx,zk->zyx", b, wz))
     return np.stack(out)
 
 

@@ -29,18 +29,20 @@ def _solver(scheme, NX, NY, NZ, precision, turb=0, steps=3):
     return S, prod, zz, steps % 4
 
 
+@pytest.mark.parametrize("fz", [1, 4])
 @pytest.mark.parametrize("precision", [0, 1])
-def test_filter_and_samples_match_oracle(precision):
+def test_filter_and_samples_match_oracle(precision, fz):
     S, p, zz, lev = _solver(VV4, 32, 16, 24, precision)
     fw = 4
     vel, pr = S.download_level(lev)
-    F = S.les_filter(lev, fw)
-    Fo = lo.box_filter(vel, pr, 32, 16, 24, fw)
+    F = S.les_filter(lev, fw, fz)
+    Fo = lo.box_filter(vel, pr, 32, 16, 24, fw, fz, np.asarray(zz))
     for k in range(10):
         assert rel_err(F[k], Fo[k]) < 1e-5, k
-    X, Y = S.les_samples(lev, fw)
+    X, Y = S.les_samples(lev, fw, fz)
     utau = p["inv_length_scale"] * p["visc"]
-    Xo, Yo = lo.features_targets(Fo, 8, 4, 24, fw * p["hx"], fw * p["hy"], np.asarray(zz), p["visc"], utau)
+    Xo, Yo = lo.features_targets(Fo, 8, 4, 24 // fz, fw * p["hx"], fw * p["hy"], np.asarray(zz)[::fz], p["visc"],
+                                 utau)
     for k in range(6):
         assert rel_err(X[:, k], Xo[:, k]) < 1e-5, k
     assert np.max(np.abs(Y - Yo)) <= 1e-4 * max(np.max(np.abs(Yo)), 1e-30)

@@ -61,3 +61,33 @@ def test_linear_shear_filters_to_zero_subfilter_stress():
     assert np.allclose(X[:, 1], -X[:, 0])
     d = np.minimum(zc - ZZ[0], ZZ[NZ] - zc)
     assert np.allclose(X.reshape(NZ, -1, 6)[:, 0, 5], 0.25 * np.log1p(d * 0.05 / 1e-3))
+
+
+def test_wall_normal_filter_is_volume_weighted():
+    """fz > 1: each coarse cell holds the volume-weighted mean of its fz x fw x fw fine
+    cells (domain integrals are kept), a z-only field gets the variance within the coarse
+    cell as its uu sub-filter stress, and fz = 1 is the x-y filter alone."""
+    NX, NY, NZ, fw, fz = 8, 8, 12, 2, 4
+    ZZ = 1.0 + np.tanh(1.8 * (2.0 * np.arange(NZ + 1) / NZ - 1.0)) / np.tanh(1.8)
+    hz = np.diff(ZZ)
+    rng = np.random.default_rng(3)
+    vel = rng.normal(size=(NX * NY * NZ, 3))
+    vel[:NX * NY, 2] = 0.0  # w = 0 on the bottom wall
+    p = rng.normal(size=NX * NY * NZ)
+    F = lo.box_filter(vel, p, NX, NY, NZ, fw, fz, ZZ)
+    assert F.shape == (10, NZ // fz, NY // fw, NX // fw)
+    c = lo.cell_centred(vel, NX, NY, NZ)
+    Hc = hz.reshape(-1, fz).sum(axis=1)
+    for k in range(3):
+        fine = np.sum(c[k] * hz[:, None, None])
+        coarse = np.sum(F[k] * Hc[:, None, None]) * fw * fw
+        assert abs(fine - coarse) <= 1e-12 * max(1.0, abs(fine))
+    assert np.allclose(lo.box_filter(vel, p, NX, NY, NZ, fw, 1, ZZ), lo.box_filter(vel, p, NX, NY, NZ, fw))
+    zc = 0.5 * (ZZ[:-1] + ZZ[1:])
+    v2 = np.zeros_like(vel)
+    v2[:, 0] = np.repeat(zc, NX * NY)
+    F2 = lo.box_filter(v2, np.zeros(len(p)), NX, NY, NZ, fw, fz, ZZ)
+    wz = (hz / np.repeat(Hc, fz)).reshape(-1, fz)
+    m = (zc.reshape(-1, fz) * wz).sum(axis=1)
+    var = ((zc.reshape(-1, fz) - m[:, None]) ** 2 * wz).sum(axis=1)
+    assert np.allclose(F2[0][:, 0, 0], m) and np.allclose(F2[4][:, 0, 0] - m * m, var)

@@ -101,8 +101,8 @@ def load_library(path: str = LIB_PATH):
     L.tc_launch_count.argtypes = [vp, C.POINTER(C.c_ulonglong)]
     L.tc_set_diag_fusion.argtypes = [vp, ip]
     ll = C.c_longlong
-    L.tc_les_filter.argtypes = [vp, ip, ip, vp]
-    L.tc_les_samples.argtypes = [vp, ip, ip, vp, vp]
+    L.tc_les_filter.argtypes = [vp, ip, ip, ip, vp]
+    L.tc_les_samples.argtypes = [vp, ip, ip, ip, vp, vp]
     L.tc_mlp_create.argtypes = [ip, C.c_ulonglong, C.POINTER(vp)]
     L.tc_mlp_destroy.argtypes = [vp]
     L.tc_mlp_get_params.argtypes = [vp, vp]
@@ -209,19 +209,20 @@ class Solver:
         self._check(self.L.tc_set_turb_model(self.h, kind, None if w is None else _ptr(w)))
 
     # ---- learned closure: training data ----
-    def les_filter(self, level: int, width: int = 4):
-        """Box filter (width in x and y): 10 fields [k][z][Y][X] (u, v, w, p, uu, vv, ww, uv, uw, vw)."""
-        M = (self.NX // width) * (self.NY // width) * self.NZ
+    def les_filter(self, level: int, width: int = 4, width_z: int = 1):
+        """Box filter (width cells in x and y, width_z in z): 10 fields [k][Z][Y][X]
+        (u, v, w, p, uu, vv, ww, uv, uw, vw)."""
+        M = (self.NX // width) * (self.NY // width) * (self.NZ // width_z)
         out = np.zeros(10 * M, dtype=np.float32)
-        self._check(self.L.tc_les_filter(self.h, level, width, _ptr(out)))
-        return out.reshape(10, self.NZ, self.NY // width, self.NX // width)
+        self._check(self.L.tc_les_filter(self.h, level, width, width_z, _ptr(out)))
+        return out.reshape(10, self.NZ // width_z, self.NY // width, self.NX // width)
 
-    def les_samples(self, level: int, width: int = 4):
+    def les_samples(self, level: int, width: int = 4, width_z: int = 1):
         """Closure training samples of the filtered level: features (M, 6), targets nu*/nu (M,)."""
-        M = (self.NX // width) * (self.NY // width) * self.NZ
+        M = (self.NX // width) * (self.NY // width) * (self.NZ // width_z)
         X = np.zeros((M, 6), dtype=np.float32)
         Y = np.zeros(M, dtype=np.float32)
-        self._check(self.L.tc_les_samples(self.h, level, width, _ptr(X), _ptr(Y)))
+        self._check(self.L.tc_les_samples(self.h, level, width, width_z, _ptr(X), _ptr(Y)))
         return X, Y
 
     # ---- diagnostics ----

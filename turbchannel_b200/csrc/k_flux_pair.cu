@@ -32,13 +32,14 @@ __device__ __forceinline__ F2& operator+=(F2& a, F2 b) { return a = a + b; }
 __device__ __forceinline__ F2& operator-=(F2& a, F2 b) { return a = a - b; }
 __device__ __forceinline__ F2& operator*=(F2& a, F2 b) { return a = a * b; }
 
-constexpr int PTX = 32, PTY = 8;  // threads per CTA
-constexpr int PCX = 2 * PTX;      // cells per tile along x
-constexpr int PSG = 4;            // x-halo (whole 16-byte chunks)
+constexpr int PTX = 32;        // threads along x (two cells each)
+constexpr int PTR = 8;         // tile rows along y (RY rows per thread)
+constexpr int PCX = 2 * PTX;   // cells per tile along x
+constexpr int PSG = 4;         // x-halo (whole 16-byte chunks)
 
 template <int H>
 struct RingX2 {
-    static constexpr int PW = PCX + 2 * PSG, PH = PTY + 2 * H, PL = PW * PH, RS = 2 * H + 2;
+    static constexpr int PW = PCX + 2 * PSG, PH = PTR + 2 * H, PL = PW * PH, RS = 2 * H + 2;
     const float* p[2 * H + 1];  // (slot of plane z+dz, component 0, this pair)
     __device__ __forceinline__ void set(const float* r, int zs, int tx, int ty) {
         const float* c = r + (ty + H) * PW + 2 * tx + PSG;
@@ -53,19 +54,19 @@ struct RingX2 {
     }
 };
 
-// This thread's share of the 16-byte chunks of one plane of the tile (3 components,
-// PH rows, PW/4 chunks per row, periodic wrap in x and y).
-template <int H>
+// This thread's share (NT threads) of the 16-byte chunks of one plane of the tile
+// (3 components, PH rows, PW/4 chunks per row, periodic wrap in x and y).
+template <int H, int NT>
 struct TileCopyX2 {
     using ACC = RingX2<H>;
     static constexpr int NCH = ACC::PW / 4, PER = ACC::PH * NCH, TOTAL = 3 * PER;
-    static constexpr int NK = (TOTAL + PTX * PTY - 1) / (PTX * PTY);
+    static constexpr int NK = (TOTAL + NT - 1) / NT;
     int sofs[NK];
     unsigned gofs[NK];  // < 2^32: checked on the host (3 N elements)
     __device__ __forceinline__ void init(int x0, int y0, int NX, int NY, long long N) {
 #pragma unroll
         for (int k = 0; k < NK; k++) {
-            const int e = threadIdx.x + k * PTX * PTY;
+            const int e = threadIdx.x + k * NT;
             if (e < TOTAL) {
                 const int c = e / PER, r = e - c * PER, py = r / NCH, ch = r - py * NCH;
                 const int gy = wrapi(y0 - H + py, NY), gx = wrapi(x0 - PSG + ch * 4, NX);
@@ -88,30 +89,169 @@ struct TileCopyX2 {
 
 __device__ __forceinline__ F2 ld2(const float* p) { return F2(__ldg(reinterpret_cast<const float2*>(p))); }
 __device__ __forceinline__ void st2(float* p, F2 v) { *reinterpret_cast<float2*>(p) = v.v; }
+__device__ __forceinline__ F2 fma2(F2 a, F2 b, F2 c) { return F2(__ffma2_rn(a.v, b.v, c.v)); }
 
-template <int SCHEME, int ORDER>
-__global__ void __launch_bounds__(PTX* PTY, 2) k_flux_pair(FluxArgs<float> a, int tz) {
+// ---------------------------------------------------------------------------------
+// Interior planes of VV4 with the CROSS viscosity (3 <= z <= NZ-4): the arithmetic of
+// conv_vv4 / visc_cross (INT = true) regrouped for packed FMAs, with the plane
+// constants K of MeshDev::FK (host-computed in double, see fill_flux_pair_consts):
+// every fourth-order interpolant 9 s - t is formed negated, t - 9 s (one FFMA2, no
+// negation needed), a face pair's fluxes Ir pr - Il pl as nl pl - nr pr, and each
+// direction's narrow and wide pairs are accumulated with their scale factors (the
+// reference's dz hy, C27 dzw hy, ... times the plane's momentum or w scale) folded
+// into K.  Same stencils and face fluxes as the reference (staggered/func_global.h:
+// 374-529 and 533-562); only the rounding order differs.
+
+// t - 9 s
+__device__ __forceinline__ F2 ni(F2 s, F2 t) { return fma2(F2(-9.f), s, t); }
+// nl pl - nr pr
+__device__ __forceinline__ F2 pd(F2 nl, F2 pl, F2 nr, F2 pr) { return nl * pl - nr * pr; }
+
+#define U(a, b, c) A(0, a, b, c)
+#define V(a, b, c) A(1, a, b, c)
+#define W(a, b, c) A(2, a, b, c)
+template <class ACC>
+__device__ __forceinline__ void visc_cross_int(const ACC& A, const F2* K, F2 s[3]) {
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        const F2 v0 = A(c, 0, 0, 0);
+        const F2 tx = fma2(F2(-2.f), v0, A(c, 1, 0, 0) + A(c, -1, 0, 0));
+        const F2 ty = fma2(F2(-2.f), v0, A(c, 0, 1, 0) + A(c, 0, -1, 0));
+        F2 r = fma2(K[22], tx, s[c]);
+        r = fma2(K[23], ty, r);
+        r = fma2(K[c < 2 ? 18 : 20], A(c, 0, 0, 1) - v0, r);
+        s[c] = fma2(K[c < 2 ? 19 : 21], A(c, 0, 0, -1) - v0, r);
+    }
+}
+
+template <class ACC>
+__device__ __forceinline__ void conv_vv4_int(const ACC& A, const F2* K, F2 s[3]) {
+    {  // u: x-faces
+        const F2 U0 = U(0, 0, 0), Um1 = U(-1, 0, 0), Up1 = U(1, 0, 0), Um2 = U(-2, 0, 0), Up2 = U(2, 0, 0);
+        const F2 a = U0 + Up1, c = Um1 + U0;
+        const F2 dn = pd(ni(c, Um2 + Up1), c, ni(a, Um1 + Up2), a);
+        const F2 ppr = U0 + U(3, 0, 0), ppl = U(-3, 0, 0) + U0;
+        const F2 dw = pd(ni(Um2 + Um1, ppl), ppl, ni(Up1 + Up2, ppr), ppr);
+        s[0] = fma2(K[0], dn, s[0]);
+        s[0] = fma2(K[1], dw, s[0]);
+    }
+    {  // u: y-faces, v interpolated in x to the rows -1..2
+        const F2 U0 = U(0, 0, 0);
+        auto J = [&](int r) { return ni(V(0, r, 0) + V(-1, r, 0), V(-2, r, 0) + V(1, r, 0)); };
+        const F2 dn = pd(J(0), U(0, -1, 0) + U0, J(1), U0 + U(0, 1, 0));
+        const F2 dw = pd(J(-1), U(0, -3, 0) + U0, J(2), U0 + U(0, 3, 0));
+        s[0] = fma2(K[2], dn, s[0]);
+        s[0] = fma2(K[3], dw, s[0]);
+    }
+    {  // u: z-faces, w interpolated in x to the planes -1..2
+        const F2 U0 = U(0, 0, 0);
+        auto Kx = [&](int p) { return ni(W(0, 0, p) + W(-1, 0, p), W(-2, 0, p) + W(1, 0, p)); };
+        const F2 dn = pd(Kx(0), U(0, 0, -1) + U0, Kx(1), U0 + U(0, 0, 1));
+        const F2 dw = pd(Kx(-1), U0 + U(0, 0, -3), Kx(2), U0 + U(0, 0, 3));
+        s[0] = fma2(K[4], dn, s[0]);
+        s[0] = fma2(K[5], dw, s[0]);
+    }
+    {  // v: x-faces, u interpolated in y to the columns -1..2
+        const F2 V0 = V(0, 0, 0);
+        auto L = [&](int c) { return ni(U(c, 0, 0) + U(c, -1, 0), U(c, -2, 0) + U(c, 1, 0)); };
+        const F2 dn = pd(L(0), V(-1, 0, 0) + V0, L(1), V0 + V(1, 0, 0));
+        const F2 dw = pd(L(-1), V(-3, 0, 0) + V0, L(2), V0 + V(3, 0, 0));
+        s[1] = fma2(K[0], dn, s[1]);
+        s[1] = fma2(K[1], dw, s[1]);
+    }
+    {  // v: y-faces
+        const F2 V0 = V(0, 0, 0), Vm1 = V(0, -1, 0), Vp1 = V(0, 1, 0), Vm2 = V(0, -2, 0), Vp2 = V(0, 2, 0);
+        const F2 a = V0 + Vp1, c = Vm1 + V0;
+        const F2 dn = pd(ni(c, Vm2 + Vp1), c, ni(a, Vm1 + Vp2), a);
+        const F2 ppr = V0 + V(0, 3, 0), ppl = V(0, -3, 0) + V0;
+        const F2 dw = pd(ni(Vm2 + Vm1, ppl), ppl, ni(Vp1 + Vp2, ppr), ppr);
+        s[1] = fma2(K[2], dn, s[1]);
+        s[1] = fma2(K[3], dw, s[1]);
+    }
+    {  // v: z-faces, w interpolated in y to the planes -1..2
+        const F2 V0 = V(0, 0, 0);
+        auto Ky = [&](int p) { return ni(W(0, 0, p) + W(0, -1, p), W(0, -2, p) + W(0, 1, p)); };
+        const F2 dn = pd(Ky(0), V(0, 0, -1) + V0, Ky(1), V0 + V(0, 0, 1));
+        const F2 dw = pd(Ky(-1), V0 + V(0, 0, -3), Ky(2), V0 + V(0, 0, 3));
+        s[1] = fma2(K[4], dn, s[1]);
+        s[1] = fma2(K[5], dw, s[1]);
+    }
+    {  // w: x-faces, u interpolated in z (cell-height weights) to the w-face, columns -1..2
+        const F2 W0 = W(0, 0, 0);
+        auto M = [&](int c) {
+            return fma2(K[11], U(c, 0, -1), fma2(K[10], U(c, 0, 0), fma2(K[13], U(c, 0, 1), K[12] * U(c, 0, -2))));
+        };
+        auto MW = [&](int c) {
+            return fma2(K[15], U(c, 0, -1), fma2(K[14], U(c, 0, 0), fma2(K[17], U(c, 0, 1), K[16] * U(c, 0, -2))));
+        };
+        const F2 dn = pd(M(0), W(-1, 0, 0) + W0, M(1), W0 + W(1, 0, 0));
+        const F2 dw = pd(MW(-1), W(-3, 0, 0) + W0, MW(2), W0 + W(3, 0, 0));
+        s[2] = fma2(K[6], dn, s[2]);
+        s[2] = fma2(K[7], dw, s[2]);
+    }
+    {  // w: y-faces, v interpolated in z to the w-face, rows -1..2
+        const F2 W0 = W(0, 0, 0);
+        auto M = [&](int r) {
+            return fma2(K[11], V(0, r, -1), fma2(K[10], V(0, r, 0), fma2(K[13], V(0, r, 1), K[12] * V(0, r, -2))));
+        };
+        auto MW = [&](int r) {
+            return fma2(K[15], V(0, r, -1), fma2(K[14], V(0, r, 0), fma2(K[17], V(0, r, 1), K[16] * V(0, r, -2))));
+        };
+        const F2 dn = pd(M(0), W(0, -1, 0) + W0, M(1), W0 + W(0, 1, 0));
+        const F2 dw = pd(MW(-1), W(0, -3, 0) + W0, MW(2), W0 + W(0, 3, 0));
+        s[2] = fma2(K[6], dn, s[2]);
+        s[2] = fma2(K[7], dw, s[2]);
+    }
+    {  // w: z-faces
+        const F2 W0 = W(0, 0, 0), Wm1 = W(0, 0, -1), Wp1 = W(0, 0, 1), Wm2 = W(0, 0, -2), Wp2 = W(0, 0, 2);
+        const F2 pr = W0 + Wp1, pl = Wm1 + W0;
+        const F2 dn = pd(ni(pl, Wm2 + Wp1), pl, ni(pr, Wm1 + Wp2), pr);
+        const F2 ppr = W0 + W(0, 0, 3), ppl = W(0, 0, -3) + W0;
+        const F2 dw = pd(ni(Wm2 + Wm1, ppl), ppl, ni(Wp1 + Wp2, ppr), ppr);
+        s[2] = fma2(K[8], dn, s[2]);
+        s[2] = fma2(K[9], dw, s[2]);
+    }
+}
+#undef U
+#undef V
+#undef W
+
+// RY: tile rows per thread (1: 256 threads; 2: 128 threads whose two rows share the
+// loads of their y-stencils, which the compiler merges as equal shared addresses).
+template <int SCHEME, int ORDER, int RY>
+__global__ void __launch_bounds__(PTX * PTR / RY, 2) k_flux_pair(FluxArgs<float> a, int tz) {
     constexpr int H = SCHEME == TC_SCHEME_VV4 ? 3 : 1;
+    constexpr int NT = PTX * PTR / RY;
     using ACC = RingX2<H>;
     constexpr int RS = ACC::RS;
     extern __shared__ __align__(16) unsigned char smraw[];
     float* ring = reinterpret_cast<float*>(smraw);
     __shared__ double sbuf[32];
+    __shared__ __align__(16) float fks[2][TC_FK];  // plane constants of z and z+1 (VV4)
+    constexpr bool FAST = SCHEME == TC_SCHEME_VV4;
 
     const Geom& g = a.g;
     const int NX = g.NX, NY = g.NY, NZ = g.NZ;
     const size_t NXY = (size_t)NX * NY;
     const int tx = threadIdx.x % PTX, ty = threadIdx.x / PTX;
-    const int x0 = blockIdx.x * PCX, y0 = blockIdx.y * PTY;
+    const int x0 = blockIdx.x * PCX, y0 = blockIdx.y * PTR;
     const int zb = blockIdx.z * tz, ze = min(NZ, zb + tz);
-    const int ix = x0 + 2 * tx, iy = y0 + ty;
-    const bool act = ix < NX && iy < NY;  // NX is even: both cells or neither
+    const int ix = x0 + 2 * tx;
+    int iy[RY];
+    bool act[RY];  // NX is even: both cells of a pair or neither
+#pragma unroll
+    for (int r = 0; r < RY; r++) {
+        iy[r] = y0 + RY * ty + r;
+        act[r] = ix < NX && iy[r] < NY;
+    }
     const int zlo = SCHEME == TC_SCHEME_VV4 ? 3 : 1, zhi = SCHEME == TC_SCHEME_VV4 ? NZ - 4 : NZ - 2;
 
-    TileCopyX2<H> cp;
+    TileCopyX2<H, NT> cp;
     cp.init(x0, y0, NX, NY, g.N);
     const float* vbase = a.vel.c[0];
     for (int z = max(0, zb - H); z <= min(NZ - 1, zb + H); z++) cp.load(ring, vbase, z, NXY);
+    if (FAST && threadIdx.x < TC_FK / 4 && zb < NZ)
+        cp_async<16>(&fks[zb & 1][4 * threadIdx.x], a.m.FK + (size_t)TC_FK * zb + 4 * threadIdx.x);
     cp_async_commit();
 
     StagZ<float> mz;
@@ -124,65 +264,92 @@ __global__ void __launch_bounds__(PTX* PTY, 2) k_flux_pair(FluxArgs<float> a, in
     mz.ihy = (float)g.inv_hy;
     mz.visc = (float)g.visc;
     const F2 inv_tau(a.inv_tau);
+    const float sour = (float)g.sour_dpdx;
+    const F2 it3(3.f * a.inv_tau), itm15(-1.5f * a.inv_tau), it13(a.inv_tau * 0.33333333333333333333f);
     double ub = 0.0;
 
     for (int z = zb; z < ze; z++) {
         if (z + 1 < ze && z + H + 1 < NZ) cp.load(ring, vbase, z + H + 1, NXY);
+        if (FAST && z + 1 < ze && threadIdx.x < TC_FK / 4)
+            cp_async<16>(&fks[(z + 1) & 1][4 * threadIdx.x], a.m.FK + (size_t)TC_FK * (z + 1) + 4 * threadIdx.x);
         cp_async_commit();
-        const size_t id = (size_t)z * NXY + (size_t)iy * NX + ix;
-        F2 hp[3], hq[3], vp[3], vq[3];
-        if (ORDER >= 2 && act) {
+        size_t id[RY];
+        F2 hp[RY][3], hq[RY][3], vp[RY][3], vq[RY][3];
 #pragma unroll
-            for (int c = 0; c < 3; c++) {
-                hp[c] = ld2(a.fp.c[c] + id);
-                vp[c] = ld2(a.velp.c[c] + id);
-                if (ORDER == 3) {
-                    hq[c] = ld2(a.fq.c[c] + id);
-                    vq[c] = ld2(a.velq.c[c] + id);
+        for (int r = 0; r < RY; r++) {
+            id[r] = (size_t)z * NXY + (size_t)iy[r] * NX + ix;
+            if (ORDER >= 2 && act[r]) {
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    hp[r][c] = ld2(a.fp.c[c] + id[r]);
+                    vp[r][c] = ld2(a.velp.c[c] + id[r]);
+                    if (ORDER == 3) {
+                        hq[r][c] = ld2(a.fq.c[c] + id[r]);
+                        vq[r][c] = ld2(a.velq.c[c] + id[r]);
+                    }
                 }
             }
         }
         cp_async_wait<1>();
         __syncthreads();
-        mz.iz = z;
+        const bool inner = z >= zlo && z <= zhi;
+        ACC A[RY];
+        F2 f[RY][3];
 #pragma unroll
-        for (int k = 0; k < 6; k++) mz.pc[k] = a.m.PC[TC_PC * z + k];
-        const float gcz = SCHEME == TC_SCHEME_VV4 ? a.m.GCZ[z] : 0.f;
-        if (act) {
-            ACC A;
-            A.set(ring, z & (RS - 1), tx, ty);
-            F2 cf[3], vf[3];
-            if (z >= zlo && z <= zhi) {
-                if constexpr (SCHEME == TC_SCHEME_VV4) conv_vv4<float, ACC, true, F2>(A, mz, gcz, cf);
-                else conv_hw2<float, ACC, true, F2>(A, mz, cf);
-                visc_cross<float, ACC, true, F2>(A, mz, vf);
-            } else {
-                if constexpr (SCHEME == TC_SCHEME_VV4) conv_vv4<float, ACC, false, F2>(A, mz, gcz, cf);
-                else conv_hw2<float, ACC, false, F2>(A, mz, cf);
-                visc_cross<float, ACC, false, F2>(A, mz, vf);
+        for (int r = 0; r < RY; r++) A[r].set(ring, z & (RS - 1), tx, RY * ty + r);
+        if (FAST && inner) {
+            const F2* K = reinterpret_cast<const F2*>(fks[z & 1]);
+#pragma unroll
+            for (int r = 0; r < RY; r++) {
+                f[r][0] = F2(sour);
+                f[r][1] = f[r][2] = F2(0.f);
+                visc_cross_int(A[r], K, f[r]);
+                conv_vv4_int(A[r], K, f[r]);
             }
-            F2 f[3];
-            f[0] = (F2((float)g.sour_dpdx) + cf[0]) + vf[0];
-            f[1] = (F2(0.f) + cf[1]) + vf[1];
-            f[2] = (F2(0.f) + cf[2]) + vf[2];
-            if (z == 0) f[2] = F2(0.f);
+        } else {
+            mz.iz = z;
 #pragma unroll
-            for (int c = 0; c < 3; c++) st2(a.fout.c[c] + id, f[c]);
+            for (int k = 0; k < 6; k++) mz.pc[k] = a.m.PC[TC_PC * z + k];
+            const float gcz = SCHEME == TC_SCHEME_VV4 ? a.m.GCZ[z] : 0.f;
+#pragma unroll
+            for (int r = 0; r < RY; r++) {
+                F2 cf[3], vf[3];
+                if (inner) {
+                    if constexpr (SCHEME == TC_SCHEME_VV4) conv_vv4<float, ACC, true, F2>(A[r], mz, gcz, cf);
+                    else conv_hw2<float, ACC, true, F2>(A[r], mz, cf);
+                    visc_cross<float, ACC, true, F2>(A[r], mz, vf);
+                } else {
+                    if constexpr (SCHEME == TC_SCHEME_VV4) conv_vv4<float, ACC, false, F2>(A[r], mz, gcz, cf);
+                    else conv_hw2<float, ACC, false, F2>(A[r], mz, cf);
+                    visc_cross<float, ACC, false, F2>(A[r], mz, vf);
+                }
+                f[r][0] = (F2(sour) + cf[0]) + vf[0];
+                f[r][1] = (F2(0.f) + cf[1]) + vf[1];
+                f[r][2] = (F2(0.f) + cf[2]) + vf[2];
+                if (z == 0) f[r][2] = F2(0.f);
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < RY; r++) {
+            if (!act[r]) continue;
+#pragma unroll
+            for (int c = 0; c < 3; c++) st2(a.fout.c[c] + id[r], f[r][c]);
             if (ORDER > 0) {
-                F2 r[3];
+                F2 rh[3];
 #pragma unroll
                 for (int c = 0; c < 3; c++) {
-                    const F2 vn = A(c, 0, 0, 0);
-                    if (ORDER == 1) r[c] = f[c] + inv_tau * vn;
-                    else if (ORDER == 2) r[c] = (F2(2.f) * f[c] - hp[c]) + inv_tau * (F2(2.f) * vn - F2(0.5f) * vp[c]);
-                    else
-                        r[c] = ((F2(3.f) * f[c] - F2(3.f) * hp[c]) + hq[c]) +
-                               inv_tau * ((F2(3.f) * vn - F2(1.5f) * vp[c]) + F2(0.33333333333333333333f) * vq[c]);
-                    st2(a.rhs.c[c] + id, r[c]);
+                    const F2 vn = A[r](c, 0, 0, 0);
+                    if (ORDER == 1) rh[c] = f[r][c] + inv_tau * vn;
+                    else if (ORDER == 2)
+                        rh[c] = (F2(2.f) * f[r][c] - hp[r][c]) + inv_tau * (F2(2.f) * vn - F2(0.5f) * vp[r][c]);
+                    else  // (3 f - 3 f_p + f_q) + (3 v - 3/2 v_p + 1/3 v_q) / tau as FMA chains
+                        rh[c] = fma2(F2(3.f), f[r][c], fma2(F2(-3.f), hp[r][c], hq[r][c])) +
+                                fma2(it3, vn, fma2(itm15, vp[r][c], it13 * vq[r][c]));
+                    st2(a.rhs.c[c] + id[r], rh[c]);
                 }
                 const double dz = (double)a.m.DZ[z];
-                ub += (double)r[0].v.x * dz;
-                ub += (double)r[0].v.y * dz;
+                ub += (double)rh[0].v.x * dz;
+                ub += (double)rh[0].v.y * dz;
             }
         }
         __syncthreads();
@@ -193,17 +360,19 @@ __global__ void __launch_bounds__(PTX* PTY, 2) k_flux_pair(FluxArgs<float> a, in
     }
 }
 
+constexpr int PAIR_RY = 2;  // rows per thread of the launched variant (measured faster than 1)
+
 template <int SCHEME, int ORDER>
 static void run_pair(const FluxArgs<float>& a, cudaStream_t s) {
     constexpr int H = SCHEME == TC_SCHEME_VV4 ? 3 : 1;
     constexpr size_t smem = sizeof(float) * (2 * H + 2) * 3 * RingX2<H>::PL;
-    auto kern = k_flux_pair<SCHEME, ORDER>;
+    auto kern = k_flux_pair<SCHEME, ORDER, PAIR_RY>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    const int tiles = ((a.g.NX + PCX - 1) / PCX) * ((a.g.NY + PTY - 1) / PTY);
+    const int tiles = ((a.g.NX + PCX - 1) / PCX) * ((a.g.NY + PTR - 1) / PTR);
     const int nch = std::max(1, (148 * 8 + tiles - 1) / tiles);
     const int tz = std::max(4, (a.g.NZ + nch - 1) / nch);
-    const dim3 grid((a.g.NX + PCX - 1) / PCX, (a.g.NY + PTY - 1) / PTY, (a.g.NZ + tz - 1) / tz);
-    kern<<<grid, PTX * PTY, smem, s>>>(a, tz);
+    const dim3 grid((a.g.NX + PCX - 1) / PCX, (a.g.NY + PTR - 1) / PTR, (a.g.NZ + tz - 1) / tz);
+    kern<<<grid, PTX * PTR / PAIR_RY, smem, s>>>(a, tz);
 }
 
 template <int SCHEME>

@@ -172,8 +172,10 @@ template <typename T> void launch_t2d(const T* src, double* dst, long long n, cu
 
 // learned LES closure (k_les.cu, k_mlp.cu)
 template <typename T>
-void launch_les_filter(const T* u, const T* v, const T* w, const T* p, const Geom& g, int fw, float* F, cudaStream_t s);
-void launch_les_features(const float* F, const Geom& g, int fw, const double* ZZ, float* X, float* Y, cudaStream_t s);
+void launch_les_filter(const T* u, const T* v, const T* w, const T* p, const double* ZZ, const Geom& g, int fw, int fz,
+                       float* F, cudaStream_t s);
+void launch_les_features(const float* F, const Geom& g, int fw, int fz, const double* ZZ, float* X, float* Y,
+                         cudaStream_t s);
 template <typename T> void launch_turb_mlp(const TurbArgs<T>& a, const float* P, cudaStream_t s);
 void launch_mlp_grad(const float* P, const float* X, const float* Y, long long n, float* part, float* grad,
                      cudaStream_t s);

@@ -85,7 +85,9 @@ __device__ __forceinline__ void ldb(const __nv_bfloat16 (*M)[LD], int kk, int nt
     b1 = *reinterpret_cast<const unsigned*>(row + 8);
 }
 
-__device__ __forceinline__ float sigm(float z) { return 1.f / (1.f + expf(-z)); }
+// sigmoid with the fast exponential and division intrinsics (a few float ulps, far
+// below the BF16 rounding that follows every activation)
+__device__ __forceinline__ float sigm(float z) { return __fdividef(1.f, 1.f + __expf(-z)); }
 __device__ __forceinline__ float silu(float z) { return z * sigm(z); }
 __device__ __forceinline__ float dsilu(float z) {
     const float s = sigm(z);

@@ -197,6 +197,7 @@ struct tc_handle {
     void* zfac = nullptr;  // time-independent factors of the z-matrices (k_zfactor)
     void* zfac_low = nullptr;  // double factors of the low modes
     void* mesh_t = nullptr;     // mesh arrays in T
+    void* fk = nullptr;         // float flux kernel plane constants (mixed precision)
     double* mesh_d = nullptr;   // mesh arrays in double
     double* tabs = nullptr;     // cos/sin tables
     void* tw = nullptr;         // twiddles (x then y), T complex
@@ -266,6 +267,7 @@ static MeshDev<T> mesh_dev(const tc_handle* h) {
     MeshDev<T> m;
     m.ZZ = t + 0 * L; m.DZ = t + 1 * L; m.DZW = t + 2 * L; m.GC1 = t + 3 * L; m.GC2 = t + 4 * L;
     m.GCZ = t + 5 * L; m.KERG = t + 6 * L; m.cellh = t + 7 * L; m.MAT_A = t + 8 * L; m.PC = t + 11 * L;
+    m.FK = (const float*)h->fk;
     m.dZZ = d + 0 * L; m.dDZ = d + 1 * L; m.dDZW = d + 2 * L; m.dKERG = d + 6 * L; m.dcellh = d + 7 * L;
     m.dMAT_A = d + 8 * L;
     for (int i = 0; i < 6; i++) m.MAT_D[i] = h->hm.MAT_D[i];
@@ -289,7 +291,7 @@ template <typename T>
 static const cplx<T>* twy(const tc_handle* h) { return (const cplx<T>*)h->tw + h->g.NX; }
 
 static void free_all(tc_handle* h) {
-    void* ptrs[] = {h->nu_t, h->ptmp, h->spec, h->zfac, h->zfac_low, h->mesh_t, h->mesh_d, h->tabs, h->tw, h->red, h->ticket,
+    void* ptrs[] = {h->nu_t, h->ptmp, h->spec, h->zfac, h->zfac_low, h->mesh_t, h->fk, h->mesh_d, h->tabs, h->tw, h->red, h->ticket,
                     h->err_flag, h->planes, h->diag_part, h->stage, h->opv, h->opf, h->ops, h->mlp_params, h->les_buf, h->fdiag_part};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -344,6 +346,43 @@ static void fill_plane_consts(const Geom& g, const HostMesh& hm, const T* t, T* 
         c[4] = T(-1) / (32 * (DZ[z] - C9 * DZW[z]) * hx * hy);
         c[5] = -T(1. / 32.) * ihx * ihy * GCZ[z];
         c[6] = c[7] = T(0);
+    }
+}
+
+// Constants of the float flux kernel's interior planes (k_flux_pair), from the double
+// mesh, each written twice: per plane z, with miv and w5 the VV4 momentum and w scales
+// of PC[4], PC[5] and C27 = 1/27,
+//   [0..5]   miv dz hy, -miv C27 dzw hy, miv dz hx, -miv C27 dzw hx, miv hx hy, -miv C27 hx hy
+//   [6..9]   w5 hy, -w5 C27 hy, w5 hx hy, -w5 C27 hx hy
+//   [10..13] -9 DZ[z], -9 DZ[z-1], DZ[z-2], DZ[z+1]; [14..17] the same of DZW
+//   [18..21] visc (2/(DZ[z]+DZ[z+1])) / DZ[z], visc (2/(DZ[z]+DZ[z-1])) / DZ[z],
+//            visc (2/(DZ[z]+DZ[z-1])) / DZ[z], visc (2/(DZ[z]+DZ[z-1])) / DZ[z-1]
+//   [22..23] visc / hx^2, visc / hy^2
+// (0 where an index leaves the mesh; those planes use the generic stencils).
+static void fill_flux_pair_consts(const Geom& g, const HostMesh& hm, std::vector<float>& fk) {
+    const int NZ = g.NZ;
+    fk.assign((size_t)TC_FK * NZ, 0.f);
+    const double hx = g.hx, hy = g.hy, nu = g.visc, C27 = 1.0 / 27.0;
+    const std::vector<double>&DZ = hm.DZ, &DZW = hm.DZW, &GCZ = hm.GCZ;
+    for (int z = 0; z < NZ; z++) {
+        double k[24] = {0};
+        const double miv = -1.0 / (32.0 * (DZ[z] - DZW[z] / 9.0) * hx * hy);
+        const double w5 = -(1.0 / 32.0) * GCZ[z] / (hx * hy);
+        k[0] = miv * DZ[z] * hy; k[1] = -miv * C27 * DZW[z] * hy;
+        k[2] = miv * DZ[z] * hx; k[3] = -miv * C27 * DZW[z] * hx;
+        k[4] = miv * hx * hy; k[5] = -miv * C27 * hx * hy;
+        k[6] = w5 * hy; k[7] = -w5 * C27 * hy; k[8] = w5 * hx * hy; k[9] = -w5 * C27 * hx * hy;
+        if (z >= 2 && z + 1 < NZ) {
+            k[10] = -9.0 * DZ[z]; k[11] = -9.0 * DZ[z - 1]; k[12] = DZ[z - 2]; k[13] = DZ[z + 1];
+            k[14] = -9.0 * DZW[z]; k[15] = -9.0 * DZW[z - 1]; k[16] = DZW[z - 2]; k[17] = DZW[z + 1];
+        }
+        if (z >= 1 && z + 1 < NZ) {
+            const double up = 2.0 / (DZ[z] + DZ[z + 1]), dn = 2.0 / (DZ[z] + DZ[z - 1]);
+            k[18] = nu * up / DZ[z]; k[19] = nu * dn / DZ[z];
+            k[20] = nu * dn / DZ[z]; k[21] = nu * dn / DZ[z - 1];
+        }
+        k[22] = nu / (hx * hx); k[23] = nu / (hy * hy);
+        for (int i = 0; i < 24; i++) fk[(size_t)TC_FK * z + 2 * i] = fk[(size_t)TC_FK * z + 2 * i + 1] = (float)k[i];
     }
 }
 
@@ -446,6 +485,12 @@ extern "C" int tc_create(const tc_params* prm, const double* zz, tc_handle** out
             for (size_t i = 0; i < mlen; i++) mf[i] = (float)md[i];
             fill_plane_consts<float>(g, hm, mf.data(), mf.data() + pc0);
             cudaMemcpy(h->mesh_t, mf.data(), mlen * sizeof(float), cudaMemcpyHostToDevice);
+            if (p.scheme != TC_SCHEME_COLLOC) {
+                std::vector<float> fk;
+                fill_flux_pair_consts(g, hm, fk);
+                TC_ALLOC(h->fk, fk.size() * sizeof(float));
+                cudaMemcpy(h->fk, fk.data(), fk.size() * sizeof(float), cudaMemcpyHostToDevice);
+            }
         }
     }
     // mode tables (staggered/func_global.h:208-211 cos tables; VV4 sin(pi k / N))
@@ -1253,47 +1298,49 @@ static int les_scratch(tc_handle* h, size_t bytes) {
     return TC_OK;
 }
 
-static int les_check(tc_handle* h, int level, int width, const char* who) {
+static int les_check(tc_handle* h, int level, int width, int width_z, const char* who) {
     if (!h || level < 0 || level > 3) return fail(TC_E_ARG, std::string(who) + ": bad handle or level");
     if (h->g.scheme == TC_SCHEME_COLLOC) return fail(TC_E_ARG, std::string(who) + ": staggered schemes only");
     if (width < 1 || h->g.NX % width || h->g.NY % width)
         return fail(TC_E_ARG, std::string(who) + ": the filter width must divide NX and NY");
+    if (width_z < 1 || h->g.NZ % width_z)
+        return fail(TC_E_ARG, std::string(who) + ": the wall-normal filter width must divide NZ");
     return TC_OK;
 }
 
 template <typename T>
-static void les_filter_run(tc_handle* h, int level, int width, float* F) {
+static void les_filter_run(tc_handle* h, int level, int width, int width_z, float* F) {
     const size_t N = (size_t)h->g.N;
     const T* v = (const T*)h->vel[level];
-    launch_les_filter<T>(v, v + N, v + 2 * N, (const T*)h->pres[level], h->g, width, F, h->st);
+    launch_les_filter<T>(v, v + N, v + 2 * N, (const T*)h->pres[level], h->mesh_d, h->g, width, width_z, F, h->st);
 }
 
-extern "C" int tc_les_filter(tc_handle* h, int level, int width, float* fields) {
-    int rc = les_check(h, level, width, "tc_les_filter");
+extern "C" int tc_les_filter(tc_handle* h, int level, int width, int width_z, float* fields) {
+    int rc = les_check(h, level, width, width_z, "tc_les_filter");
     if (rc) return rc;
     if (!fields) return fail(TC_E_ARG, "tc_les_filter: null output");
     cudaSetDevice(h->prm.device);
-    const size_t M = (size_t)(h->g.NX / width) * (h->g.NY / width) * h->g.NZ;
+    const size_t M = (size_t)(h->g.NX / width) * (h->g.NY / width) * (h->g.NZ / width_z);
     if ((rc = les_scratch(h, 10 * M * sizeof(float)))) return rc;
-    TC_DISPATCH(h, les_filter_run, h, level, width, h->les_buf);
+    TC_DISPATCH(h, les_filter_run, h, level, width, width_z, h->les_buf);
     if ((rc = check_launch("tc_les_filter"))) return rc;
     TC_CUDA(cudaMemcpyAsync(fields, h->les_buf, 10 * M * sizeof(float), cudaMemcpyDeviceToHost, h->st));
     TC_CUDA(cudaStreamSynchronize(h->st));
     return TC_OK;
 }
 
-extern "C" int tc_les_samples(tc_handle* h, int level, int width, float* features, float* targets) {
-    int rc = les_check(h, level, width, "tc_les_samples");
+extern "C" int tc_les_samples(tc_handle* h, int level, int width, int width_z, float* features, float* targets) {
+    int rc = les_check(h, level, width, width_z, "tc_les_samples");
     if (rc) return rc;
     if (!features || !targets) return fail(TC_E_ARG, "tc_les_samples: null output");
     cudaSetDevice(h->prm.device);
-    const size_t M = (size_t)(h->g.NX / width) * (h->g.NY / width) * h->g.NZ;
+    const size_t M = (size_t)(h->g.NX / width) * (h->g.NY / width) * (h->g.NZ / width_z);
     if ((rc = les_scratch(h, 17 * M * sizeof(float)))) return rc;
     float* F = h->les_buf;
     float* X = F + 10 * M;
     float* Y = X + 6 * M;
-    TC_DISPATCH(h, les_filter_run, h, level, width, F);
-    launch_les_features(F, h->g, width, h->mesh_d, X, Y, h->st);
+    TC_DISPATCH(h, les_filter_run, h, level, width, width_z, F);
+    launch_les_features(F, h->g, width, width_z, h->mesh_d, X, Y, h->st);
     if ((rc = check_launch("tc_les_samples"))) return rc;
     TC_CUDA(cudaMemcpyAsync(features, X, 6 * M * sizeof(float), cudaMemcpyDeviceToHost, h->st));
     TC_CUDA(cudaMemcpyAsync(targets, Y, M * sizeof(float), cudaMemcpyDeviceToHost, h->st));

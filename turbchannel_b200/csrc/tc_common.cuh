@@ -28,9 +28,14 @@ struct Geom {
 // (DZ[-1] = 0), [2] 2/(DZ[z]+DZ[z+1]) (DZ[NZ] = 0), [3] 1/DZ[z-1] (0 at z = 0),
 // [4] VV4 convective scale -1/(32 (DZ-DZW/9) hx hy), [5] VV4 w scale -GCZ/(32 hx hy).
 constexpr int TC_PC = 8;
+// FK (mixed precision only): per plane the 24 constants of the float flux kernel's
+// interior-plane stencils, each stored twice (a float2 for the packed arithmetic):
+// TC_FK floats per plane, layout in k_flux_pair.cu.
+constexpr int TC_FK = 48;
 template <typename T>
 struct MeshDev {
     const T *ZZ, *DZ, *DZW, *GC1, *GC2, *GCZ, *KERG, *MAT_A, *cellh, *PC;
+    const float* FK = nullptr;
     const double *dZZ, *dDZ, *dDZW, *dKERG, *dMAT_A, *dcellh;
     double MAT_D[6];
     double KERG_norm2;

@@ -2,21 +2,23 @@
 LES with the learned closure, the Smagorinsky-van Driest fallback and no model, each
 compared with the filtered-DNS mean velocity profile.
 
-    python -m turbchannel_b200.les_experiment [--dns-steps 20000 --stat-steps 5000 ...] --out res.json
+    python -m turbchannel_b200.les_experiment [--coarsen 4x4 8x4 --dns-steps 50000 ...] --out res.json
 
 1. DNS: staggered VV4, 384x256x384 cells (x, wall-normal, span), Re_b 21900, 2pi x 2 x pi,
-   tanh 2.2, dt 0.0008, constant flow rate, mixed precision, from the seeded field plus
+   tanh 2.2, dt 0.0006, constant flow rate, mixed precision, from the seeded field plus
    large-scale vortices as a transition trigger (--vortex; the seeded noise alone decays
    and the flow stays laminar); spin-up,
    then statistics: the mean u profile every `--stat-every` steps and, every
-   `--snap-every` steps, the box-filtered snapshot (width 4 in x and span) as closure
-   training samples (features, targets nu*/nu, tc_les_samples).
-2. Training of the MLP closure (tc_mlp_*, BF16 tensor cores, Adam) on the shuffled samples.
-3. LES: staggered HW2 + NAIVE viscosity, 96x64x96 cells on the same domain (its faces are
-   every 4th DNS face in every direction), started from the DNS's last field restricted by
-   face averages (flux-conserving on the nested grids), run with each closure; mean u
-   profile over the statistics window against the filtered DNS profile restricted to the
-   LES cells.  Reported: relative L2 and max errors, bulk-normalised.
+   `--snap-every` steps, for each LES grid of `--coarsen` (R x RZ: every R-th DNS face in x
+   and span, every RZ-th wall-normal), the snapshot box-filtered over the LES cells as
+   closure training samples (features, targets nu*/nu, tc_les_samples).
+2. Per LES grid, training of the MLP closure (tc_mlp_*, BF16 tensor cores, Adam) on the
+   shuffled samples.
+3. LES: staggered HW2 + NAIVE viscosity on that grid (4x4: 96x64x96 cells), started from
+   the DNS's last field restricted by face averages (flux-conserving on the nested grids),
+   run with each closure; mean u profile over the statistics window against the filtered
+   DNS profile restricted to the LES cells.  Reported: relative L2 and max errors,
+   bulk-normalised, and the profiles.
 """
 from __future__ import annotations
 
@@ -31,21 +33,21 @@ import turbchannel_b200 as tb
 LX, LY, RE_B, GAMMA = 2 * np.pi, np.pi, 21900.0, 2.2
 
 
-def restrict_to_les(vel, NX, NY, NZ, r, dz_fine):
+def restrict_to_les(vel, NX, NY, NZ, r, rz, dz_fine):
     """Face-average restriction of a staggered DNS field (N, 3) to the grid r times coarser
-    in x, y and z (nested faces); dz_fine: the DNS cell heights."""
+    in x and y and rz times in z (nested faces); dz_fine: the DNS cell heights."""
     u = vel[:, 0].reshape(NZ, NY, NX)
     v = vel[:, 1].reshape(NZ, NY, NX)
     w = vel[:, 2].reshape(NZ, NY, NX)
-    nz, ny, nx = NZ // r, NY // r, NX // r
-    wz = dz_fine.reshape(nz, r)
+    nz, ny, nx = NZ // rz, NY // r, NX // r
+    wz = dz_fine.reshape(nz, rz)
     wz = wz / wz.sum(axis=1, keepdims=True)
-    # u on coarse x-face X = fine face r X, averaged over the coarse face (r fine y, r fine z cells)
-    uf = u[:, :, ::r].reshape(nz, r, ny, r, nx)
+    # u on coarse x-face X = fine face r X, averaged over the coarse face (r fine y, rz fine z cells)
+    uf = u[:, :, ::r].reshape(nz, rz, ny, r, nx)
     uc = np.einsum("zkyjx,zk->zyx", uf, wz) / r
-    vf = v[:, ::r, :].reshape(nz, r, ny, nx, r)
+    vf = v[:, ::r, :].reshape(nz, rz, ny, nx, r)
     vc = np.einsum("zkyxi,zk->zyx", vf, wz) / r
-    wf = w[::r, :, :].reshape(nz, ny, r, nx, r)
+    wf = w[::rz, :, :].reshape(nz, ny, r, nx, r)
     wc = wf.mean(axis=(2, 4))
     out = np.zeros((nx * ny * nz, 3))
     out[:, 0], out[:, 1], out[:, 2] = uc.reshape(-1), vc.reshape(-1), wc.reshape(-1)
@@ -92,7 +94,7 @@ def run_dns(args, log):
     S.set_forcing(1, 1.0)
     tau, cur = args.dt, 0
     prof, nprof = np.zeros(args.nz), 0
-    Xs, Ys = [], []
+    samples = {cz: ([], []) for cz in args.coarsen}
     rng = np.random.default_rng(1)
     t0 = time.time()
     total = args.dns_steps + args.stat_steps
@@ -105,22 +107,23 @@ def run_dns(args, log):
                 prof += S.CalcProfiles(cur)[:, 0]
                 nprof += 1
             if k % args.snap_every == 0:
-                X, Y = S.les_samples(cur, 4)
-                sel = rng.random(len(Y)) < args.sample_frac
-                Xs.append(X[sel])
-                Ys.append(Y[sel])
+                for (r, rz), (Xs, Ys) in samples.items():
+                    X, Y = S.les_samples(cur, r, rz)
+                    sel = rng.random(len(Y)) < args.sample_frac * r * r * rz / 64
+                    Xs.append(X[sel])
+                    Ys.append(Y[sel])
         if (it + 1) % 1000 == 0:
             ub = S.CalcIntegral(cur)[0] / p["area"]
             log(f"DNS step {it + 1}/{total}  Ub {ub:.5f}  dp/dx {S.last_dpdx():.5f}  {time.time() - t0:.0f} s")
     S.sync()
     vel, _ = S.download_level(cur)
     S.close()
-    return dict(params=p, zz=zz, prof=prof / max(nprof, 1), X=np.concatenate(Xs), Y=np.concatenate(Ys), vel=vel,
-                wall_s=time.time() - t0)
+    return dict(params=p, zz=zz, prof=prof / max(nprof, 1), vel=vel, wall_s=time.time() - t0,
+                samples={cz: (np.concatenate(Xs), np.concatenate(Ys)) for cz, (Xs, Ys) in samples.items()})
 
 
-def run_les(args, model, params, vel0, log):
-    p, zz = tb.channel_params(tb.HW2, args.nx // 4, args.ny // 4, args.nz // 4, LX, LY, RE_B, GAMMA,
+def run_les(args, model, params, vel0, r, rz, log):
+    p, zz = tb.channel_params(tb.HW2, args.nx // r, args.ny // r, args.nz // rz, LX, LY, RE_B, GAMMA,
                               precision=tb.FP64, visc_type=tb.VISC_NAIVE, turb=tb.TURB_SMAGORINSKY)
     S = tb.Solver(p, zz)
     if model == "mlp":
@@ -164,7 +167,8 @@ def run_les(args, model, params, vel0, log):
     ub = S.CalcIntegral(cur)[0] / p["area"]
     ok = bool(np.all(np.isfinite(prof)))
     S.close()
-    log(f"LES {model}: Ub {ub:.5f}, {ms:.4f} ms/step (with the per-sample profile calls)")
+    log(f"LES {args.nx // r}x{args.nz // rz}x{args.ny // r} {model}: Ub {ub:.5f}, {ms:.4f} ms/step "
+        f"(with the per-sample profile calls)")
     return dict(prof=prof / max(wsum, 1e-300), ms_per_step=ms, ub=ub, finite=ok, zz=zz, final_tau=tau)
 
 
@@ -173,12 +177,14 @@ def main():
     ap.add_argument("--nx", type=int, default=384)
     ap.add_argument("--ny", type=int, default=384)
     ap.add_argument("--nz", type=int, default=256)
-    ap.add_argument("--dt", type=float, default=0.0008)
+    ap.add_argument("--dt", type=float, default=0.0006,
+                    help="DNS time step; during transition the CFL number at 0.0008 reaches 0.8-1.0, the edge of "
+                         "the explicit SBDF3 convection's stability")
     ap.add_argument("--vortex", type=float, default=0.5,
                     help="maximum amplitude (units of the bulk velocity) of large-scale vortices added to the "
                          "seeded field as a transition trigger; the seeded noise alone decays without transition")
-    ap.add_argument("--dns-steps", type=int, default=40000)
-    ap.add_argument("--stat-steps", type=int, default=5000)
+    ap.add_argument("--dns-steps", type=int, default=50000)
+    ap.add_argument("--stat-steps", type=int, default=25000)
     ap.add_argument("--stat-every", type=int, default=10)
     ap.add_argument("--snap-every", type=int, default=500)
     ap.add_argument("--sample-frac", type=float, default=0.2)
@@ -189,7 +195,9 @@ def main():
     ap.add_argument("--cfl-min", type=float, default=0.1)
     ap.add_argument("--cfl-max", type=float, default=0.4)
     ap.add_argument("--les-steps", type=int, default=10000)
-    ap.add_argument("--les-stat-steps", type=int, default=10000)
+    ap.add_argument("--les-stat-steps", type=int, default=20000)
+    ap.add_argument("--coarsen", type=lambda t: tuple(int(v) for v in t.split("x")), nargs="+", default=[(4, 4)],
+                    help="LES grids as coarsening factors RxRZ (x and span R, wall-normal RZ), e.g. 4x4 8x4")
     ap.add_argument("--out", default="les_experiment.json")
     args = ap.parse_args()
     t_start = time.time()
@@ -198,37 +206,40 @@ def main():
         print(f"[{time.time() - t_start:7.1f} s] {msg}", flush=True)
 
     dns = run_dns(args, log)
-    X, Y = dns["X"], dns["Y"]
-    log(f"samples: {len(Y)}  target mean {Y.mean():.4g}  max {Y.max():.4g}")
-    perm = np.random.default_rng(2).permutation(len(Y))
-    X, Y = X[perm], Y[perm]
-    nval = max(1, len(Y) // 10)
-    m = tb.Mlp(seed=12345)
-    m.set_data(X[nval:], Y[nval:])
-    losses = m.train(args.epochs, args.batch, args.lr)
-    pred = m.forward(X[:nval])
-    params = m.params
-    m.close()
-    val_mse = float(np.mean((pred - Y[:nval]) ** 2))
-    zero_mse = float(np.mean(Y[:nval] ** 2))
-    log(f"training: loss {losses[0]:.4g} -> {losses[-1]:.4g}; held-out MSE {val_mse:.4g} (nu_t = 0: {zero_mse:.4g})")
-
     dz = np.diff(dns["zz"])
-    vel0 = restrict_to_les(dns["vel"], args.nx, args.ny, args.nz, 4, dz)
-    # filtered-DNS mean u profile on the LES cells (dz-weighted average of 4 DNS cells)
-    wz = dz.reshape(-1, 4)
-    ref = (dns["prof"].reshape(-1, 4) * wz).sum(axis=1) / wz.sum(axis=1)
-    res = {"dns": {"grid": [args.nx, args.nz, args.ny], "steps": args.dns_steps + args.stat_steps, "wall_s": dns["wall_s"]},
-           "training": {"samples": int(len(Y)), "epochs": args.epochs, "loss_first": float(losses[0]),
-                        "loss_last": float(losses[-1]), "heldout_mse": val_mse, "heldout_mse_no_model": zero_mse},
-           "les": {}}
-    for model in ("mlp", "smagorinsky", "none"):
-        r = run_les(args, model, params, vel0, log)
-        err = r["prof"] - ref
-        res["les"][model] = {"rel_l2_err_mean_u": float(np.linalg.norm(err) / np.linalg.norm(ref)),
-                             "max_err_mean_u": float(np.max(np.abs(err))), "ms_per_step": r["ms_per_step"],
-                             "bulk_velocity": r["ub"], "finite": r["finite"]}
-        log(f"  {model}: rel L2 error of the mean u profile {res['les'][model]['rel_l2_err_mean_u']:.4f}")
+    res = {"dns": {"grid": [args.nx, args.nz, args.ny], "steps": args.dns_steps + args.stat_steps, "dt": args.dt,
+                   "wall_s": dns["wall_s"]}, "cases": []}
+    for r, rz in args.coarsen:
+        X, Y = dns["samples"][(r, rz)]
+        log(f"coarsening {r} x {rz} x {r}: samples {len(Y)}  target mean {Y.mean():.4g}  max {Y.max():.4g}")
+        perm = np.random.default_rng(2).permutation(len(Y))
+        X, Y = X[perm], Y[perm]
+        nval = max(1, len(Y) // 10)
+        m = tb.Mlp(seed=12345)
+        m.set_data(X[nval:], Y[nval:])
+        losses = m.train(args.epochs, args.batch, args.lr)
+        pred = m.forward(X[:nval])
+        params = m.params
+        m.close()
+        val_mse = float(np.mean((pred - Y[:nval]) ** 2))
+        zero_mse = float(np.mean(Y[:nval] ** 2))
+        log(f"training: loss {losses[0]:.4g} -> {losses[-1]:.4g}; held-out MSE {val_mse:.4g} (nu_t = 0: {zero_mse:.4g})")
+        vel0 = restrict_to_les(dns["vel"], args.nx, args.ny, args.nz, r, rz, dz)
+        # filtered-DNS mean u profile on the LES cells (dz-weighted average of rz DNS cells)
+        wz = dz.reshape(-1, rz)
+        ref = (dns["prof"].reshape(-1, rz) * wz).sum(axis=1) / wz.sum(axis=1)
+        case = {"les_grid": [args.nx // r, args.nz // rz, args.ny // r], "filter": [r, rz, r],
+                "training": {"samples": int(len(Y)), "epochs": args.epochs, "loss_first": float(losses[0]),
+                             "loss_last": float(losses[-1]), "heldout_mse": val_mse, "heldout_mse_no_model": zero_mse},
+                "filtered_dns_mean_u": ref.tolist(), "les": {}}
+        for model in ("mlp", "smagorinsky", "none"):
+            out = run_les(args, model, params, vel0, r, rz, log)
+            err = out["prof"] - ref
+            case["les"][model] = {"rel_l2_err_mean_u": float(np.linalg.norm(err) / np.linalg.norm(ref)),
+                                  "max_err_mean_u": float(np.max(np.abs(err))), "ms_per_step": out["ms_per_step"],
+                                  "bulk_velocity": out["ub"], "finite": out["finite"], "mean_u": out["prof"].tolist()}
+            log(f"  {model}: rel L2 error of the mean u profile {case['les'][model]['rel_l2_err_mean_u']:.4f}")
+        res["cases"].append(case)
     with open(args.out, "w") as f:
         json.dump(res, f, indent=1)
     log(f"wrote {args.out}")
