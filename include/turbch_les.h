@@ -32,8 +32,9 @@ extern "C" {
 int tc_les_filter(tc_handle* h, int level, int width, int width_z, float* fields);
 
 /* Training samples of the closure from the same filter: features[M][6] (above) and
- * targets[M] = nu* / nu, nu* = max(0, -tau^d_ij S_ij / (2 S_kl S_kl)) the least-squares
- * eddy viscosity of the sub-filter stress tau_ij = <u_i u_j> - <u_i><u_j>. */
+ * targets[M] = nu* / nu, nu* = -tau^d_ij S_ij / (2 S_kl S_kl) the least-squares eddy
+ * viscosity of the sub-filter stress tau_ij = <u_i u_j> - <u_i><u_j> (negative where the
+ * sub-filter scales return energy; 0 where S = 0). */
 int tc_les_samples(tc_handle* h, int level, int width, int width_z, float* features, float* targets);
 
 typedef struct tc_mlp tc_mlp;

@@ -110,7 +110,7 @@ def features_targets(F, NXc, NYc, NZ, dx, dy, ZZ, nu, utau):
     S = 0.5 * (G + np.swapaxes(G, 0, 1))
     num = -np.einsum("ij...,ij...->...", tau, S)
     den = 2 * np.einsum("ij...,ij...->...", S, S)
-    nus = np.where(den > 1e-300, np.maximum(0.0, num / np.where(den > 1e-300, den, 1.0)), 0.0)
+    nus = np.where(den > 1e-300, num / np.where(den > 1e-300, den, 1.0), 0.0)
     return X, (nus / nu).reshape(-1)
 
 

@@ -21,9 +21,13 @@ namespace tc {
 // ---------------------------------------------------------------------------
 // y-FFT
 // ---------------------------------------------------------------------------
+constexpr int YFFT_LINE_BUDGET = 128;  // lines x N1 per CTA
+// Lines per CTA: few (8 at N = 384: 26 KB of shared memory in float, 51 KB in double),
+// so that many CTAs share an SM and hide each other's global-memory latency (measured
+// at 384 x 384 x 256: 32 float lines per CTA 0.082 ms, 16 lines 0.074, 8 lines 0.058).
 template <typename T, int N>
 constexpr int yfft_reg_lines() {
-    const int l = (512 / FftSplit<N>::N1) / (sizeof(T) == 8 ? 2 : 1);
+    const int l = YFFT_LINE_BUDGET / FftSplit<N>::N1;
     return l < 1 ? 1 : l;
 }
 
@@ -310,14 +314,17 @@ static void ixfft_reg_launch(const IxFftArgs<T>& a, int rows, cudaStream_t s) {
 // dispatch on the transform length
 // ---------------------------------------------------------------------------
 // Rows per CTA of the x-FFT kernels: the largest of 32, 16, 8 that divides NY and
-// whose shared memory stays within 110 KB (two CTAs per SM); 0 if none.
+// whose shared memory stays within XFFT_SMEM_PREF (four CTAs per SM: measured faster
+// than two), else within 110 KB (two CTAs per SM); 0 if none.
+constexpr size_t XFFT_SMEM_PREF = 56 * 1024;
 template <typename T, int N>
 static int xfft_reg_rows(int NY, bool inverse) {
-    for (int r : {32, 16, 8}) {
-        if (NY % r) continue;
-        const size_t sm = inverse ? ixfft_reg_smem<T, N>(r) : div_xfft_reg_smem<T, N>(r);
-        if (sm <= 110 * 1024) return r;
-    }
+    for (size_t cap : {XFFT_SMEM_PREF, (size_t)110 * 1024})
+        for (int r : {32, 16, 8}) {
+            if (NY % r) continue;
+            const size_t sm = inverse ? ixfft_reg_smem<T, N>(r) : div_xfft_reg_smem<T, N>(r);
+            if (sm <= cap) return r;
+        }
     return 0;
 }
 

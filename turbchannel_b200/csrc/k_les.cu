@@ -8,7 +8,8 @@
 //                   sub-filter stresses tau_ij = <u_i u_j> - <u_i><u_j>;
 //   k_les_features  per coarse cell the closure's 6 inputs (les_features) from the
 //                   filtered gradient, and its training target nu*/nu, the
-//                   least-squares eddy viscosity -tau^d_ij S_ij / (2 S_kl S_kl) >= 0;
+//                   least-squares eddy viscosity -tau^d_ij S_ij / (2 S_kl S_kl) (of
+//                   either sign);
 //   k_turb_mlp      a run's nu_t = nu * MLP(features of the resolved field), one warp
 //                   per 32 cells: features by every lane in float, the network on the
 //                   tensor cores as two 16-row tiles (inference of mlp.cuh).
@@ -155,7 +156,10 @@ __global__ void __launch_bounds__(256) k_les_features(const float* __restrict__ 
             num -= (tau[i][j] - (i == j ? tr : 0.0)) * Sij;
             den += 2 * Sij * Sij;
         }
-    const double nus = den > 1e-300 ? fmax(0.0, num / den) : 0.0;
+    // not clipped at zero: the backscatter points (negative nu*) stay in the training data,
+    // so the network (softplus output, >= 0) learns the conditional mean; clipping them
+    // to 0 biased it upward and over-dissipated the LES near the walls
+    const double nus = den > 1e-300 ? num / den : 0.0;
     Yo[c] = (float)(nus / nu);
 }
 
