@@ -103,6 +103,24 @@ int tc_step(tc_handle* h, double t, double tau, int current_field, int bdf_order
 int tc_set_forcing(tc_handle* h, int mode, double value);
 int tc_last_dpdx(tc_handle* h, double* dpdx);
 
+/* Binary checkpoint for an exact restart (replaces the reference's single-level VTK
+ * ASCII q*.vtk / input.vtk, staggered/io.cpp:6-68, whose restart loses the BDF history):
+ * a 256-byte header (scheme, precision, grid, current field, time t, forcing state) and
+ * the four ring levels' velocity, flux and pressure in the device layout and working
+ * precision.  Load checks scheme, precision and grid against the solver; the turbulence
+ * model and its parameters are set by the caller, as at creation. */
+int tc_checkpoint_save(tc_handle* h, const char* path, int current_field, double t);
+int tc_checkpoint_load(tc_handle* h, const char* path, int* current_field, double* t);
+
+/* Time-averaged plane statistics on the device (the reference's driver averages the
+ * per-step profiles on the host, staggered/main.cpp:316-326): tc_stats_accumulate adds
+ * weight x the per-plane means of level `level` (tc_profiles' 12 quantities per plane)
+ * to a device accumulator without synchronising; tc_stats_read returns the weighted
+ * means (NZ x 12) and the total weight; tc_stats_reset clears them. */
+int tc_stats_accumulate(tc_handle* h, int level, double weight);
+int tc_stats_read(tc_handle* h, double* profiles, double* total_weight);
+int tc_stats_reset(tc_handle* h);
+
 /* Turbulence model: kind TC_TURB_*; weights only for TC_TURB_MLP (see
  * tc_mlp_* in turbch_les.h).  Requires visc_type NAIVE (staggered) or GALERKIN. */
 int tc_set_turb_model(tc_handle* h, int kind, const void* weights);

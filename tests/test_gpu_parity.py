@@ -175,3 +175,69 @@ def test_fused_diagnostics_match_separate_pass(name, precision):
         assert rel_err(i1, i0) < tol
         assert abs(c1 - c0) <= tol * abs(c0)
         assert rel_err(p1, p0) < tol
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("name", ["vv4_dns", "hw2_les", "coll_gal_stab1"])
+def test_checkpoint_restart_is_exact(name, precision, tmp_path):
+    """A run restarted from tc_checkpoint_save / tc_checkpoint_load continues bit for bit
+    like the uninterrupted run (all four ring levels and the forcing state restored)."""
+    import turbchannel_b200 as tb
+
+    prod, _, zz = make_case(precision=precision, **CASES[name])
+    tau, k0, k1 = 2e-3, 5, 4
+    A = tb.Solver(prod, zz)
+    A.init_channel(0, seed=31, amp=0.2, project=True)
+    A.set_forcing(1, 1.0)
+    for it in range(k0):
+        A.Step(it * tau, tau, it % 4, min(it + 1, 3))
+    path = str(tmp_path / "run.tchk")
+    A.save_checkpoint(path, k0 % 4, k0 * tau)
+    for it in range(k0, k0 + k1):
+        A.Step(it * tau, tau, it % 4, min(it + 1, 3))
+    B = tb.Solver(prod, zz)
+    cur, t = B.load_checkpoint(path)
+    assert cur == k0 % 4 and t == k0 * tau
+    for it in range(k0, k0 + k1):
+        B.Step(it * tau, tau, it % 4, min(it + 1, 3))
+    for lvl in range(4):
+        va, pa = A.download_level(lvl)
+        vb, pb = B.download_level(lvl)
+        assert np.array_equal(va, vb) and np.array_equal(pa, pb), lvl
+    assert A.last_dpdx() == B.last_dpdx()
+    # a checkpoint of another grid is rejected
+    other, _, zz2 = make_case(precision=precision, **dict(CASES[name], NX=CASES[name]["NX"] * 2))
+    C = tb.Solver(other, zz2)
+    with pytest.raises(tb.TcError):
+        C.load_checkpoint(path)
+    A.close()
+    B.close()
+    C.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("name", ["vv4_les", "coll_gal"])
+def test_device_time_averaged_profiles(name, precision):
+    """tc_stats_accumulate / tc_stats_read equal the weighted host average of the
+    per-step tc_profiles (summation order only), and tc_stats_reset clears them."""
+    import turbchannel_b200 as tb
+
+    prod, _, zz = make_case(precision=precision, **CASES[name])
+    S = tb.Solver(prod, zz)
+    S.init_channel(0, seed=7, amp=0.2, project=True)
+    S.set_forcing(1, 1.0)
+    tau = 2e-3
+    acc, wsum = 0.0, 0.0
+    for it in range(6):
+        S.Step(it * tau, tau, it % 4, min(it + 1, 3))
+        w = 1.0 + 0.5 * it
+        S.stats_accumulate((it + 1) % 4, w)
+        acc = acc + w * S.CalcProfiles((it + 1) % 4)
+        wsum += w
+    mean, wt = S.stats_read()
+    assert wt == wsum
+    assert rel_err(mean, acc / wsum) < 1e-13
+    S.stats_reset()
+    mean0, wt0 = S.stats_read()
+    assert wt0 == 0.0 and not mean0.any()
+    S.close()

@@ -42,7 +42,8 @@ EXPORTS = [
     "tc_diagnostics", "tc_op_explicit_term", "tc_op_apply_gradient", "tc_op_apply_divergence",
     "tc_op_unapply_gradient", "tc_op_pressure_solve", "tc_op_turb_visc", "tc_set_nu_t", "tc_get_nu_t",
     "tc_init_channel", "tc_mesh_tanh", "tc_phase_timing", "tc_phase_times", "tc_launch_count",
-    "tc_op_pressure_solve_static", "tc_set_diag_fusion",
+    "tc_op_pressure_solve_static", "tc_set_diag_fusion", "tc_checkpoint_save", "tc_checkpoint_load",
+    "tc_stats_accumulate", "tc_stats_read", "tc_stats_reset",
 ]
 # Every entry point declared in include/turbch_les.h (learned LES closure).
 EXPORTS_LES = [
@@ -82,6 +83,11 @@ def load_library(path: str = LIB_PATH):
     L.tc_step.argtypes = [vp, C.c_double, C.c_double, ip, ip]
     L.tc_set_forcing.argtypes = [vp, ip, C.c_double]
     L.tc_last_dpdx.argtypes = [vp, dp]
+    L.tc_checkpoint_save.argtypes = [vp, C.c_char_p, ip, C.c_double]
+    L.tc_checkpoint_load.argtypes = [vp, C.c_char_p, C.POINTER(ip), dp]
+    L.tc_stats_accumulate.argtypes = [vp, ip, C.c_double]
+    L.tc_stats_read.argtypes = [vp, vp, dp]
+    L.tc_stats_reset.argtypes = [vp]
     L.tc_set_turb_model.argtypes = [vp, ip, vp]
     L.tc_integral.argtypes = [vp, ip, vp]
     L.tc_kinetic_energy.argtypes = [vp, ip, dp]
@@ -202,6 +208,31 @@ class Solver:
         d = C.c_double()
         self._check(self.L.tc_last_dpdx(self.h, C.byref(d)))
         return d.value
+
+    def save_checkpoint(self, path: str, current_field: int, t: float):
+        """All four ring levels and the forcing state, for an exact restart."""
+        self._check(self.L.tc_checkpoint_save(self.h, os.fsencode(path), current_field, t))
+
+    def stats_accumulate(self, level: int, weight: float = 1.0):
+        """Adds weight x the per-plane means of `level` to the device accumulator (no sync)."""
+        self._check(self.L.tc_stats_accumulate(self.h, level, weight))
+
+    def stats_read(self):
+        """Weighted time means of the profiles (NZ, 12) and the total weight."""
+        out = np.zeros(self.NZ * 12)
+        w = C.c_double()
+        self._check(self.L.tc_stats_read(self.h, _ptr(out), C.byref(w)))
+        return out.reshape(self.NZ, 12), w.value
+
+    def stats_reset(self):
+        self._check(self.L.tc_stats_reset(self.h))
+
+    def load_checkpoint(self, path: str):
+        """Restores a checkpoint of a solver with the same scheme, precision and grid;
+        returns (current_field, t)."""
+        cf, t = C.c_int(), C.c_double()
+        self._check(self.L.tc_checkpoint_load(self.h, os.fsencode(path), C.byref(cf), C.byref(t)))
+        return cf.value, t.value
 
     def set_turb_model(self, kind: int, weights=None):
         """kind TURB_NONE / TURB_SMAGORINSKY / TURB_MLP (weights: MLP_NPAR float parameters)."""

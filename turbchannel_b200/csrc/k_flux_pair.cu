@@ -369,7 +369,9 @@ static void run_pair(const FluxArgs<float>& a, cudaStream_t s) {
     auto kern = k_flux_pair<SCHEME, ORDER, PAIR_RY>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     const int tiles = ((a.g.NX + PCX - 1) / PCX) * ((a.g.NY + PTR - 1) / PTR);
-    const int nch = std::max(1, (148 * 8 + tiles - 1) / tiles);
+    // z-chunks: about one CTA per resident slot (2 per SM; measured at 384x384x256:
+    // 0.699 ms against 0.710 ms with 8 slots per SM, shorter chunks)
+    const int nch = std::max(1, (148 * 2 + tiles - 1) / tiles);
     const int tz = std::max(4, (a.g.NZ + nch - 1) / nch);
     const dim3 grid((a.g.NX + PCX - 1) / PCX, (a.g.NY + PTR - 1) / PTR, (a.g.NZ + tz - 1) / tz);
     kern<<<grid, PTX * PTR / PAIR_RY, smem, s>>>(a, tz);

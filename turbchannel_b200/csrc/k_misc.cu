@@ -375,11 +375,14 @@ __global__ void __launch_bounds__(256) k_diag(DiagArgs<T> a, double* part, int S
     double sm[NDIAG];
 #pragma unroll
     for (int k = 0; k < NDIAG; k++) sm[k] = 0;
-    double mconv = 0, mvisc = 0, mboth = 0;
-    const double ihx = g.inv_hx, ihy = g.inv_hy;
-    const double ihz = coll ? 1.0 / (double)a.m.cellh[z] : 1.0 / (double)a.m.DZ[z];
-    const double kv = coll ? (g.visc_type == TC_VISC_GALERKIN ? 2.0 : 1.0) : (g.visc_type != TC_VISC_CROSS ? 2.0 : 1.0);
-    const double lap = ihx * ihx + ihy * ihy + ihz * ihz;
+    // per-cell arithmetic in the working type T, each 4-cell group's sums and maxima
+    // promoted to double (the plane sums stay double; FP64 work per cell / 4 in float)
+    T mconv = 0, mvisc = 0, mboth = 0;
+    const T ihx = (T)g.inv_hx, ihy = (T)g.inv_hy;
+    const T ihz = coll ? T(1) / a.m.cellh[z] : T(1) / a.m.DZ[z];
+    const T kv = coll ? (g.visc_type == TC_VISC_GALERKIN ? T(2) : T(1)) : (g.visc_type != TC_VISC_CROSS ? T(2) : T(1));
+    const T lap = ihx * ihx + ihy * ihy + ihz * ihz;
+    const T tau = (T)a.tau, visc = (T)g.visc;
     const size_t pl = (size_t)z * NXY;
     const bool wtop = !coll && z == NZ - 1;  // staggered: w above the top cell is the wall (0)
     for (size_t j = j0 + 4 * threadIdx.x; j < j1; j += 4 * blockDim.x) {
@@ -389,15 +392,18 @@ __global__ void __launch_bounds__(256) k_diag(DiagArgs<T> a, double* part, int S
         if (!coll && !wtop) WN = ld4(a.v.c[2] + id + NXY);
         if (a.p) P = ld4(a.p + id);
         if (a.nu_t) NT = ld4(a.nu_t + id);
+        T s4[NDIAG];
+#pragma unroll
+        for (int k = 0; k < NDIAG; k++) s4[k] = 0;
 #pragma unroll
         for (int q = 0; q < 4; q++) {
-            const double u = U.v[q], v = V.v[q], w = W.v[q];
-            const double wc = coll ? w : 0.5 * (w + (wtop ? 0.0 : (double)WN.v[q]));
-            sm[0] += u; sm[1] += v; sm[2] += wc;
-            sm[3] += u * u; sm[4] += v * v; sm[5] += wc * wc; sm[6] += u * v; sm[7] += u * wc; sm[8] += v * wc;
-            double nt = 0;
+            const T u = U.v[q], v = V.v[q], w = W.v[q];
+            const T wc = coll ? w : T(0.5) * (w + (wtop ? T(0) : WN.v[q]));
+            s4[0] += u; s4[1] += v; s4[2] += wc;
+            s4[3] += u * u; s4[4] += v * v; s4[5] += wc * wc; s4[6] += u * v; s4[7] += u * wc; s4[8] += v * wc;
+            T nt = 0;
             if (a.nu_t) {
-                sm[9] += (double)NT.v[q];
+                s4[9] += NT.v[q];
                 if (!coll) nt = NT.v[q];
                 else if (z != 0 && z != NZ - 1) {
                     const size_t jj = j + q;
@@ -405,18 +411,20 @@ __global__ void __launch_bounds__(256) k_diag(DiagArgs<T> a, double* part, int S
                     const int xm = ix == 0 ? NX - 1 : ix - 1, ym = iy == 0 ? g.NY - 1 : iy - 1;
                     const T* n = a.nu_t;
                     const size_t p0 = pl, p1 = p0 - NXY;
-                    nt = 0.125 * ((double)n[p0 + iy * NX + ix] + n[p0 + iy * NX + xm] + n[p0 + ym * NX + ix] + n[p0 + ym * NX + xm] +
-                                  n[p1 + iy * NX + ix] + n[p1 + iy * NX + xm] + n[p1 + ym * NX + ix] + n[p1 + ym * NX + xm]);
+                    nt = T(0.125) * (n[p0 + iy * NX + ix] + n[p0 + iy * NX + xm] + n[p0 + ym * NX + ix] + n[p0 + ym * NX + xm] +
+                                     n[p1 + iy * NX + ix] + n[p1 + iy * NX + xm] + n[p1 + ym * NX + ix] + n[p1 + ym * NX + xm]);
                 }
             }
-            const double p = a.p ? (double)P.v[q] : 0.0;
-            sm[10] += p; sm[11] += p * p; sm[12] += w; sm[13] += w * w;
-            const double cc = a.tau * (fabs(u) * ihx + fabs(v) * ihy + fabs(w) * ihz);
-            const double cv = 4 * kv * a.tau * ((double)g.visc + nt) * lap;
+            const T p = a.p ? P.v[q] : T(0);
+            s4[10] += p; s4[11] += p * p; s4[12] += w; s4[13] += w * w;
+            const T cc = tau * (fabs(u) * ihx + fabs(v) * ihy + fabs(w) * ihz);
+            const T cv = 4 * kv * tau * (visc + nt) * lap;
             mconv = fmax(mconv, cc);
             mvisc = fmax(mvisc, cv);
             mboth = fmax(mboth, cc + cv);
         }
+#pragma unroll
+        for (int k = 0; k < NDIAG; k++) sm[k] += (double)s4[k];
     }
     __shared__ double sb[NDIAG + 3][8];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -425,13 +433,11 @@ __global__ void __launch_bounds__(256) k_diag(DiagArgs<T> a, double* part, int S
         const double r = warp_sum(sm[k]);
         if (lane == 0) sb[k][wid] = r;
     }
-    mconv = warp_max(mconv);
-    mvisc = warp_max(mvisc);
-    mboth = warp_max(mboth);
+    const double m0 = warp_max((double)mconv), m1 = warp_max((double)mvisc), m2 = warp_max((double)mboth);
     if (lane == 0) {
-        sb[NDIAG][wid] = mconv;
-        sb[NDIAG + 1][wid] = mvisc;
-        sb[NDIAG + 2][wid] = mboth;
+        sb[NDIAG][wid] = m0;
+        sb[NDIAG + 1][wid] = m1;
+        sb[NDIAG + 2][wid] = m2;
     }
     __syncthreads();
     if (threadIdx.x < NDIAG + 3) {
@@ -616,6 +622,20 @@ void launch_correct_diag(const CorrArgs<T>& a, cudaStream_t s) {
     constexpr int ZN = correct_quad_planes<T>();
     const dim3 gq((a.g.NX / 4 + QX - 1) / QX, (a.g.NY + QY - 1) / QY, (a.g.NZ + ZN - 1) / ZN);
     k_correct_diag<T, SCHEME><<<gq, QX * QY, 0, s>>>(a);
+}
+
+// Time averaging on the device: acc[z][k] += w * planes[z][k] / NXY for the 12 profile
+// sums of a plane, acc[NZ*12] += w (the total weight).
+__global__ void k_stats_acc(const double* __restrict__ planes, double* __restrict__ acc, int NZ, double inv_nxy,
+                            double w) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < NZ * 12) acc[e] += w * planes[(e / 12) * TC_DIAG_STRIDE + e % 12] * inv_nxy;
+    else if (e == NZ * 12) acc[e] += w;
+}
+
+void launch_stats_acc(const double* planes, double* acc, int NZ, double inv_nxy, double w, cudaStream_t s) {
+    const int n = NZ * 12 + 1;
+    k_stats_acc<<<(n + 255) / 256, 256, 0, s>>>(planes, acc, NZ, inv_nxy, w);
 }
 
 void launch_diag_finish(const double* part, double* planes, int NZ, int S, cudaStream_t s) {

@@ -190,6 +190,7 @@ size_t zfactor_low_bytes(const Geom& g);
 int diag_chunks(const Geom& g);
 int correct_diag_chunks(const Geom& g);  // xy-CTAs per plane of the fused diagnostics
 void launch_diag_finish(const double* part, double* planes, int NZ, int S, cudaStream_t s);
+void launch_stats_acc(const double* planes, double* acc, int NZ, double inv_nxy, double w, cudaStream_t s);
 int flux_grid_blocks(const Geom& g);
 
 }  // namespace tc

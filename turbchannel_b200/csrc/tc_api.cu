@@ -206,6 +206,7 @@ struct tc_handle {
     unsigned* ticket = nullptr;
     int* err_flag = nullptr;
     double* planes = nullptr;
+    double* stats = nullptr;     // time-averaged profile sums (NZ x 12) and the total weight
     double* diag_part = nullptr;  // per-chunk partial sums of the diagnostics
     double* planes_h = nullptr;  // pinned
     double* stage = nullptr;     // AoS double staging (3N), lazily
@@ -291,7 +292,7 @@ template <typename T>
 static const cplx<T>* twy(const tc_handle* h) { return (const cplx<T>*)h->tw + h->g.NX; }
 
 static void free_all(tc_handle* h) {
-    void* ptrs[] = {h->nu_t, h->ptmp, h->spec, h->zfac, h->zfac_low, h->mesh_t, h->fk, h->mesh_d, h->tabs, h->tw, h->red, h->ticket,
+    void* ptrs[] = {h->nu_t, h->ptmp, h->spec, h->zfac, h->zfac_low, h->mesh_t, h->fk, h->stats, h->mesh_d, h->tabs, h->tw, h->red, h->ticket,
                     h->err_flag, h->planes, h->diag_part, h->stage, h->opv, h->opf, h->ops, h->mlp_params, h->les_buf, h->fdiag_part};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -530,6 +531,8 @@ extern "C" int tc_create(const tc_params* prm, const double* zz, tc_handle** out
     TC_ALLOC(h->ticket, sizeof(unsigned));
     TC_ALLOC(h->err_flag, sizeof(int));
     TC_ALLOC(h->planes, (size_t)g.NZ * TC_DIAG_STRIDE * sizeof(double));
+    TC_ALLOC(h->stats, ((size_t)g.NZ * 12 + 1) * sizeof(double));
+    cudaMemset(h->stats, 0, ((size_t)g.NZ * 12 + 1) * sizeof(double));
     TC_ALLOC(h->diag_part, (size_t)g.NZ * diag_chunks(g) * TC_DIAG_STRIDE * sizeof(double));
     if (cudaMallocHost((void**)&h->planes_h, (size_t)g.NZ * TC_DIAG_STRIDE * sizeof(double)) != cudaSuccess) {
         free_all(h); delete h;
@@ -961,6 +964,28 @@ static int diag_run(tc_handle* h, int level, double tau) {
     TC_CUDA(cudaMemcpyAsync(h->planes_h, h->planes, (size_t)h->g.NZ * TC_DIAG_STRIDE * sizeof(double),
                             cudaMemcpyDeviceToHost, h->st));
     TC_CUDA(cudaStreamSynchronize(h->st));
+    return TC_OK;
+}
+
+// The diagnostics pass into h->planes without the copy to the host (time averaging).
+template <typename T>
+static int diag_device(tc_handle* h, int level) {
+    if (h->fused_valid && level == h->fused_level) {
+        launch_diag_finish(h->fdiag_part, h->planes, h->g.NZ, correct_diag_chunks(h->g), h->st);
+        h->fused_used = true;
+    } else {
+        DiagArgs<T> a;
+        a.g = h->g;
+        a.m = mesh_dev<T>(h);
+        a.v = cvec<T>(h->vel[level], h->g.N);
+        a.p = (const T*)h->pres[level];
+        a.nu_t = (h->nu_t && h->turb_kind != TC_TURB_NONE) ? (const T*)h->nu_t : nullptr;
+        a.tau = 0.0;
+        a.planes = h->planes;
+        a.part = h->diag_part;
+        launch_diag<T>(a, h->st);
+    }
+    TC_CUDA(cudaGetLastError());
     return TC_OK;
 }
 
@@ -1539,5 +1564,157 @@ extern "C" int tc_set_diag_fusion(tc_handle* h, int mode) {
     h->diag_fuse = mode;
     h->diag_follow = false;
     h->fused_valid = false;
+    return TC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Binary checkpoint of the whole step state: the four ring levels (velocity, flux,
+// pressure, in the device layout) and the forcing state, so that a restarted run
+// continues the SBDF history exactly.  The reference writes VTK ASCII fields of one
+// level only (staggered/io.cpp:6-68), which loses the BDF history on restart.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr char TC_CKPT_MAGIC[8] = {'T', 'C', 'H', 'K', 'P', 'T', '0', '1'};
+struct CkptHeader {
+    char magic[8];
+    int32_t version, scheme, precision, NX, NY, NZ, current_field, forcing_mode;
+    double t, forcing_value, sour_dpdx, last_tau, last_bd0, last_du;
+    int64_t N;
+    char pad[256 - 8 - 8 * 4 - 6 * 8 - 8];
+};
+static_assert(sizeof(CkptHeader) == 256, "checkpoint header size");
+
+struct FileCloser {
+    FILE* f;
+    ~FileCloser() {
+        if (f) fclose(f);
+    }
+};
+
+// Moves `bytes` between a device buffer and the file through a pinned bounce buffer.
+int ckpt_stream(tc_handle* h, FILE* f, void* dev, size_t bytes, bool save, std::vector<char>& host) {
+    const size_t chunk = host.size();
+    for (size_t off = 0; off < bytes; off += chunk) {
+        const size_t n = std::min(chunk, bytes - off);
+        char* d = static_cast<char*>(dev) + off;
+        if (save) {
+            TC_CUDA(cudaMemcpyAsync(host.data(), d, n, cudaMemcpyDeviceToHost, h->st));
+            TC_CUDA(cudaStreamSynchronize(h->st));
+            if (fwrite(host.data(), 1, n, f) != n) return fail(TC_E_ARG, "tc_checkpoint_save: write failed");
+        } else {
+            if (fread(host.data(), 1, n, f) != n) return fail(TC_E_ARG, "tc_checkpoint_load: file too short");
+            TC_CUDA(cudaMemcpyAsync(d, host.data(), n, cudaMemcpyHostToDevice, h->st));
+            TC_CUDA(cudaStreamSynchronize(h->st));
+        }
+    }
+    return TC_OK;
+}
+
+int ckpt_levels(tc_handle* h, FILE* f, bool save) {
+    const size_t N = (size_t)h->g.N, E = h->esz;
+    std::vector<char> host(std::min<size_t>((size_t)64 << 20, 3 * N * E));
+    for (int l = 0; l < 4; l++) {
+        int rc;
+        if ((rc = ckpt_stream(h, f, h->vel[l], 3 * N * E, save, host))) return rc;
+        if ((rc = ckpt_stream(h, f, h->flux[l], 3 * N * E, save, host))) return rc;
+        if ((rc = ckpt_stream(h, f, h->pres[l], N * E, save, host))) return rc;
+    }
+    return TC_OK;
+}
+}  // namespace
+
+extern "C" int tc_checkpoint_save(tc_handle* h, const char* path, int current_field, double t) {
+    if (!h || !path || current_field < 0 || current_field > 3) return fail(TC_E_ARG, "tc_checkpoint_save: bad argument");
+    cudaSetDevice(h->prm.device);
+    TC_CUDA(cudaStreamSynchronize(h->st));
+    CkptHeader hd;
+    memset(&hd, 0, sizeof(hd));
+    memcpy(hd.magic, TC_CKPT_MAGIC, 8);
+    hd.version = 1;
+    hd.scheme = h->prm.scheme;
+    hd.precision = h->prm.precision;
+    hd.NX = h->g.NX;
+    hd.NY = h->g.NY;
+    hd.NZ = h->g.NZ;
+    hd.current_field = current_field;
+    hd.forcing_mode = h->forcing_mode;
+    hd.t = t;
+    hd.forcing_value = h->forcing_value;
+    hd.sour_dpdx = h->g.sour_dpdx;
+    hd.last_tau = h->last_tau;
+    hd.last_bd0 = h->last_bd0;
+    double du = 0.0;
+    TC_CUDA(cudaMemcpy(&du, h->red + 1, sizeof(double), cudaMemcpyDeviceToHost));
+    hd.last_du = du;
+    hd.N = h->g.N;
+    FileCloser fc{fopen(path, "wb")};
+    if (!fc.f) return fail(TC_E_ARG, std::string("tc_checkpoint_save: cannot open ") + path);
+    if (fwrite(&hd, sizeof(hd), 1, fc.f) != 1) return fail(TC_E_ARG, "tc_checkpoint_save: write failed");
+    int rc = ckpt_levels(h, fc.f, true);
+    if (rc) return rc;
+    if (fflush(fc.f) != 0) return fail(TC_E_ARG, "tc_checkpoint_save: write failed");
+    return TC_OK;
+}
+
+extern "C" int tc_checkpoint_load(tc_handle* h, const char* path, int* current_field, double* t) {
+    if (!h || !path) return fail(TC_E_ARG, "tc_checkpoint_load: bad argument");
+    cudaSetDevice(h->prm.device);
+    FileCloser fc{fopen(path, "rb")};
+    if (!fc.f) return fail(TC_E_ARG, std::string("tc_checkpoint_load: cannot open ") + path);
+    CkptHeader hd;
+    if (fread(&hd, sizeof(hd), 1, fc.f) != 1 || memcmp(hd.magic, TC_CKPT_MAGIC, 8) != 0 || hd.version != 1)
+        return fail(TC_E_ARG, "tc_checkpoint_load: not a checkpoint of this library");
+    if (hd.scheme != h->prm.scheme || hd.precision != h->prm.precision || hd.NX != h->g.NX || hd.NY != h->g.NY ||
+        hd.NZ != h->g.NZ || hd.N != h->g.N || hd.current_field < 0 || hd.current_field > 3)
+        return fail(TC_E_ARG, "tc_checkpoint_load: the checkpoint's scheme, precision or grid differ from the solver's");
+    TC_CUDA(cudaStreamSynchronize(h->st));
+    int rc = ckpt_levels(h, fc.f, false);
+    if (rc) return rc;
+    h->forcing_mode = hd.forcing_mode;
+    h->forcing_value = hd.forcing_value;
+    h->prm.sour_dpdx = hd.sour_dpdx;
+    h->g.sour_dpdx = hd.sour_dpdx;
+    h->last_tau = hd.last_tau;
+    h->last_bd0 = hd.last_bd0;
+    TC_CUDA(cudaMemcpy(h->red + 1, &hd.last_du, sizeof(double), cudaMemcpyHostToDevice));
+    h->fused_valid = false;
+    if (current_field) *current_field = hd.current_field;
+    if (t) *t = hd.t;
+    return TC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Time-averaged plane statistics kept on the device (the reference's driver adds the
+// profiles of each step on the host, staggered/main.cpp:316-326): per call one
+// diagnostics pass of the level and a weighted add into a device accumulator, no
+// host synchronisation; a read returns the weighted means in tc_profiles' layout.
+// ---------------------------------------------------------------------------
+extern "C" int tc_stats_accumulate(tc_handle* h, int level, double weight) {
+    if (!h || level < 0 || level > 3 || !(weight >= 0.0)) return fail(TC_E_ARG, "tc_stats_accumulate: bad argument");
+    cudaSetDevice(h->prm.device);
+    int rc = TC_DISPATCH(h, diag_device, h, level);
+    if (rc) return rc;
+    launch_stats_acc(h->planes, h->stats, h->g.NZ, 1.0 / (double)h->g.NXY, weight, h->st);
+    TC_CUDA(cudaGetLastError());
+    return TC_OK;
+}
+
+extern "C" int tc_stats_read(tc_handle* h, double* profiles, double* total_weight) {
+    if (!h || !profiles) return fail(TC_E_ARG, "tc_stats_read: bad argument");
+    cudaSetDevice(h->prm.device);
+    const size_t n = (size_t)h->g.NZ * 12;
+    std::vector<double> acc(n + 1);
+    TC_CUDA(cudaMemcpyAsync(acc.data(), h->stats, (n + 1) * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    TC_CUDA(cudaStreamSynchronize(h->st));
+    const double w = acc[n];
+    for (size_t i = 0; i < n; i++) profiles[i] = w > 0.0 ? acc[i] / w : 0.0;
+    if (total_weight) *total_weight = w;
+    return TC_OK;
+}
+
+extern "C" int tc_stats_reset(tc_handle* h) {
+    if (!h) return fail(TC_E_ARG, "tc_stats_reset: null handle");
+    cudaSetDevice(h->prm.device);
+    TC_CUDA(cudaMemsetAsync(h->stats, 0, ((size_t)h->g.NZ * 12 + 1) * sizeof(double), h->st));
     return TC_OK;
 }

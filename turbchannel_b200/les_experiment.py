@@ -24,6 +24,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import os
 import time
 
 import numpy as np
@@ -107,6 +108,9 @@ def run_dns(args, log):
                 prof += S.CalcProfiles(cur)[:, 0]
                 nprof += 1
             if k % args.snap_every == 0:
+                if args.snap_dir:  # the filtered snapshot of the first LES grid, 10 fields
+                    r0, rz0 = args.coarsen[0]
+                    np.save(os.path.join(args.snap_dir, f"snap_{k:07d}.npy"), S.les_filter(cur, r0, rz0))
                 for (r, rz), (Xs, Ys) in samples.items():
                     X, Y = S.les_samples(cur, r, rz)
                     sel = rng.random(len(Y)) < args.sample_frac * r * r * rz / 64
@@ -198,8 +202,13 @@ def main():
     ap.add_argument("--les-stat-steps", type=int, default=20000)
     ap.add_argument("--coarsen", type=lambda t: tuple(int(v) for v in t.split("x")), nargs="+", default=[(4, 4)],
                     help="LES grids as coarsening factors RxRZ (x and span R, wall-normal RZ), e.g. 4x4 8x4")
+    ap.add_argument("--snap-dir", default="",
+                    help="directory for the box-filtered snapshots (float32 .npy, fields u, v, w, p, uu, vv, ww, uv, "
+                         "uw, vw on the first LES grid of --coarsen)")
     ap.add_argument("--out", default="les_experiment.json")
     args = ap.parse_args()
+    if args.snap_dir:
+        os.makedirs(args.snap_dir, exist_ok=True)
     t_start = time.time()
 
     def log(msg):
