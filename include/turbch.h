@@ -121,6 +121,19 @@ int tc_stats_accumulate(tc_handle* h, int level, double weight);
 int tc_stats_read(tc_handle* h, double* profiles, double* total_weight);
 int tc_stats_reset(tc_handle* h);
 
+/* Device-controlled run (the reference's driver loop with its CFL control,
+ * staggered/main.cpp:308-370, without a host synchronisation per step): up to `nsteps`
+ * SBDF3 steps of time step `tau` from ring level `current_field`, replayed by a CUDA
+ * graph whose while-loop repeats `check_every` steps (a multiple of 4, so the ring comes
+ * back to `current_field`) and then computes on the device the CFL number of that level
+ * (mode as tc_cfl); the loop ends when the CFL leaves [cfl_min, cfl_max] or the steps
+ * are done.  Returns the steps done and the last CFL.  The caller has ramped the BDF
+ * order to 3 with tc_step, and reacts to the returned CFL as the reference does (new
+ * tau, order restart).  The graph is kept for the next call with the same tau,
+ * current_field, check_every and mode.  Phase timing must be off. */
+int tc_run_graph(tc_handle* h, double tau, int current_field, int nsteps, int check_every, int cfl_mode,
+                 double cfl_min, double cfl_max, int* steps_done, double* cfl);
+
 /* Turbulence model: kind TC_TURB_*; weights only for TC_TURB_MLP (see
  * tc_mlp_* in turbch_les.h).  Requires visc_type NAIVE (staggered) or GALERKIN. */
 int tc_set_turb_model(tc_handle* h, int kind, const void* weights);

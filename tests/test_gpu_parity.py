@@ -241,3 +241,62 @@ def test_device_time_averaged_profiles(name, precision):
     mean0, wt0 = S.stats_read()
     assert wt0 == 0.0 and not mean0.any()
     S.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("name", ["vv4_dns", "hw2_les", "coll_cross"])
+def test_run_graph_matches_host_steps(name, precision):
+    """tc_run_graph (order-3 steps replayed by a device-controlled CUDA graph) gives the
+    same fields, bit for bit, as the same steps launched one by one, and reports the CFL
+    number tc_cfl gives for the level it ends on; it stops after the first check when
+    the CFL is above cfl_max."""
+    import turbchannel_b200 as tb
+
+    prod, _, zz = make_case(precision=precision, **CASES[name])
+    tau, n = 2e-3, 16
+    res = []
+    for mode in ("host", "graph"):
+        S = tb.Solver(prod, zz)
+        S.init_channel(0, seed=11, amp=0.2, project=True)
+        S.set_forcing(1, 1.0)
+        for it in range(2):
+            S.Step(it * tau, tau, it % 4, it + 1)
+        cur = 2
+        if mode == "host":
+            for it in range(n):
+                S.Step((2 + it) * tau, tau, (cur + it) % 4, 3)
+            cfl = S.CalcCFL(cur, tau, 3)
+        else:
+            done, cfl = S.run_graph(tau, cur, n, 8, 3, 0.0, 1e30)
+            assert done == n
+        res.append(([S.download_level(l) for l in range(4)], cfl))
+        if mode == "graph":
+            done2, cfl2 = S.run_graph(tau, cur, 16, 4, 3, 0.0, 0.5 * cfl)
+            assert done2 == 4 and cfl2 > 0.5 * cfl
+        S.close()
+    (la, ca), (lb, cb) = res
+    for (va, pa), (vb, pb) in zip(la, lb):
+        assert np.array_equal(va, vb) and np.array_equal(pa, pb)
+    assert cb == ca
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_run_adaptive_controls_cfl(precision):
+    """run_adaptive halves tau when the CFL number exceeds its bound and the run stays
+    finite and divergence-free in flow rate (bulk velocity 1)."""
+    import turbchannel_b200 as tb
+
+    prod, _, zz = make_case(precision=precision, **CASES["vv4_dns"])
+    S = tb.Solver(prod, zz)
+    S.init_channel(0, seed=3, amp=0.2, project=True)
+    S.set_forcing(1, 1.0)
+    tau0 = 2e-2
+    S.Step(0.0, tau0, 0, 1)
+    cfl0 = S.CalcCFL(1, tau0, 3)
+    t, tau, cur = tb.run_adaptive(S, tau0, tau0, 1, 40, 0.1 * cfl0, 0.5 * cfl0, check_every=4)
+    assert tau < tau0
+    assert S.CalcCFL(cur, tau, 3) < cfl0
+    v, p = S.download_level(cur)
+    assert np.all(np.isfinite(v)) and np.all(np.isfinite(p))
+    assert abs(S.CalcIntegral(cur)[0] / prod["area"] - 1.0) < (1e-10 if precision == 0 else 1e-5)
+    S.close()

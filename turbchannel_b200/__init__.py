@@ -43,7 +43,7 @@ EXPORTS = [
     "tc_op_unapply_gradient", "tc_op_pressure_solve", "tc_op_turb_visc", "tc_set_nu_t", "tc_get_nu_t",
     "tc_init_channel", "tc_mesh_tanh", "tc_phase_timing", "tc_phase_times", "tc_launch_count",
     "tc_op_pressure_solve_static", "tc_set_diag_fusion", "tc_checkpoint_save", "tc_checkpoint_load",
-    "tc_stats_accumulate", "tc_stats_read", "tc_stats_reset",
+    "tc_stats_accumulate", "tc_stats_read", "tc_stats_reset", "tc_run_graph",
 ]
 # Every entry point declared in include/turbch_les.h (learned LES closure).
 EXPORTS_LES = [
@@ -88,6 +88,7 @@ def load_library(path: str = LIB_PATH):
     L.tc_stats_accumulate.argtypes = [vp, ip, C.c_double]
     L.tc_stats_read.argtypes = [vp, vp, dp]
     L.tc_stats_reset.argtypes = [vp]
+    L.tc_run_graph.argtypes = [vp, C.c_double, ip, ip, ip, ip, C.c_double, C.c_double, C.POINTER(ip), dp]
     L.tc_set_turb_model.argtypes = [vp, ip, vp]
     L.tc_integral.argtypes = [vp, ip, vp]
     L.tc_kinetic_energy.argtypes = [vp, ip, dp]
@@ -212,6 +213,15 @@ class Solver:
     def save_checkpoint(self, path: str, current_field: int, t: float):
         """All four ring levels and the forcing state, for an exact restart."""
         self._check(self.L.tc_checkpoint_save(self.h, os.fsencode(path), current_field, t))
+
+    def run_graph(self, tau: float, current_field: int, nsteps: int, check_every: int = 8, cfl_mode: int = 3,
+                  cfl_min: float = 0.0, cfl_max: float = float("inf")):
+        """Up to nsteps order-3 steps as one device-controlled CUDA graph (see tc_run_graph);
+        returns (steps done, CFL number of the last check)."""
+        n, c = C.c_int(), C.c_double()
+        self._check(self.L.tc_run_graph(self.h, tau, current_field, nsteps, check_every, cfl_mode, cfl_min, cfl_max,
+                                        C.byref(n), C.byref(c)))
+        return n.value, c.value
 
     def stats_accumulate(self, level: int, weight: float = 1.0):
         """Adds weight x the per-plane means of `level` to the device accumulator (no sync)."""
@@ -425,3 +435,37 @@ def channel_params(scheme: int, NX: int, NY: int, NZ: int, Lx: float, Ly: float,
              stab_type=stab_type, fd_mode=fd_mode, device=device, visc=visc, sour_dpdx=sour_dpdx,
              inv_length_scale=u_tau / visc, xmin=0.0, ymin=0.0, hx=Lx / NX, hy=Ly / NY, area=area, low_modes=0)
     return p, zz
+
+
+def run_adaptive(S: "Solver", t: float, tau: float, current_field: int, nsteps: int, cfl_min: float, cfl_max: float,
+                 check_every: int = 8, cfl_mode: int = 3):
+    """The reference driver's loop with CFL-adaptive dt (staggered/main.cpp:308-370): after
+    a change of tau the BDF order restarts at 1 (tc_step ramps it), then order-3 steps run
+    as device-controlled graphs (Solver.run_graph) that stop on the device when the CFL
+    number leaves [cfl_min, cfl_max]; the host then halves tau until the CFL estimate is
+    below cfl_max, or enlarges it by 1.5 below cfl_min, as the reference does.
+    Returns (t, tau, current_field) after nsteps steps."""
+    done, order, cur = 0, 1, current_field
+    while done < nsteps:
+        if order < 3 or nsteps - done < check_every:
+            S.Step(t, tau, cur, order)
+            t += tau
+            cur = (cur + 1) % 4
+            done += 1
+            order = min(order + 1, 3)
+            continue
+        n, cfl = S.run_graph(tau, cur, (nsteps - done) // check_every * check_every, check_every, cfl_mode,
+                             cfl_min, cfl_max)
+        done += n
+        t += n * tau  # n is a multiple of 4: the ring is back at `cur`
+        if not np.isfinite(cfl):
+            raise TcError(f"run_adaptive: non-finite CFL number after step {done}")
+        if cfl > cfl_max:
+            while cfl > cfl_max:
+                cfl *= 0.5
+                tau *= 0.5
+            order = 1
+        elif cfl < cfl_min:
+            tau *= 1.5
+            order = 1
+    return t, tau, cur

@@ -633,6 +633,41 @@ __global__ void k_stats_acc(const double* __restrict__ planes, double* __restric
     else if (e == NZ * 12) acc[e] += w;
 }
 
+// The loop condition of a device-controlled run: the CFL number (maximum over the
+// planes of the chosen estimate, slots 16..18 of the diagnostics) of the level just
+// written, then continue while bodies remain and the CFL lies in [cfl_min, cfl_max]
+// (a NaN stops the loop).  One CTA.
+__global__ void __launch_bounds__(256) k_run_ctl(cudaGraphConditionalHandle hnd, const double* __restrict__ planes,
+                                                 int NZ, int mode, RunCtl* ctl) {
+    __shared__ double sb[8];
+    double m = 0.0;
+    bool nan = false;
+    for (int z = threadIdx.x; z < NZ; z += blockDim.x) {
+        const double c = planes[(size_t)z * TC_DIAG_STRIDE + 15 + mode];
+        nan |= !(c == c);
+        m = fmax(m, c);
+    }
+    nan = __syncthreads_or(nan);
+    m = warp_max(m);
+    if ((threadIdx.x & 31) == 0) sb[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); w++) m = fmax(m, sb[w]);
+        m = fmax(m, sb[0]);
+        const double cfl = nan ? __longlong_as_double(0x7ff8000000000000LL) : m;
+        const unsigned it = ctl->iters + 1;
+        ctl->iters = it;
+        ctl->cfl = cfl;
+        const bool go = it < ctl->max_iters && cfl >= ctl->cfl_min && cfl <= ctl->cfl_max;
+        cudaGraphSetConditional(hnd, go ? 1u : 0u);
+    }
+}
+
+void launch_run_ctl(cudaGraphConditionalHandle hnd, const double* planes, int NZ, int mode, RunCtl* ctl,
+                    cudaStream_t s) {
+    k_run_ctl<<<1, 256, 0, s>>>(hnd, planes, NZ, mode, ctl);
+}
+
 void launch_stats_acc(const double* planes, double* acc, int NZ, double inv_nxy, double w, cudaStream_t s) {
     const int n = NZ * 12 + 1;
     k_stats_acc<<<(n + 255) / 256, 256, 0, s>>>(planes, acc, NZ, inv_nxy, w);

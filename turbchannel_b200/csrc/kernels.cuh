@@ -191,6 +191,15 @@ int diag_chunks(const Geom& g);
 int correct_diag_chunks(const Geom& g);  // xy-CTAs per plane of the fused diagnostics
 void launch_diag_finish(const double* part, double* planes, int NZ, int S, cudaStream_t s);
 void launch_stats_acc(const double* planes, double* acc, int NZ, double inv_nxy, double w, cudaStream_t s);
+
+// State of a device-controlled run (tc_run_graph): bodies done, their bound, the CFL
+// number of the last check and the bounds that keep the loop going.
+struct RunCtl {
+    unsigned iters, max_iters;
+    double cfl, cfl_min, cfl_max;
+};
+void launch_run_ctl(cudaGraphConditionalHandle hnd, const double* planes, int NZ, int mode, RunCtl* ctl,
+                    cudaStream_t s);
 int flux_grid_blocks(const Geom& g);
 
 }  // namespace tc

@@ -207,6 +207,12 @@ struct tc_handle {
     int* err_flag = nullptr;
     double* planes = nullptr;
     double* stats = nullptr;     // time-averaged profile sums (NZ x 12) and the total weight
+    // tc_run_graph: the instantiated loop and the parameters it was captured for
+    cudaGraph_t run_graph = nullptr;
+    cudaGraphExec_t run_exec = nullptr;
+    RunCtl* run_ctl = nullptr;
+    double run_tau = 0.0;
+    int run_cur = -1, run_every = 0, run_mode = 0;
     double* diag_part = nullptr;  // per-chunk partial sums of the diagnostics
     double* planes_h = nullptr;  // pinned
     double* stage = nullptr;     // AoS double staging (3N), lazily
@@ -571,6 +577,9 @@ extern "C" int tc_destroy(tc_handle* h) {
     if (!h) return TC_OK;
     cudaSetDevice(h->prm.device);
     cudaStreamSynchronize(h->st);
+    if (h->run_exec) cudaGraphExecDestroy(h->run_exec);
+    if (h->run_graph) cudaGraphDestroy(h->run_graph);
+    if (h->run_ctl) cudaFree(h->run_ctl);
     free_all(h);
     delete h;
     return TC_OK;
@@ -1716,5 +1725,104 @@ extern "C" int tc_stats_reset(tc_handle* h) {
     if (!h) return fail(TC_E_ARG, "tc_stats_reset: null handle");
     cudaSetDevice(h->prm.device);
     TC_CUDA(cudaMemsetAsync(h->stats, 0, ((size_t)h->g.NZ * 12 + 1) * sizeof(double), h->st));
+    return TC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Device-controlled runs: SBDF3 steps of a fixed tau replayed by a CUDA graph whose
+// while-loop ends on the device when the CFL number leaves [cfl_min, cfl_max] (the
+// reference's driver checks it on the host every 10 steps and halves or enlarges tau,
+// staggered/main.cpp:361-370).  The body is `every` steps (a multiple of 4, so that the
+// ring comes back to the same levels) followed by the diagnostics pass of the level just
+// written and the condition kernel; the host waits once per run, not per step.
+// ---------------------------------------------------------------------------
+template <typename T>
+static int run_capture_body(tc_handle* h, double tau, int cur, int every, int mode, cudaGraphConditionalHandle hnd) {
+    for (int k = 0; k < every; k++) {
+        int rc = step_impl<T>(h, tau, (cur + k) % 4, 3);
+        if (rc) return rc;
+    }
+    DiagArgs<T> a;
+    a.g = h->g;
+    a.m = mesh_dev<T>(h);
+    a.v = cvec<T>(h->vel[cur], h->g.N);
+    a.p = (const T*)h->pres[cur];
+    a.nu_t = (h->nu_t && h->turb_kind != TC_TURB_NONE) ? (const T*)h->nu_t : nullptr;
+    a.tau = tau;
+    a.planes = h->planes;
+    a.part = h->diag_part;
+    launch_diag<T>(a, h->st);
+    launch_run_ctl(hnd, h->planes, h->g.NZ, mode, h->run_ctl, h->st);
+    return check_launch("tc_run_graph");
+}
+
+static void run_graph_drop(tc_handle* h) {
+    if (h->run_exec) cudaGraphExecDestroy(h->run_exec);
+    if (h->run_graph) cudaGraphDestroy(h->run_graph);
+    h->run_exec = nullptr;
+    h->run_graph = nullptr;
+    h->run_cur = -1;
+}
+
+static int run_graph_build(tc_handle* h, double tau, int cur, int every, int mode) {
+    run_graph_drop(h);
+    TC_CUDA(cudaGraphCreate(&h->run_graph, 0));
+    cudaGraphConditionalHandle hnd;
+    TC_CUDA(cudaGraphConditionalHandleCreate(&hnd, h->run_graph, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = hnd;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    TC_CUDA(cudaGraphAddNode(&node, h->run_graph, nullptr, 0, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    TC_CUDA(cudaStreamBeginCaptureToGraph(h->st, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    const int diag_fuse = h->diag_fuse;
+    h->diag_fuse = 0;  // no lazily allocated fused-diagnostics buffer inside the capture
+    int rc = TC_DISPATCH(h, run_capture_body, h, tau, cur, every, mode, hnd);
+    h->diag_fuse = diag_fuse;
+    cudaGraph_t captured = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(h->st, &captured);
+    if (rc || ec != cudaSuccess) {
+        cudaGetLastError();
+        run_graph_drop(h);
+        return rc ? rc : fail(TC_E_CUDA, std::string("tc_run_graph: capture failed: ") + cudaGetErrorString(ec));
+    }
+    TC_CUDA(cudaGraphInstantiate(&h->run_exec, h->run_graph, 0));
+    h->run_tau = tau;
+    h->run_cur = cur;
+    h->run_every = every;
+    h->run_mode = mode;
+    return TC_OK;
+}
+
+extern "C" int tc_run_graph(tc_handle* h, double tau, int current_field, int nsteps, int check_every, int cfl_mode,
+                            double cfl_min, double cfl_max, int* steps_done, double* cfl) {
+    if (!h || current_field < 0 || current_field > 3 || cfl_mode < 1 || cfl_mode > 3)
+        return fail(TC_E_ARG, "tc_run_graph: bad argument");
+    if (!(tau > 0) || !std::isfinite(tau)) return fail(TC_E_ARG, "tc_run_graph: tau must be positive");
+    if (check_every < 4 || check_every % 4 != 0 || nsteps < check_every)
+        return fail(TC_E_ARG, "tc_run_graph: check_every must be a positive multiple of 4 and at most nsteps");
+    if (h->timing) return fail(TC_E_STATE, "tc_run_graph: phase timing is on");
+    cudaSetDevice(h->prm.device);
+    if (!h->run_ctl && cudaMalloc((void**)&h->run_ctl, sizeof(RunCtl)) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(TC_E_NOMEM, "tc_run_graph: allocation failed");
+    }
+    if (!h->run_exec || h->run_tau != tau || h->run_cur != current_field || h->run_every != check_every ||
+        h->run_mode != cfl_mode) {
+        int rc = run_graph_build(h, tau, current_field, check_every, cfl_mode);
+        if (rc) return rc;
+    }
+    RunCtl c{0u, (unsigned)(nsteps / check_every), 0.0, cfl_min, cfl_max};
+    TC_CUDA(cudaMemcpyAsync(h->run_ctl, &c, sizeof(c), cudaMemcpyHostToDevice, h->st));
+    TC_CUDA(cudaGraphLaunch(h->run_exec, h->st));
+    TC_CUDA(cudaMemcpyAsync(&c, h->run_ctl, sizeof(c), cudaMemcpyDeviceToHost, h->st));
+    TC_CUDA(cudaStreamSynchronize(h->st));
+    h->fused_valid = false;
+    h->last_out = current_field;
+    if (steps_done) *steps_done = (int)c.iters * check_every;
+    if (cfl) *cfl = c.cfl;
     return TC_OK;
 }
