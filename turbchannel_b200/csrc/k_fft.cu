@@ -1,7 +1,7 @@
 // k_fft.cu -- the pressure solve's FFT kernels for the lengths that have a compiled
 // two-pass register transform (fft_reg.cuh: 16 ... 1024 = 2^a 3^b); other lengths
 // keep the Stockham kernels of k_poisson.cu.  Same data layouts and results:
-//   k_div_quad     : divergence of the vector RHS (streaming, 16-byte row loads)
+//   k_div_quad_z   : divergence of the vector RHS (streaming, 16-byte row loads)
 //                    into a scratch real field;
 //   k_xfft_reg     : forward x-FFT of `rows` y-rows of a real field (the divergence
 //                    or the scalar RHS), two rows packed as one complex line,
@@ -73,103 +73,103 @@ static void yfft_reg_launch(const YFftArgs<T>& a, cudaStream_t s) {
 // divergence of the vector RHS (streaming, 4 cells of a row per thread) and the
 // forward x-FFT of a real field
 // ---------------------------------------------------------------------------
-// Same expressions as div_at (stencil_div.cuh), evaluated for x..x+3 from 16-byte
-// row loads; NX % 4 == 0 (the periodic wrap then moves whole 4-cell chunks).
-template <typename T, int SCHEME>
-__global__ void __launch_bounds__(256) k_div_quad(DivFftArgs<T> a, T* __restrict__ out) {
+// Same expressions as div_at (stencil_div.cuh), evaluated for x..x+3 from 16-byte row
+// loads (NX % 4 == 0: the periodic wrap then moves whole 4-cell chunks), each thread
+// marching over ZC consecutive planes of its 4-cell row: the w planes z-1 .. z+2 of the
+// stencils stay in registers from one plane to the next (one new w load per plane
+// instead of four; measured at 384x384x256, float: 0.188 ms with the x-FFT against 0.223
+// ms for one plane per thread).
+template <typename T, int SCHEME, int ZC>
+__global__ void __launch_bounds__(256) k_div_quad_z(DivFftArgs<T> a, T* __restrict__ out) {
     const Geom& g = a.g;
-    const int NX = g.NX, NY = g.NY, NZ = g.NZ, NQ = NX >> 2;
-    const int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= (int)(g.N >> 2)) return;
-    const int row = q / NQ, x = (q - row * NQ) * 4;
-    const int y = row % NY, z = row / NY;
-    const size_t NXY = (size_t)NX * NY, pl = (size_t)z * NXY, rb = pl + (size_t)y * NX, id = rb + x;
+    const int NX = g.NX, NY = g.NY, NZ = g.NZ, NQ = NX >> 2, NZB = (NZ + ZC - 1) / ZC;
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= (long long)NQ * NY * NZB) return;
+    const int row = (int)(q / NQ), x = (int)(q - (long long)row * NQ) * 4;
+    const int y = row % NY, z0 = (row / NY) * ZC;
+    const size_t NXY = (size_t)NX * NY, col = (size_t)y * NX + x;
     const T *u = a.v.c[0], *v = a.v.c[1], *w = a.v.c[2];
     const T ihx = (T)g.inv_hx, ihy = (T)g.inv_hy;
     const int xq = x + 4 == NX ? 0 : x + 4, xm = x == 0 ? NX - 1 : x - 1;
     const int yp = y + 1 == NY ? 0 : y + 1, ym = y == 0 ? NY - 1 : y - 1;
-    T e[9];  // u at x-1 .. x+7
-    {
-        const Acc4<T> U0 = ld4(u + id), U1 = ld4(u + rb + xq);
-        e[0] = __ldg(u + rb + xm);
+    const int ypp = yp + 1 == NY ? 0 : yp + 1;
+    auto ldw = [&](int zz) {
+        Acc4<T> r;
+        if (zz >= 0 && zz < NZ) r = ld4(w + (size_t)zz * NXY + col);
+        else
 #pragma unroll
-        for (int k = 0; k < 4; k++) {
-            e[1 + k] = U0.v[k];
-            e[5 + k] = U1.v[k];
+            for (int k = 0; k < 4; k++) r.v[k] = T(0);
+        return r;
+    };
+    Acc4<T> Wz[4];  // w at the planes z-1, z, z+1, z+2
+    Wz[0] = ldw(z0 - 1);
+    Wz[1] = ldw(z0);
+    Wz[2] = ldw(z0 + 1);
+    Wz[3] = ldw(z0 + 2);
+#pragma unroll
+    for (int kz = 0; kz < ZC; kz++) {
+        const int z = z0 + kz;
+        if (z >= NZ) break;
+        if (kz > 0) {
+            Wz[0] = Wz[1];
+            Wz[1] = Wz[2];
+            Wz[2] = Wz[3];
+            Wz[3] = ldw(z + 2);
         }
-    }
-    T d[4];
-    if constexpr (SCHEME == TC_SCHEME_VV4) {
-        const T C27 = T(0.03703703703703703703);
-        const int ypp = yp + 1 == NY ? 0 : yp + 1;
-        const T dz = a.m.DZ[z], dzw = a.m.DZW[z];
-        const Acc4<T> V0 = ld4(v + id), Vp = ld4(v + pl + (size_t)yp * NX + x), Vpp = ld4(v + pl + (size_t)ypp * NX + x),
-                      Vm = ld4(v + pl + (size_t)ym * NX + x);
-        const Acc4<T> W0 = ld4(w + id);
-        Acc4<T> Wr, Wrr, Wll;
-        if (z == NZ - 1) {
+        const size_t pl = (size_t)z * NXY, rb = pl + (size_t)y * NX, id = rb + x;
+        T e[9];  // u at x-1 .. x+7
+        {
+            const Acc4<T> U0 = ld4(u + id), U1 = ld4(u + rb + xq);
+            e[0] = __ldg(u + rb + xm);
 #pragma unroll
-            for (int k = 0; k < 4; k++) Wr.v[k] = T(0);
-            Wrr = W0;
-        } else {
-            Wr = ld4(w + id + NXY);
-            if (z == NZ - 2) {
-#pragma unroll
-                for (int k = 0; k < 4; k++) Wrr.v[k] = T(0);
-            } else {
-                Wrr = ld4(w + id + 2 * NXY);
+            for (int k = 0; k < 4; k++) {
+                e[1 + k] = U0.v[k];
+                e[5 + k] = U1.v[k];
             }
         }
-        if (z == 0) Wll = ld4(w + id + NXY);
-        else if (z == 1) {
+        T d[4];
+        if constexpr (SCHEME == TC_SCHEME_VV4) {
+            const T C27 = T(0.03703703703703703703);
+            const T dz = a.m.DZ[z], dzw = a.m.DZW[z];
+            const Acc4<T> V0 = ld4(v + id), Vp = ld4(v + pl + (size_t)yp * NX + x),
+                          Vpp = ld4(v + pl + (size_t)ypp * NX + x), Vm = ld4(v + pl + (size_t)ym * NX + x);
 #pragma unroll
-            for (int k = 0; k < 4; k++) Wll.v[k] = T(0);
+            for (int k = 0; k < 4; k++) {
+                const T W0 = Wz[1].v[k];
+                const T Wr = z == NZ - 1 ? T(0) : Wz[2].v[k];
+                const T Wrr = z == NZ - 1 ? W0 : (z == NZ - 2 ? T(0) : Wz[3].v[k]);
+                const T Wll = z == 0 ? Wz[2].v[k] : (z == 1 ? T(0) : Wz[0].v[k]);
+                const T dudx = ihx * (dz * (e[k + 2] - e[k + 1]) - C27 * dzw * (e[k + 3] - e[k]));
+                const T dvdy = ihy * (dz * (Vp.v[k] - V0.v[k]) - C27 * dzw * (Vpp.v[k] - Vm.v[k]));
+                d[k] = dudx + dvdy + (Wr - W0) - C27 * (Wrr - Wll);
+            }
+        } else if constexpr (SCHEME == TC_SCHEME_HW2) {
+            const T hz = a.m.DZ[z];
+            const Acc4<T> V0 = ld4(v + id), Vp = ld4(v + pl + (size_t)yp * NX + x);
+#pragma unroll
+            for (int k = 0; k < 4; k++)
+                d[k] = (e[k + 2] - e[k + 1]) * ihx * hz + (Vp.v[k] - V0.v[k]) * ihy * hz +
+                       ((z < NZ - 1) ? (Wz[2].v[k] - Wz[1].v[k]) : (-Wz[1].v[k]));
         } else {
-            Wll = ld4(w + id - NXY);
-        }
+            const T hz = a.m.cellh[z], hx = (T)g.hx, hy = (T)g.hy;
+            const Acc4<T> Vp = ld4(v + pl + (size_t)yp * NX + x), Vm = ld4(v + pl + (size_t)ym * NX + x);
 #pragma unroll
-        for (int k = 0; k < 4; k++) {
-            const T dudx = ihx * (dz * (e[k + 2] - e[k + 1]) - C27 * dzw * (e[k + 3] - e[k]));
-            const T dvdy = ihy * (dz * (Vp.v[k] - V0.v[k]) - C27 * dzw * (Vpp.v[k] - Vm.v[k]));
-            d[k] = dudx + dvdy + (Wr.v[k] - W0.v[k]) - C27 * (Wrr.v[k] - Wll.v[k]);
+            for (int k = 0; k < 4; k++) {
+                const T Wa = z == 0 ? Wz[2].v[k] : (z == NZ - 1 ? Wz[1].v[k] : Wz[2].v[k]);
+                const T Wb = z == 0 ? Wz[1].v[k] : Wz[0].v[k];
+                T dd = 0;
+                dd += T(0.5) * (e[k + 2] - e[k]) * hy * hz;
+                dd += T(0.5) * (Vp.v[k] - Vm.v[k]) * hx * hz;
+                dd += T(0.5) * (Wa - Wb) * hx * hy;
+                d[k] = dd;
+            }
         }
-    } else if constexpr (SCHEME == TC_SCHEME_HW2) {
-        const T hz = a.m.DZ[z];
-        const Acc4<T> V0 = ld4(v + id), Vp = ld4(v + pl + (size_t)yp * NX + x), W0 = ld4(w + id);
-        Acc4<T> Wr;
-        if (z < NZ - 1) Wr = ld4(w + id + NXY);
-#pragma unroll
-        for (int k = 0; k < 4; k++)
-            d[k] = (e[k + 2] - e[k + 1]) * ihx * hz + (Vp.v[k] - V0.v[k]) * ihy * hz +
-                   ((z < NZ - 1) ? (Wr.v[k] - W0.v[k]) : (-W0.v[k]));
-    } else {
-        const T hz = a.m.cellh[z], hx = (T)g.hx, hy = (T)g.hy;
-        const Acc4<T> Vp = ld4(v + pl + (size_t)yp * NX + x), Vm = ld4(v + pl + (size_t)ym * NX + x);
-        Acc4<T> Wa, Wb;  // the two w planes of the z-difference
-        if (z == 0) {
-            Wa = ld4(w + id + NXY);
-            Wb = ld4(w + id);
-        } else if (z == NZ - 1) {
-            Wa = ld4(w + id);
-            Wb = ld4(w + id - NXY);
+        if constexpr (sizeof(T) == 4) {
+            *reinterpret_cast<float4*>(out + id) = make_float4(d[0], d[1], d[2], d[3]);
         } else {
-            Wa = ld4(w + id + NXY);
-            Wb = ld4(w + id - NXY);
+            reinterpret_cast<double2*>(out + id)[0] = make_double2(d[0], d[1]);
+            reinterpret_cast<double2*>(out + id)[1] = make_double2(d[2], d[3]);
         }
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-            T dd = 0;
-            dd += T(0.5) * (e[k + 2] - e[k]) * hy * hz;
-            dd += T(0.5) * (Vp.v[k] - Vm.v[k]) * hx * hz;
-            dd += T(0.5) * (Wa.v[k] - Wb.v[k]) * hx * hy;
-            d[k] = dd;
-        }
-    }
-    if constexpr (sizeof(T) == 4) {
-        *reinterpret_cast<float4*>(out + id) = make_float4(d[0], d[1], d[2], d[3]);
-    } else {
-        reinterpret_cast<double2*>(out + id)[0] = make_double2(d[0], d[1]);
-        reinterpret_cast<double2*>(out + id)[1] = make_double2(d[2], d[3]);
     }
 }
 
@@ -227,12 +227,14 @@ static void xfft_reg_launch(const DivFftArgs<T>& a, const T* src, int rows, cuda
     k<<<dim3(a.g.NY / rows, a.g.NZ), 256, smem, s>>>(a, src, rows, lr);
 }
 
+constexpr int DIV_ZC = 4;  // planes per thread of k_div_quad_z
 template <typename T>
 static void div_quad_launch(const DivFftArgs<T>& a, T* out, cudaStream_t s) {
-    const unsigned nb = (unsigned)(((a.g.N >> 2) + 255) / 256);
-    if (a.g.scheme == TC_SCHEME_VV4) k_div_quad<T, TC_SCHEME_VV4><<<nb, 256, 0, s>>>(a, out);
-    else if (a.g.scheme == TC_SCHEME_HW2) k_div_quad<T, TC_SCHEME_HW2><<<nb, 256, 0, s>>>(a, out);
-    else k_div_quad<T, TC_SCHEME_COLLOC><<<nb, 256, 0, s>>>(a, out);
+    const long long nq = (long long)(a.g.NX / 4) * a.g.NY * ((a.g.NZ + DIV_ZC - 1) / DIV_ZC);
+    const unsigned nb = (unsigned)((nq + 255) / 256);
+    if (a.g.scheme == TC_SCHEME_VV4) k_div_quad_z<T, TC_SCHEME_VV4, DIV_ZC><<<nb, 256, 0, s>>>(a, out);
+    else if (a.g.scheme == TC_SCHEME_HW2) k_div_quad_z<T, TC_SCHEME_HW2, DIV_ZC><<<nb, 256, 0, s>>>(a, out);
+    else k_div_quad_z<T, TC_SCHEME_COLLOC, DIV_ZC><<<nb, 256, 0, s>>>(a, out);
 }
 
 // ---------------------------------------------------------------------------
@@ -343,7 +345,7 @@ bool launch_yfft_reg(const YFftArgs<T>& a, cudaStream_t s) {
     }
 }
 
-// The vector RHS first goes through k_div_quad into a.dtmp (needs NX % 4 == 0 and a
+// The vector RHS first goes through k_div_quad_z into a.dtmp (needs NX % 4 == 0 and a
 // scratch buffer), then the real field is transformed.
 template <typename T>
 int launch_div_xfft_reg(const DivFftArgs<T>& a, cudaStream_t s) {

@@ -202,6 +202,9 @@ def main():
     ap.add_argument("--les-stat-steps", type=int, default=20000)
     ap.add_argument("--coarsen", type=lambda t: tuple(int(v) for v in t.split("x")), nargs="+", default=[(4, 4)],
                     help="LES grids as coarsening factors RxRZ (x and span R, wall-normal RZ), e.g. 4x4 8x4")
+    ap.add_argument("--dissipation-weighted", action="store_true",
+                    help="train on samples drawn with probability proportional to (S:S)^2 (the squared "
+                         "sub-filter dissipation error per unit viscosity error)")
     ap.add_argument("--snap-dir", default="",
                     help="directory for the box-filtered snapshots (float32 .npy, fields u, v, w, p, uu, vv, ww, uv, "
                          "uw, vw on the first LES grid of --coarsen)")
@@ -225,7 +228,15 @@ def main():
         X, Y = X[perm], Y[perm]
         nval = max(1, len(Y) // 10)
         m = tb.Mlp(seed=12345)
-        m.set_data(X[nval:], Y[nval:])
+        Xt, Yt = X[nval:], Y[nval:]
+        if args.dissipation_weighted:
+            # weighted least squares by resampling: the sub-filter dissipation error of a
+            # prediction is 2 (nu - nu*) S:S, so each sample counts with (S:S)^2, S:S =
+            # sinh of the first feature (wall units)
+            wgt = np.sinh(Xt[:, 0].astype(np.float64)) ** 2
+            idx = np.random.default_rng(3).choice(len(Yt), size=len(Yt), p=wgt / wgt.sum())
+            Xt, Yt = Xt[idx], Yt[idx]
+        m.set_data(Xt, Yt)
         losses = m.train(args.epochs, args.batch, args.lr)
         pred = m.forward(X[:nval])
         params = m.params
