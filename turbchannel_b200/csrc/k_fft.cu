@@ -173,6 +173,13 @@ __global__ void __launch_bounds__(256) k_div_quad_z(DivFftArgs<T> a, T* __restri
     }
 }
 
+// Whether the forward x-FFT of `rows` rows (256 threads) keeps its transformed lines in
+// the first pass's buffer: one second-pass line segment per thread at most.
+template <int N>
+__host__ __device__ constexpr bool xfft_alias(int rows) {
+    return (rows / 2) * FftSplit<N>::N1 <= 256;
+}
+
 template <typename T, int N>
 __global__ void __launch_bounds__(256, 2) k_xfft_reg(DivFftArgs<T> a, const T* __restrict__ src, int rows, int lrows) {
     constexpr int N1 = FftSplit<N>::N1, N2 = FftSplit<N>::N2, YL = FftSplit<N>::YL, ZS = N + 1;
@@ -180,7 +187,10 @@ __global__ void __launch_bounds__(256, 2) k_xfft_reg(DivFftArgs<T> a, const T* _
     const Geom& g = a.g;
     const int NY = g.NY, NXH = N / 2 + 1, nl = rows >> 1;
     cplx<T>* Y = reinterpret_cast<cplx<T>*>(smraw);
-    cplx<T>* Zs = Y + nl * YL;  // transformed lines, stride N+1
+    // transformed lines, stride N+1: over Y itself when every thread holds at most one
+    // line segment of the second pass (read all, barrier, write), else after Y
+    const bool alias = xfft_alias<N>(rows);
+    cplx<T>* Zs = alias ? Y : Y + nl * YL;
     const int z = blockIdx.y, y0 = blockIdx.x * rows;
     const T* plane = src + ((size_t)z * NY + y0) * N;
     for (int it = threadIdx.x; it < nl * N2; it += blockDim.x) {
@@ -192,13 +202,26 @@ __global__ void __launch_bounds__(256, 2) k_xfft_reg(DivFftArgs<T> a, const T* _
         fft_pass_a<T, N, -1>(v, n2, a.twx, Y + l * YL);
     }
     __syncthreads();
-    for (int it = threadIdx.x; it < nl * N1; it += blockDim.x) {
-        const int l = it / N1, k1 = it - l * N1;
+    if (alias) {
+        const bool mine = (int)threadIdx.x < nl * N1;
+        const int l = threadIdx.x / N1, k1 = threadIdx.x - l * N1;
         cplx<T> v[N2];
-        fft_pass_b<T, N, -1>(v, k1, Y + l * YL);
-        cplx<T>* zl = Zs + l * ZS + k1;
+        if (mine) fft_pass_b<T, N, -1>(v, k1, Y + l * YL);
+        __syncthreads();
+        if (mine) {
+            cplx<T>* zl = Zs + l * ZS + k1;
 #pragma unroll
-        for (int k2 = 0; k2 < N2; k2++) zl[k2 * N1] = v[k2];
+            for (int k2 = 0; k2 < N2; k2++) zl[k2 * N1] = v[k2];
+        }
+    } else {
+        for (int it = threadIdx.x; it < nl * N1; it += blockDim.x) {
+            const int l = it / N1, k1 = it - l * N1;
+            cplx<T> v[N2];
+            fft_pass_b<T, N, -1>(v, k1, Y + l * YL);
+            cplx<T>* zl = Zs + l * ZS + k1;
+#pragma unroll
+            for (int k2 = 0; k2 < N2; k2++) zl[k2 * N1] = v[k2];
+        }
     }
     __syncthreads();
     // unpack the two real rows of each line: X_a = (Z_k + conj Z_{N-k}) / 2, X_b = (Z_k - conj Z_{N-k}) / 2i
@@ -214,7 +237,7 @@ __global__ void __launch_bounds__(256, 2) k_xfft_reg(DivFftArgs<T> a, const T* _
 
 template <typename T, int N>
 static size_t div_xfft_reg_smem(int rows) {
-    return (size_t)(rows / 2) * (FftSplit<N>::YL + N + 1) * sizeof(cplx<T>);
+    return (size_t)(rows / 2) * (FftSplit<N>::YL + (xfft_alias<N>(rows) ? 0 : N + 1)) * sizeof(cplx<T>);
 }
 
 template <typename T, int N>
