@@ -258,23 +258,34 @@ def cpu_baseline(small=False, budget_s=20.0, max_steps=3):
                       f"FP64, {op.get_threads()} OpenMP threads, {dt:.1f} s"}
 
 
+def aggregate_value(world: int, cells: int, steps: int, ms_max: float) -> float:
+    """Whole-job cell-steps/s of `world` replicas, each of `cells` cells and `steps` steps,
+    timed by the slowest rank (ms_max, the maximum over ranks)."""
+    return world * cells * steps / (ms_max * 1e-3)
+
+
 class Dist:
-    def __init__(self):
+    """The ranks of a multi-GPU run (one process per GPU, replicas of the workload): a
+    barrier before and after the timed region and the maximum over ranks of each time.
+    backend "nccl" on the GPUs; "gloo" (CPU tensors) serves the CPU tests of this logic."""
+
+    def __init__(self, backend: str = "nccl"):
         import datetime
 
         import torch
         import torch.distributed as dist
 
         self.dist = dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
         self.rank, self.world = dist.get_rank(), dist.get_world_size()
         self.torch = torch
+        self.device = "cuda" if backend == "nccl" else "cpu"
 
     def barrier(self):
         self.dist.barrier()
 
     def max(self, x: float) -> float:
-        t = self.torch.tensor([x], dtype=self.torch.float64, device="cuda")
+        t = self.torch.tensor([x], dtype=self.torch.float64, device=self.device)
         self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
         return float(t.item())
 
@@ -354,7 +365,7 @@ def main():
     launches = mixed["launches"]
     clocks = mixed["clocks"]
     N = mixed["params"]["NX"] * mixed["params"]["NY"] * mixed["params"]["NZ"]
-    value = world * N * args.steps / (mixed["ms"] * 1e-3)
+    value = aggregate_value(world, N, args.steps, mixed["ms"])
     ub_mixed = mixed["ub"]
     mixed["solver"].close()
     del mixed["solver"]
