@@ -375,8 +375,9 @@ __global__ void __launch_bounds__(256) k_diag(DiagArgs<T> a, double* part, int S
     double sm[NDIAG];
 #pragma unroll
     for (int k = 0; k < NDIAG; k++) sm[k] = 0;
-    // per-cell arithmetic in the working type T, each 4-cell group's sums and maxima
-    // promoted to double (the plane sums stay double; FP64 work per cell / 4 in float)
+    // per-cell arithmetic and this thread's sums over its chunk (8 groups of 4 cells at
+    // most) in the working type T, promoted to double once; the plane sums across threads
+    // stay double
     T mconv = 0, mvisc = 0, mboth = 0;
     const T ihx = (T)g.inv_hx, ihy = (T)g.inv_hy;
     const T ihz = coll ? T(1) / a.m.cellh[z] : T(1) / a.m.DZ[z];
@@ -385,6 +386,9 @@ __global__ void __launch_bounds__(256) k_diag(DiagArgs<T> a, double* part, int S
     const T tau = (T)a.tau, visc = (T)g.visc;
     const size_t pl = (size_t)z * NXY;
     const bool wtop = !coll && z == NZ - 1;  // staggered: w above the top cell is the wall (0)
+    T s4[NDIAG];
+#pragma unroll
+    for (int k = 0; k < NDIAG; k++) s4[k] = 0;
     for (size_t j = j0 + 4 * threadIdx.x; j < j1; j += 4 * blockDim.x) {
         const size_t id = pl + j;
         const Acc4<T> U = ld4(a.v.c[0] + id), V = ld4(a.v.c[1] + id), W = ld4(a.v.c[2] + id);
@@ -392,9 +396,6 @@ __global__ void __launch_bounds__(256) k_diag(DiagArgs<T> a, double* part, int S
         if (!coll && !wtop) WN = ld4(a.v.c[2] + id + NXY);
         if (a.p) P = ld4(a.p + id);
         if (a.nu_t) NT = ld4(a.nu_t + id);
-        T s4[NDIAG];
-#pragma unroll
-        for (int k = 0; k < NDIAG; k++) s4[k] = 0;
 #pragma unroll
         for (int q = 0; q < 4; q++) {
             const T u = U.v[q], v = V.v[q], w = W.v[q];
@@ -423,9 +424,9 @@ __global__ void __launch_bounds__(256) k_diag(DiagArgs<T> a, double* part, int S
             mvisc = fmax(mvisc, cv);
             mboth = fmax(mboth, cc + cv);
         }
-#pragma unroll
-        for (int k = 0; k < NDIAG; k++) sm[k] += (double)s4[k];
     }
+#pragma unroll
+    for (int k = 0; k < NDIAG; k++) sm[k] = (double)s4[k];
     __shared__ double sb[NDIAG + 3][8];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
@@ -465,7 +466,9 @@ int diag_chunks(const Geom& g) {
     const long long nxy = (long long)g.NX * g.NY;
     int S = (int)std::min<long long>(64, std::max<long long>(1, nxy / 2048));
     while (S > 1 && (long long)S * g.NZ > 148 * 32) S--;
-    return S;
+    // at most 8 groups of 4 cells per thread (256 threads): k_diag's per-thread sums in
+    // the working type stay short
+    return (int)std::max<long long>(S, (nxy + 8191) / 8192);
 }
 
 // ---------------------------------------------------------------------------
