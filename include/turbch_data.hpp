@@ -81,6 +81,28 @@ class Data {
         return d;
     }
 
+    // restart, time averaging and device-controlled runs (no counterpart in the reference's object)
+    void SaveCheckpoint(const std::string& path, int current_field, double t) {
+        check(tc_checkpoint_save(h_, path.c_str(), current_field, t));
+    }
+    void LoadCheckpoint(const std::string& path, int& current_field, double& t) {
+        check(tc_checkpoint_load(h_, path.c_str(), &current_field, &t));
+    }
+    void StatsAccumulate(int level, double weight = 1.0) { check(tc_stats_accumulate(h_, level, weight)); }
+    double StatsRead(double* profiles) {
+        double w;
+        check(tc_stats_read(h_, profiles, &w));
+        return w;
+    }
+    void StatsReset() { check(tc_stats_reset(h_)); }
+    // steps done; cfl receives the CFL number of the last device-side check
+    int RunGraph(double tau, int current_field, int nsteps, int check_every, int cfl_mode, double cfl_min,
+                 double cfl_max, double& cfl) {
+        int done;
+        check(tc_run_graph(h_, tau, current_field, nsteps, check_every, cfl_mode, cfl_min, cfl_max, &done, &cfl));
+        return done;
+    }
+
    private:
     tc_params prm_;
     tc_handle* h_ = nullptr;
