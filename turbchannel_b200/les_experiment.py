@@ -89,9 +89,9 @@ def add_vortices(S, p, zz, amp, seed=7):
 def run_dns(args, log):
     p, zz = tb.channel_params(tb.VV4, args.nx, args.ny, args.nz, LX, LY, RE_B, GAMMA, precision=tb.MIXED)
     S = tb.Solver(p, zz)
-    S.init_channel(0, seed=12345, amp=0.1, project=True)
+    S.init_channel(0, seed=args.seed, amp=0.1, project=True)
     if args.vortex > 0:
-        add_vortices(S, p, zz, args.vortex)
+        add_vortices(S, p, zz, args.vortex, seed=7 + args.seed - 12345)
     S.set_forcing(1, 1.0)
     tau, cur = args.dt, 0
     prof, nprof = np.zeros(args.nz), 0
@@ -187,6 +187,8 @@ def main():
     ap.add_argument("--vortex", type=float, default=0.5,
                     help="maximum amplitude (units of the bulk velocity) of large-scale vortices added to the "
                          "seeded field as a transition trigger; the seeded noise alone decays without transition")
+    ap.add_argument("--seed", type=int, default=12345,
+                    help="seed of the DNS initial noise (the vortex trigger uses seed - 12338)")
     ap.add_argument("--dns-steps", type=int, default=50000)
     ap.add_argument("--stat-steps", type=int, default=25000)
     ap.add_argument("--stat-every", type=int, default=10)
