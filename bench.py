@@ -44,9 +44,10 @@ PHASE_WORDS = {"turb": 2, "flux": 21, "div_xfft": 4, "yfft": 2, "zsolve": 2, "iy
 STEP_WORDS = 40
 FALLBACK_HBM_GBS = 6650.0
 # DRAM bytes per cell of one launch (dram__bytes_read.sum + dram__bytes_write.sum) from
-# the ncu capture summarised in profiles/flux_vv4_192x128x192.md (4.7 M cells, inputs
-# larger than L2); traffic grows with the cell count, so it is scaled to the grid.
-TRAFFIC_BYTES_PER_CELL = {("flux", 4): (284.9e6 + 90.76e6) / 4718592, ("flux", 8): (591.3e6 + 208.6e6) / 4718592}
+# the ncu captures summarised in profiles/flux_pair_vv4_192x192x128.md (float kernel) and
+# profiles/flux_vv4_192x128x192.md (double kernel), 4.7 M cells, inputs larger than L2;
+# traffic grows with the cell count, so it is scaled to the grid.
+TRAFFIC_BYTES_PER_CELL = {("flux", 4): (286.44e6 + 90.22e6) / 4718592, ("flux", 8): (591.3e6 + 208.6e6) / 4718592}
 
 
 def peaks():
