@@ -12,7 +12,11 @@
  * symmetric and antisymmetric parts times nu/u_tau^2, u_tau = inv_length_scale * visc)
  * and log(1 + y+)/4.  Parameters are a packed float vector of TC_MLP_NPAR values:
  * W1[6][64], b1[64], W2[64][64], b2[64], w3[64], b3 (W[in][out]).
- * Staggered schemes only.  Every call returns TC_OK or a TC_E_* code (tc_last_error).
+ * Samples (tc_les_filter, tc_les_samples): staggered schemes.  A run with TC_TURB_MLP:
+ * staggered (nu_t per cell) and collocated (nu_t per element between 8 nodes, from the
+ * element gradient; the inputs are the same physical invariants, so one network serves
+ * both at the filter width it was trained for).  Every call returns TC_OK or a TC_E_*
+ * code (tc_last_error).
  */
 #ifndef TURBCH_LES_H
 #define TURBCH_LES_H

@@ -114,6 +114,27 @@ def features_targets(F, NXc, NYc, NZ, dx, dy, ZZ, nu, utau):
     return X, (nus / nu).reshape(-1)
 
 
+def element_features(vel, NX, NY, NZ, hx, hy, ZZ, nu, utau):
+    """k_turb_mlp's collocated inputs: per element between the 8 nodes (ix..ix+1, iy..iy+1,
+    iz..iz+1), iz < NZ-1, the element gradient of the nodal velocity (vel: (N, 3) at the
+    nodes, ZZ the NZ node heights) and the wall distance of the element centre ->
+    ((NZ-1) NY NX, 6) features, elements in node-index order."""
+    ZZ = np.asarray(ZZ, dtype=np.float64)
+    q = vel.reshape(NZ, NY, NX, 3).transpose(3, 0, 1, 2)
+    xp = lambda a: np.roll(a, -1, axis=-1)
+    yp = lambda a: np.roll(a, -1, axis=-2)
+    lo, hi = q[:, :-1], q[:, 1:]
+    c = [lo, xp(lo), yp(lo), xp(yp(lo)), hi, xp(hi), yp(hi), xp(yp(hi))]  # 000 100 010 110 001 101 011 111
+    hz = np.diff(ZZ)[:, None, None]
+    G = np.zeros((3, 3) + lo.shape[1:])
+    G[:, 0] = ((c[1] + c[3] + c[5] + c[7]) - (c[0] + c[2] + c[4] + c[6])) / (4 * hx)
+    G[:, 1] = ((c[2] + c[3] + c[6] + c[7]) - (c[0] + c[1] + c[4] + c[5])) / (4 * hy)
+    G[:, 2] = ((c[4] + c[5] + c[6] + c[7]) - (c[0] + c[1] + c[2] + c[3])) / (4 * hz)
+    zc = 0.5 * (ZZ[:-1] + ZZ[1:])
+    d = np.minimum(zc - ZZ[0], ZZ[-1] - zc)[:, None, None]
+    return features_from_gradient(G, nu, utau, d).reshape(-1, 6)
+
+
 def smagorinsky_nut(X, hx, hy, dz_local, utau, nu, cs=0.1):
     """The reference's Smagorinsky-van Driest model (staggered/func_global.h:875-890, as in
     k_turb_stag's smag_nut) as nu_t/nu from the features: |S| = sqrt(2 S:S) from tr(S^2),

@@ -174,3 +174,36 @@ def test_run_with_learned_closure_matches_oracle_nu_t():
     v2, p2 = S.download_level(10 % 4)
     assert np.all(np.isfinite(v2)) and np.all(np.isfinite(p2))
     S.close()
+
+
+def test_collocated_run_with_learned_closure_matches_oracle_nu_t():
+    """The closure on the collocated scheme: nu_t on the elements from the element
+    gradient of the nodal velocity, against the oracle's features and network; the top
+    node plane (no element) keeps nu_t = 0; a short run stays finite."""
+    import turbchannel_b200 as tb
+    from cases import COLLOC
+
+    NX, NY, NZ = 32, 16, 25
+    prod, _, zz = make_case(scheme=COLLOC, NX=NX, NY=NY, NZ=NZ, precision=0, turb=1)
+    S = tb.Solver(prod, zz)
+    m = tb.Mlp(seed=23)
+    P = m.params
+    m.close()
+    S.set_turb_model(tb.TURB_MLP, P)
+    S.init_channel(0, seed=5, amp=0.2, project=True)
+    v, _ = S.download_level(0)
+    nt = S.RecalcTurbVisc(v)
+    utau = prod["inv_length_scale"] * prod["visc"]
+    X = lo.element_features(v, NX, NY, NZ, prod["hx"], prod["hy"], np.asarray(zz), prod["visc"], utau)
+    want = prod["visc"] * lo.mlp_forward(P, X.astype(np.float32))
+    ne = NX * NY * (NZ - 1)
+    assert np.all(np.isfinite(nt)) and np.all(nt[:ne] >= 0)
+    assert np.linalg.norm(nt[:ne] - want) / np.linalg.norm(want) < 1e-2
+    assert not nt[ne:].any()
+    tau = 1e-3
+    S.set_forcing(1, 1.0)
+    for it in range(10):
+        S.Step(it * tau, tau, it % 4, min(it + 1, 3))
+    v2, p2 = S.download_level(10 % 4)
+    assert np.all(np.isfinite(v2)) and np.all(np.isfinite(p2))
+    S.close()

@@ -11,8 +11,9 @@
 //                   least-squares eddy viscosity -tau^d_ij S_ij / (2 S_kl S_kl) (of
 //                   either sign);
 //   k_turb_mlp      a run's nu_t = nu * MLP(features of the resolved field), one warp
-//                   per 32 cells: features by every lane in float, the network on the
-//                   tensor cores as two 16-row tiles (inference of mlp.cuh).
+//                   per 32 cells (staggered) or elements (collocated): features by
+//                   every lane in float, the network on the tensor cores as two 16-row
+//                   tiles (inference of mlp.cuh).
 // Cell-centred velocities: u_c = (u_x + u_{x+1})/2 etc. (u on the lower x-face,
 // v on the lower y-face, w on the lower z-face, w = 0 on the top wall).  Gradients:
 // central differences; at the walls the no-slip value 0 at the wall plane is the
@@ -201,11 +202,15 @@ __device__ __forceinline__ void les_features_f(const float G[3][3], float sc, fl
     f[5] = 0.25f * log1pf(yplus);
 }
 
-// nu_t of a staggered run from the learned closure.  P: packed FP32 parameters.
-// Each warp takes 32 cells at a time: every lane gathers its cell's centred-velocity
-// gradient (differences in T, then float) and features, then two 16-row tiles go
-// through the network on the tensor cores.
-template <typename T>
+// nu_t of a run from the learned closure.  P: packed FP32 parameters.  Each warp takes
+// 32 cells at a time: every lane gathers its cell's velocity gradient (differences in
+// T, then float) and features, then two 16-row tiles go through the network on the
+// tensor cores.  Staggered (COLL = false): the centred-velocity gradient of the cell.
+// Collocated (COLL = true): the elements between 8 nodes, where that scheme keeps nu_t
+// (iz < NZ-1, the top plane untouched as in the Smagorinsky kernel), with the element
+// gradient of the nodal velocity -- the network's inputs are invariants of the resolved
+// gradient in wall units and y+, the same physical quantities for both schemes.
+template <typename T, bool COLL>
 __global__ void __launch_bounds__(128, 4) k_turb_mlp(TurbArgs<T> a, const float* __restrict__ P) {
     __shared__ MlpSmem S;
     __shared__ float Xs[4][32][MLP_IN];
@@ -226,7 +231,33 @@ __global__ void __launch_bounds__(128, 4) k_turb_mlp(TurbArgs<T> a, const float*
     for (long long grp = (long long)blockIdx.x * 4 + wid; grp < ngrp; grp += (long long)gridDim.x * 4) {
         const long long c0 = grp * 32;
         const int nrow = (int)min(32LL, N - c0);
-        if (lane < nrow) {
+        if (COLL && lane < nrow && (c0 + lane) / (long long)NXY >= NZ - 1) {
+#pragma unroll
+            for (int k = 0; k < MLP_IN; k++) Xs[wid][lane][k] = 0.f;  // top node plane: no element
+        } else if (COLL && lane < nrow) {
+            const long long c = c0 + lane;
+            const int ix = (int)(c % NX), iy = (int)((c / NX) % NY), iz = (int)(c / NXY);
+            const int xp = ix + 1 == NX ? 0 : ix + 1, yp = iy + 1 == NY ? 0 : iy + 1;
+            const size_t p0 = (size_t)iz * NXY, p1 = p0 + NXY;
+            const size_t i00 = (size_t)iy * NX + ix, i10 = (size_t)iy * NX + xp, i01 = (size_t)yp * NX + ix,
+                         i11 = (size_t)yp * NX + xp;
+            const float ghx = (float)(0.25 * g.inv_hx), ghy = (float)(0.25 * g.inv_hy);
+            const float ghz = (float)(0.25 / (a.m.dZZ[iz + 1] - a.m.dZZ[iz]));
+            float G[3][3];
+#pragma unroll
+            for (int cc = 0; cc < 3; cc++) {
+                const T* q = a.v.c[cc];
+                const T q000 = q[p0 + i00], q100 = q[p0 + i10], q010 = q[p0 + i01], q110 = q[p0 + i11];
+                const T q001 = q[p1 + i00], q101 = q[p1 + i10], q011 = q[p1 + i01], q111 = q[p1 + i11];
+                G[cc][0] = (float)((q100 + q110 + q101 + q111) - (q000 + q010 + q001 + q011)) * ghx;
+                G[cc][1] = (float)((q010 + q110 + q011 + q111) - (q000 + q100 + q001 + q101)) * ghy;
+                G[cc][2] = (float)((q001 + q101 + q011 + q111) - (q000 + q100 + q010 + q110)) * ghz;
+            }
+            const double* ZZ = a.m.dZZ;
+            const double zc = 0.5 * (ZZ[iz] + ZZ[iz + 1]);
+            const double d = fmin(zc - ZZ[0], ZZ[NZ - 1] - zc);
+            les_features_f(G, sc, (float)(d * utau / nu), Xs[wid][lane]);
+        } else if (lane < nrow) {
             const long long c = c0 + lane;
             const int ix = (int)(c % NX), iy = (int)((c / NX) % NY), iz = (int)(c / NXY);
             const int xm = ix == 0 ? NX - 1 : ix - 1, xp = ix + 1 == NX ? 0 : ix + 1;
@@ -281,8 +312,9 @@ __global__ void __launch_bounds__(128, 4) k_turb_mlp(TurbArgs<T> a, const float*
             mlp_forward_tile(S, ax, z1, z2, h1a, z3);
             if (t == 0) {
                 const long long cb = c0 + 16 * h;
-                if (gq < nr) a.nu_t[cb + gq] = (T)(nu * softplus(z3[0]));
-                if (gq + 8 < nr) a.nu_t[cb + gq + 8] = (T)(nu * softplus(z3[1]));
+                const long long top = COLL ? (long long)(NZ - 1) * (long long)NXY : N;  // first cell without element
+                if (gq < nr && cb + gq < top) a.nu_t[cb + gq] = (T)(nu * softplus(z3[0]));
+                if (gq + 8 < nr && cb + gq + 8 < top) a.nu_t[cb + gq + 8] = (T)(nu * softplus(z3[1]));
             }
         }
         __syncwarp();
@@ -308,7 +340,8 @@ template <typename T>
 void launch_turb_mlp(const TurbArgs<T>& a, const float* P, cudaStream_t s) {
     const long long ngrp = (a.g.N + 31) / 32;
     const int nb = (int)std::max<long long>(1, std::min<long long>((ngrp + 3) / 4, 148 * 6));
-    k_turb_mlp<T><<<nb, 128, 0, s>>>(a, P);
+    if (a.g.scheme == TC_SCHEME_COLLOC) k_turb_mlp<T, true><<<nb, 128, 0, s>>>(a, P);
+    else k_turb_mlp<T, false><<<nb, 128, 0, s>>>(a, P);
 }
 
 template void launch_les_filter<double>(const double*, const double*, const double*, const double*, const double*,

@@ -929,7 +929,6 @@ extern "C" int tc_set_turb_model(tc_handle* h, int kind, const void* weights) {
     if (h->g.visc_type == TC_VISC_CROSS) return fail(TC_E_ARG, "tc_set_turb_model: CROSS viscosity has no nu_t");
     cudaSetDevice(h->prm.device);
     if (kind == TC_TURB_MLP) {
-        if (h->g.scheme == TC_SCHEME_COLLOC) return fail(TC_E_ARG, "tc_set_turb_model: the learned closure is for the staggered schemes");
         if (!weights) return fail(TC_E_ARG, "tc_set_turb_model: TC_TURB_MLP needs TC_MLP_NPAR float parameters");
         if (!h->mlp_params && cudaMalloc(&h->mlp_params, MLP_NPAR * sizeof(float)) != cudaSuccess)
             return fail(TC_E_NOMEM, "closure parameters");
