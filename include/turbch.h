@@ -166,6 +166,12 @@ int tc_op_apply_gradient(tc_handle* h, const double* p, double* grad_aos);      
 int tc_op_apply_divergence(tc_handle* h, const double* vel_aos, double* div);      /* ApplyDivergence */
 int tc_op_unapply_gradient(tc_handle* h, const double* vel_aos, double* p);        /* UnapplyGradient */
 int tc_op_pressure_solve(tc_handle* h, const double* rhs, double* p);              /* LinearSystemSolveFFT */
+/* LinearSystemSolveFFT on device arrays (staggered/func_global.h:214-248 works on the
+ * data object's device members): rhs and p are device buffers of N values in the working
+ * precision (double for TC_FP64, float for TC_MIXED), cells [z][y][x]; rhs may equal p.
+ * Asynchronous on the solver's stream (tc_get_stream); the same kernels as
+ * tc_op_pressure_solve. */
+int tc_pressure_solve_device(tc_handle* h, const void* rhs, void* p);
 int tc_op_turb_visc(tc_handle* h, const double* vel_aos, double* nu_t);            /* RecalcTurbVisc  */
 int tc_set_nu_t(tc_handle* h, const double* nu_t);
 int tc_get_nu_t(tc_handle* h, double* nu_t);

@@ -300,3 +300,32 @@ def test_run_adaptive_controls_cfl(precision):
     assert np.all(np.isfinite(v)) and np.all(np.isfinite(p))
     assert abs(S.CalcIntegral(cur)[0] / prod["area"] - 1.0) < (1e-10 if precision == 0 else 1e-5)
     S.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("name", ["hw2_dns", "vv4_pow23", "coll_cross"])
+def test_pressure_solve_on_device_buffers(name, precision):
+    """tc_pressure_solve_device (device arrays in the working precision, in place or not)
+    gives exactly tc_op_pressure_solve's result."""
+    import torch
+
+    import turbchannel_b200 as tb
+
+    prod, _, zz = make_case(precision=precision, **CASES[name])
+    S = tb.Solver(prod, zz)
+    rng = np.random.default_rng(4)
+    rhs = rng.standard_normal(S.N)
+    rhs -= rhs.mean()
+    want = S.LinearSystemSolveFFT(rhs)
+    dt = torch.float64 if precision == 0 else torch.float32
+    r = torch.tensor(rhs, dtype=dt, device="cuda")
+    out = torch.empty_like(r)
+    torch.cuda.synchronize()
+    S.pressure_solve_device(r.data_ptr(), out.data_ptr())
+    S.sync()
+    got = out.double().cpu().numpy()
+    assert np.array_equal(got, want.astype(np.float32).astype(np.float64) if precision else want)
+    S.pressure_solve_device(r.data_ptr(), r.data_ptr())  # in place
+    S.sync()
+    assert np.array_equal(r.double().cpu().numpy(), got)
+    S.close()

@@ -43,7 +43,7 @@ EXPORTS = [
     "tc_op_unapply_gradient", "tc_op_pressure_solve", "tc_op_turb_visc", "tc_set_nu_t", "tc_get_nu_t",
     "tc_init_channel", "tc_mesh_tanh", "tc_phase_timing", "tc_phase_times", "tc_launch_count",
     "tc_op_pressure_solve_static", "tc_set_diag_fusion", "tc_checkpoint_save", "tc_checkpoint_load",
-    "tc_stats_accumulate", "tc_stats_read", "tc_stats_reset", "tc_run_graph",
+    "tc_stats_accumulate", "tc_stats_read", "tc_stats_reset", "tc_run_graph", "tc_pressure_solve_device",
 ]
 # Every entry point declared in include/turbch_les.h (learned LES closure).
 EXPORTS_LES = [
@@ -88,6 +88,7 @@ def load_library(path: str = LIB_PATH):
     L.tc_stats_accumulate.argtypes = [vp, ip, C.c_double]
     L.tc_stats_read.argtypes = [vp, vp, dp]
     L.tc_stats_reset.argtypes = [vp]
+    L.tc_pressure_solve_device.argtypes = [vp, vp, vp]
     L.tc_run_graph.argtypes = [vp, C.c_double, ip, ip, ip, ip, C.c_double, C.c_double, C.POINTER(ip), dp]
     L.tc_set_turb_model.argtypes = [vp, ip, vp]
     L.tc_integral.argtypes = [vp, ip, vp]
@@ -213,6 +214,11 @@ class Solver:
     def save_checkpoint(self, path: str, current_field: int, t: float):
         """All four ring levels and the forcing state, for an exact restart."""
         self._check(self.L.tc_checkpoint_save(self.h, os.fsencode(path), current_field, t))
+
+    def pressure_solve_device(self, rhs_ptr: int, p_ptr: int):
+        """The pressure solve on device buffers (addresses, working precision), asynchronous
+        on the solver's stream."""
+        self._check(self.L.tc_pressure_solve_device(self.h, rhs_ptr, p_ptr))
 
     def run_graph(self, tau: float, current_field: int, nsteps: int, check_every: int = 8, cfl_mode: int = 3,
                   cfl_min: float = 0.0, cfl_max: float = float("inf")):

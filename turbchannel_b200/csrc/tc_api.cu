@@ -1162,6 +1162,19 @@ extern "C" int tc_op_pressure_solve(tc_handle* h, const double* rhs, double* p) 
     TC_OPCHK(h, rhs, p);
     return TC_DISPATCH(h, op_psolve, h, rhs, p);
 }
+
+// LinearSystemSolveFFT on device arrays (staggered/func_global.h:214-248): the same
+// kernels as tc_op_pressure_solve without the host copies, asynchronous on the solver's
+// stream; rhs and p in the working precision, cells [z][y][x]; rhs may equal p.
+template <typename T>
+static int dev_psolve(tc_handle* h, const void* rhs, void* p) {
+    poisson<T>(h, nullptr, rhs, p);
+    return check_launch("tc_pressure_solve_device");
+}
+extern "C" int tc_pressure_solve_device(tc_handle* h, const void* rhs, void* p) {
+    TC_OPCHK(h, rhs, p);
+    return TC_DISPATCH(h, dev_psolve, h, rhs, p);
+}
 extern "C" int tc_op_turb_visc(tc_handle* h, const double* v, double* nt) {
     if (h) h->fused_valid = false;
     TC_OPCHK(h, v, nt);
