@@ -364,3 +364,47 @@ def test_config1_hundred_steps_match_oracle(precision):
     assert rel_err(ps, po) < tp, rel_err(ps, po)
     assert abs(S.CalcKineticEnergy(cur) - O.kinetic_energy(cur)) <= tv * O.kinetic_energy(cur)
     S.close()
+
+
+FULL_SIZE = {
+    # staggered VV4 DNS, 384 x 256 x 384 cells (x, wall-normal, span), Re_b 21900, tanh 2.2
+    "vv4_384x256x384": dict(scheme=VV4, NX=384, NY=384, NZ=256, Lx=2 * np.pi, Ly=np.pi, Re_b=21900.0, gamma=2.2,
+                            tau=0.0008),
+    # collocated DNS, 256 x 192 x 256 nodes, Re_b 13750, tanh 2.0
+    "coll_256x192x256": dict(scheme=COLLOC, NX=256, NY=256, NZ=192, Lx=2 * np.pi, Ly=np.pi, Re_b=13750.0, gamma=2.0,
+                             tau=0.001),
+}
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("name", list(FULL_SIZE))
+def test_full_size_configurations_match_oracle(name, precision):
+    """The flow configurations at their full sizes, three SBDF steps (orders 1, 2, 3) from
+    the seeded field with constant flow rate, against the FP64 oracle: 1e-10 (FP64) /
+    2e-4 (mixed) relative on the velocity, 20x that on the pressure."""
+    import oracle_py as op
+    import turbchannel_b200 as tb
+
+    c = dict(FULL_SIZE[name])
+    tau = c.pop("tau")
+    prod, orc, zz = make_case(precision=precision, **c)
+    S = tb.Solver(prod, zz)
+    O = op.Oracle(orc, zz, "f64")
+    O.init_channel(0, seed=12345, amp=0.1, project=True)
+    v0, p0 = O.get_level(0)
+    for lvl in range(4):
+        S.upload_level(lvl, np.zeros_like(v0), np.zeros_like(p0))
+    S.upload_level(0, v0, p0)
+    del v0, p0
+    S.set_forcing(1, 1.0)
+    cur = 0
+    for it in range(3):
+        S.Step(it * tau, tau, cur, it + 1)
+        O.step(it * tau, tau, cur, it + 1, cfr=1.0)
+        cur = (cur + 1) % 4
+    tol = TOL[precision]["step"]
+    vs, ps = S.download_level(cur)
+    vo, po = O.get_level(cur)
+    assert rel_err(vs, vo) < tol, rel_err(vs, vo)
+    assert rel_err(ps, po) < 20 * tol, rel_err(ps, po)
+    S.close()
