@@ -487,14 +487,6 @@ void launch_zsolve(const ZSolveArgs<T>& a, cudaStream_t s, cudaStream_t side, cu
 // {F0,F1} then B[i][mh] = B0.  The per-step solve streams r, F, B with no divide and
 // a one-FMA recurrence chain, one thread per pair (ky, NY-ky) reading the factors once.
 // ---------------------------------------------------------------------------
-template <typename T>
-struct alignas(4 * sizeof(T)) Q4 {
-    T x, y, z, w;
-};
-template <typename T>
-struct alignas(2 * sizeof(T)) Q2 {
-    T x, y;
-};
 
 size_t zfactor_low_bytes(const Geom& g) {
     const size_t per = g.scheme == TC_SCHEME_VV4 ? 8 : 3;
@@ -753,14 +745,48 @@ __global__ void __launch_bounds__(128) k_zsolve_fac(ZSolveArgs<T> a) {
 
 // The low-|k| modes (kx < LM, |ky| < LM) in double from their double factors; mode
 // (0,0) also normalised.  One CTA per mode: the column and its factors are staged into
-// shared memory by all threads, one thread runs the two sweeps there (shared-memory
-// latency per row), all threads write the column back.
+// shared memory by all threads, one thread runs the two sweeps there, LOWB rows at a
+// time (the batch's shared loads issued before its recurrence, so only the one-FMA
+// chain per row is serial), all threads normalise the mean mode and write the column
+// back.
+constexpr int LOWB = 8;
+
+// Mean-mode normalisation of a column held in shared memory (stride 1), every thread
+// of the CTA taking part: the same shift as normalize_mean_mode, the weighted sum
+// reduced over the CTA instead of one thread.
+template <typename MD>
+__device__ void normalize_mean_column(const Geom& g, const MD& m, cplx<double>* xs, double* red) {
+    const int NZ = g.NZ;
+    double part = 0;
+    for (int i = threadIdx.x; i < NZ; i += blockDim.x) {
+        double wgt;
+        if (g.scheme == TC_SCHEME_VV4) wgt = m.dKERG[i] * m.dDZ[i];
+        else if (g.scheme == TC_SCHEME_HW2) wgt = m.dDZ[i];
+        else wgt = m.dcellh[i] * g.hx * g.hy;
+        part += xs[i].x * wgt;
+    }
+    part = warp_sum(part);
+    const int nw = (int)(blockDim.x >> 5);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = part;
+    __syncthreads();
+    double psum = 0;
+    for (int w = 0; w < nw; w++) psum += red[w];
+    double c;
+    if (g.scheme == TC_SCHEME_VV4) c = psum / m.KERG_norm2;
+    else if (g.scheme == TC_SCHEME_HW2) c = psum / (m.dZZ[NZ] - m.dZZ[0]);
+    else c = (double)g.NXY * (psum * g.hx * g.hy / g.area);  // collocated_AB3/func_global.h:163-170
+    for (int i = threadIdx.x; i < NZ; i += blockDim.x)
+        xs[i].x -= g.scheme == TC_SCHEME_VV4 ? c * m.dKERG[i] : c;
+    __syncthreads();
+}
+
 template <typename T, int SCHEME>
 __global__ void __launch_bounds__(128) k_zsolve_low_fac(ZSolveArgs<T> a) {
     constexpr bool VV = SCHEME == TC_SCHEME_VV4;
     using FQ = typename std::conditional<VV, Q4<double>, Q2<double>>::type;
     using BQ = typename std::conditional<VV, Q4<double>, double>::type;
     extern __shared__ __align__(32) unsigned char smraw[];
+    __shared__ double red[4];
     const Geom& g = a.g;
     const int LM = g.low_modes, nky = 2 * LM - 1;
     const int idx = blockIdx.x;
@@ -788,59 +814,80 @@ __global__ void __launch_bounds__(128) k_zsolve_low_fac(ZSolveArgs<T> a) {
     __syncthreads();
     if (threadIdx.x == 0) {
         cplx<double> z1 = {0, 0}, z2 = {0, 0}, z3 = {0, 0};
-        for (int i = 0; i < NZ; i++) {
-            const FQ f = sF[i];
-            const cplx<double> r = xs[i];
-            cplx<double> z;
-            if constexpr (VV) {
-                z.x = r.x * f.x - f.w * z3.x - f.z * z2.x;
-                z.y = r.y * f.x - f.w * z3.y - f.z * z2.y;
-            } else {
-                z.x = r.x * f.x;
-                z.y = r.y * f.x;
+        for (int i0 = 0; i0 < NZ; i0 += LOWB) {
+            FQ f[LOWB];
+            cplx<double> r[LOWB];
+#pragma unroll
+            for (int k = 0; k < LOWB; k++)
+                if (i0 + k < NZ) {
+                    f[k] = sF[i0 + k];
+                    r[k] = xs[i0 + k];
+                }
+#pragma unroll
+            for (int k = 0; k < LOWB; k++) {
+                if (i0 + k >= NZ) break;
+                cplx<double> z;
+                if constexpr (VV) {
+                    z.x = r[k].x * f[k].x - f[k].w * z3.x - f[k].z * z2.x;
+                    z.y = r[k].y * f[k].x - f[k].w * z3.y - f[k].z * z2.y;
+                } else {
+                    z.x = r[k].x * f[k].x;
+                    z.y = r[k].y * f[k].x;
+                }
+                z.x -= f[k].y * z1.x;
+                z.y -= f[k].y * z1.y;
+                xs[i0 + k] = z;
+                z3 = z2;
+                z2 = z1;
+                z1 = z;
             }
-            z.x -= f.y * z1.x;
-            z.y -= f.y * z1.y;
-            xs[i] = z;
-            z3 = z2;
-            z2 = z1;
-            z1 = z;
         }
         cplx<double> x1 = {0, 0}, x2 = {0, 0}, x3 = {0, 0};
-        for (int i = NZ - 1; i >= 0; i--) {
-            const BQ b = sB[i];
-            const cplx<double> zz = xs[i];
-            cplx<double> v;
-            if constexpr (VV) {
-                v.x = zz.x - b.z * x3.x - b.y * x2.x;
-                v.y = zz.y - b.z * x3.y - b.y * x2.y;
-                v.x -= b.x * x1.x;
-                v.y -= b.x * x1.y;
-            } else {
-                v.x = zz.x - b * x1.x;
-                v.y = zz.y - b * x1.y;
+        for (int i0 = NZ - 1; i0 >= 0; i0 -= LOWB) {
+            BQ bq[LOWB];
+            cplx<double> zz[LOWB];
+#pragma unroll
+            for (int k = 0; k < LOWB; k++)
+                if (i0 - k >= 0) {
+                    bq[k] = sB[i0 - k];
+                    zz[k] = xs[i0 - k];
+                }
+#pragma unroll
+            for (int k = 0; k < LOWB; k++) {
+                if (i0 - k < 0) break;
+                cplx<double> v;
+                if constexpr (VV) {
+                    v.x = zz[k].x - bq[k].z * x3.x - bq[k].y * x2.x;
+                    v.y = zz[k].y - bq[k].z * x3.y - bq[k].y * x2.y;
+                    v.x -= bq[k].x * x1.x;
+                    v.y -= bq[k].x * x1.y;
+                } else {
+                    v.x = zz[k].x - bq[k] * x1.x;
+                    v.y = zz[k].y - bq[k] * x1.y;
+                }
+                xs[i0 - k] = v;
+                x3 = x2;
+                x2 = x1;
+                x1 = v;
             }
-            xs[i] = v;
-            x3 = x2;
-            x2 = x1;
-            x1 = v;
-        }
-        if (m == 0) {
-            ZSolveArgs<double> b;
-            b.g = g;
-            b.g.NXH = 1;
-            b.g.NY = 1;  // a single column: stride 1 between z
-            b.m.dDZ = a.m.dDZ; b.m.dKERG = a.m.dKERG; b.m.dcellh = a.m.dcellh; b.m.dZZ = a.m.dZZ;
-            b.m.KERG_norm2 = a.m.KERG_norm2;
-            b.spec = xs;
-            normalize_mean_mode(b);
         }
     }
     __syncthreads();
+    if (m == 0) normalize_mean_column(g, a.m, xs, red);
     for (int i = threadIdx.x; i < NZ; i += blockDim.x) {
         const cplx<double> v = xs[i];
         a.spec[(size_t)i * M + m] = {(T)v.x, (T)v.y};
     }
+}
+
+template <typename T, int SCHEME>
+static void zsolve_low_scheme(const ZSolveArgs<T>& a, cudaStream_t s) {
+    const int nlow = a.g.low_modes * (2 * a.g.low_modes - 1);
+    const size_t smem = (((size_t)a.g.NZ * (SCHEME == TC_SCHEME_VV4 ? 64 : 24) + 31) & ~(size_t)31) +
+                        (size_t)a.g.NZ * sizeof(cplx<double>);
+    auto k = k_zsolve_low_fac<T, SCHEME>;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k<<<nlow, 128, smem, s>>>(a);
 }
 
 template <typename T, int SCHEME>
@@ -850,12 +897,7 @@ static void zsolve_fac_scheme(const ZSolveArgs<T>& a, cudaStream_t s, cudaStream
     // stream next to the factored solve of all other modes; the two sets are disjoint
     cudaEventRecord(fork, s);
     cudaStreamWaitEvent(side, fork, 0);
-    const int nlow = a.g.low_modes * (2 * a.g.low_modes - 1);
-    const size_t smem = (((size_t)a.g.NZ * (SCHEME == TC_SCHEME_VV4 ? 64 : 24) + 31) & ~(size_t)31) +
-                        (size_t)a.g.NZ * sizeof(cplx<double>);
-    auto k = k_zsolve_low_fac<T, SCHEME>;
-    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k<<<nlow, 128, smem, side>>>(a);
+    zsolve_low_scheme<T, SCHEME>(a, side);
     cudaEventRecord(join, side);
     const size_t MH = (size_t)a.g.NXH * (a.g.NY / 2 + 1);
     k_zsolve_fac<T, SCHEME><<<(unsigned)((2 * MH + 127) / 128), 128, 0, s>>>(a);

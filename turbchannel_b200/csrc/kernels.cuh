@@ -61,6 +61,16 @@ struct YFftArgs {
     int sign;
 };
 
+// Rows of the z-solve factors (k_zfactor layout): four or two values of one mode.
+template <typename T>
+struct alignas(4 * sizeof(T)) Q4 {
+    T x, y, z, w;
+};
+template <typename T>
+struct alignas(2 * sizeof(T)) Q2 {
+    T x, y;
+};
+
 // Banded wall-normal solve per (kx, ky) mode, in place on spec; normalisation of
 // the mean mode (staggered/func_global.h:657-675) applied to mode (0, 0).
 template <typename T>
