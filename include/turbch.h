@@ -159,6 +159,29 @@ int tc_diagnostics(tc_handle* h, int level, double tau, double integral[3], doub
  * The results agree to round-off (summation order). */
 int tc_set_diag_fusion(tc_handle* h, int mode);
 
+/* Segregated IMEX Runge-Kutta step of the collocated scheme (collocated_SRK:
+ * data::Step, func_global.h:317-408; method tables as collocated_SRK/imex.h:10-41).
+ * The handle must be collocated with cross viscosity and no turbulence model; the
+ * explicit term is then collocated_SRK's ExplicitTerm (func_global.h:270-307), the
+ * source term the handle's sour_dpdx.  tc_srk_init takes the method as the reference's
+ * main.cpp copies it into its data object (main.cpp:342-352): type TC_IMEX_*, stage
+ * count S <= TC_SRK_MAX_STAGES, Butcher tables of (S+1) x S row-major values (last row
+ * b), StabType 0 (Du + Sp = 0) or 1 (Du + S dp/dt = 0) and alpha_tau (the reference
+ * uses half the method's alpha_tau_max).  It allocates the stage buffers (S+3 vectors,
+ * 2S+4 scalars of the working precision) and switches the handle's pressure
+ * normalisation to collocated_SRK's (shift sum(p vol)/area, func_global.h:130-137).
+ * tc_srk_step advances ring level 0 (velocity, pressure) by tau, with dp/dt (StabType
+ * 1) in the pressure slot of level 1 (the reference's qressure); t is accepted for the
+ * reference's signature.  The reference's implicit term is identically zero
+ * (func_global.h:310-315), so its Ku terms are left out (exact zeros). */
+#define TC_SRK_MAX_STAGES 6
+#define TC_IMEX_A 0
+#define TC_IMEX_ARS 1
+#define TC_IMEX_CK 2
+int tc_srk_init(tc_handle* h, int imex_type, int nstages, const double* butcher_e, const double* butcher_i,
+                int stab_type, double alpha_tau);
+int tc_srk_step(tc_handle* h, double t, double tau);
+
 /* Operator-level entry points on host buffers (the reference's operator methods,
  * used by its CPU/GPU self-checks, staggered/selftest.cpp:360-438). */
 int tc_op_explicit_term(tc_handle* h, const double* vel_aos, double* flux_aos);    /* ExplicitTerm    */

@@ -44,6 +44,7 @@ EXPORTS = [
     "tc_init_channel", "tc_mesh_tanh", "tc_phase_timing", "tc_phase_times", "tc_launch_count",
     "tc_op_pressure_solve_static", "tc_set_diag_fusion", "tc_checkpoint_save", "tc_checkpoint_load",
     "tc_stats_accumulate", "tc_stats_read", "tc_stats_reset", "tc_run_graph", "tc_pressure_solve_device",
+    "tc_srk_init", "tc_srk_step",
 ]
 # Every entry point declared in include/turbch_les.h (learned LES closure).
 EXPORTS_LES = [
@@ -108,6 +109,8 @@ def load_library(path: str = LIB_PATH):
     L.tc_phase_times.argtypes = [vp, vp, C.POINTER(C.c_int)]
     L.tc_launch_count.argtypes = [vp, C.POINTER(C.c_ulonglong)]
     L.tc_set_diag_fusion.argtypes = [vp, ip]
+    L.tc_srk_init.argtypes = [vp, ip, ip, vp, vp, ip, C.c_double]
+    L.tc_srk_step.argtypes = [vp, C.c_double, C.c_double]
     ll = C.c_longlong
     L.tc_les_filter.argtypes = [vp, ip, ip, ip, vp]
     L.tc_les_samples.argtypes = [vp, ip, ip, ip, vp, vp]
@@ -337,6 +340,22 @@ class Solver:
     def set_diag_fusion(self, mode: int):
         """0 (default): separate diagnostics pass, 1: fused into the step, 2: fused while read every step."""
         self._check(self.L.tc_set_diag_fusion(self.h, mode))
+
+    def srk_init(self, method, stab_type: int = 1, alpha_tau: float = None):
+        """Set up the segregated IMEX Runge-Kutta step (collocated_SRK data::Step) with a
+        method of turbchannel_b200.imex (or any object with kind, S, E, I); alpha_tau
+        defaults to half the method's limit for the StabType, as the reference's driver
+        sets it (collocated_SRK/main.cpp:351-352)."""
+        if alpha_tau is None:
+            alpha_tau = method.alpha_tau(stab_type)
+        E = np.ascontiguousarray(method.E, dtype=np.float64)
+        I = np.ascontiguousarray(method.I, dtype=np.float64)
+        self._check(self.L.tc_srk_init(self.h, int(method.kind), int(method.S), _ptr(E), _ptr(I), int(stab_type),
+                                       float(alpha_tau)))
+
+    def srk_step(self, t: float, tau: float):
+        """One SRK step of ring level 0 (velocity, pressure); dp/dt in level 1's pressure."""
+        self._check(self.L.tc_srk_step(self.h, float(t), float(tau)))
 
     def phase_timing(self, on: bool):
         self._check(self.L.tc_phase_timing(self.h, 1 if on else 0))

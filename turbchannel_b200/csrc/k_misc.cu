@@ -751,4 +751,26 @@ TC_INST(double)
 TC_INST(float)
 #undef TC_INST
 
+// ---------------------------------------------------------------------------
+// Linear combinations of device arrays (SRK stage updates)
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) k_lincomb(LinComb<T> a) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride) {
+        T acc = (T)a.c[0] * a.x[0][i];
+        for (int k = 1; k < a.nt; k++) acc += (T)a.c[k] * a.x[k][i];
+        if (a.post != 1.0) acc = (T)a.post * acc;
+        a.out[i] = acc;
+    }
+}
+
+template <typename T>
+void launch_lincomb(const LinComb<T>& a, cudaStream_t s) {
+    const long long nb = std::min<long long>((a.n + 255) / 256, 148LL * 16);
+    k_lincomb<T><<<(unsigned)std::max<long long>(nb, 1), 256, 0, s>>>(a);
+}
+template void launch_lincomb<double>(const LinComb<double>&, cudaStream_t);
+template void launch_lincomb<float>(const LinComb<float>&, cudaStream_t);
+
 }  // namespace tc

@@ -153,9 +153,10 @@ __device__ void normalize_mean_mode(const ZSolveArgs<T>& a) {
         const double c = psum / (a.m.dZZ[g.NZ] - a.m.dZZ[0]);
         for (int i = 0; i < g.NZ; i++) x[i * zs].x = (T)((double)x[i * zs].x - c);
     } else {
-        // collocated_AB3/func_global.h:163-170 (shift = sum(p vol) hx hy / area)
+        // collocated_AB3/func_global.h:163-170 (shift = sum(p vol) hx hy / area) or, for
+        // the SRK step, collocated_SRK/func_global.h:130-137 (shift = sum(p vol) / area)
         for (int i = 0; i < g.NZ; i++) psum += (double)x[i * zs].x * (a.m.dcellh[i] * g.hx * g.hy);
-        const double c = (double)g.NXY * (psum * g.hx * g.hy / g.area);
+        const double c = (double)g.NXY * (g.norm_srk ? psum / g.area : psum * g.hx * g.hy / g.area);
         for (int i = 0; i < g.NZ; i++) x[i * zs].x = (T)((double)x[i * zs].x - c);
     }
 }
@@ -774,7 +775,7 @@ __device__ void normalize_mean_column(const Geom& g, const MD& m, cplx<double>* 
     double c;
     if (g.scheme == TC_SCHEME_VV4) c = psum / m.KERG_norm2;
     else if (g.scheme == TC_SCHEME_HW2) c = psum / (m.dZZ[NZ] - m.dZZ[0]);
-    else c = (double)g.NXY * (psum * g.hx * g.hy / g.area);  // collocated_AB3/func_global.h:163-170
+    else c = (double)g.NXY * (g.norm_srk ? psum / g.area : psum * g.hx * g.hy / g.area);
     for (int i = threadIdx.x; i < NZ; i += blockDim.x)
         xs[i].x -= g.scheme == TC_SCHEME_VV4 ? c * m.dKERG[i] : c;
     __syncthreads();

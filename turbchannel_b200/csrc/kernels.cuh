@@ -204,6 +204,20 @@ void launch_stats_acc(const double* planes, double* acc, int NZ, double inv_nxy,
 
 // State of a device-controlled run (tc_run_graph): bodies done, their bound, the CFL
 // number of the last check and the bounds that keep the loop going.
+// out[i] = post * (c[0] x[0][i] + c[1] x[1][i] + ... + c[nt-1] x[nt-1][i]), summed left
+// to right in T; x may alias out (elementwise).  The stage updates of the SRK step.
+constexpr int TC_LIN_MAX = 8;
+template <typename T>
+struct LinComb {
+    T* out;
+    const T* x[TC_LIN_MAX];
+    double c[TC_LIN_MAX];
+    double post;
+    int nt;
+    long long n;
+};
+template <typename T> void launch_lincomb(const LinComb<T>& a, cudaStream_t s);
+
 struct RunCtl {
     unsigned iters, max_iters;
     double cfl, cfl_min, cfl_max;

@@ -16,6 +16,8 @@
 #include <mutex>
 #include <random>
 #include <string>
+#include <initializer_list>
+#include <utility>
 #include <vector>
 
 #include "../../include/turbch_les.h"
@@ -234,6 +236,13 @@ struct tc_handle {
     double* fdiag_part = nullptr;  // NZ x correct_diag_chunks x TC_DIAG_STRIDE
     float* les_buf = nullptr;     // box-filter / feature scratch (tc_les_*), grown on demand
     size_t les_bytes = 0;
+    // segregated IMEX Runge-Kutta step of the collocated scheme (tc_srk_init/tc_srk_step)
+    struct Srk {
+        int S = 0, type = 0, stab = 1;
+        double BE[TC_SRK_MAX_STAGES * (TC_SRK_MAX_STAGES + 1)] = {}, BI[TC_SRK_MAX_STAGES * (TC_SRK_MAX_STAGES + 1)] = {};
+        double d[TC_SRK_MAX_STAGES] = {}, alpha_tau = 0;
+        void* buf = nullptr;  // one allocation: kuhat[S], bufv, gradv, nu1 (vectors); mujt[S], qj[S], bufs, muj, pjhat, pj
+    } srk;
     // instrumentation
     unsigned long long launches = 0;
     bool timing = false;
@@ -299,7 +308,8 @@ static const cplx<T>* twy(const tc_handle* h) { return (const cplx<T>*)h->tw + h
 
 static void free_all(tc_handle* h) {
     void* ptrs[] = {h->nu_t, h->ptmp, h->spec, h->zfac, h->zfac_low, h->mesh_t, h->fk, h->stats, h->mesh_d, h->tabs, h->tw, h->red, h->ticket,
-                    h->err_flag, h->planes, h->diag_part, h->stage, h->opv, h->opf, h->ops, h->mlp_params, h->les_buf, h->fdiag_part};
+                    h->err_flag, h->planes, h->diag_part, h->stage, h->opv, h->opf, h->ops, h->mlp_params, h->les_buf, h->fdiag_part,
+                    h->srk.buf};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (int l = 0; l < 4; l++) {
@@ -1175,6 +1185,216 @@ extern "C" int tc_pressure_solve_device(tc_handle* h, const void* rhs, void* p) 
     TC_OPCHK(h, rhs, p);
     return TC_DISPATCH(h, dev_psolve, h, rhs, p);
 }
+// ---------------------------------------------------------------------------
+// Segregated IMEX Runge-Kutta step of the collocated scheme (collocated_SRK/
+// func_global.h:317-408, data::Step).  The reference's implicit part is empty
+// (ImplicitTerm sets Ku = 0, ImplicitStage copies u*: func_global.h:310-315), so
+// every Ku term is an exact zero and is left out.  Velocity and pressure live in ring
+// level 0, dp/dt (StabType 1) in the pressure slot of level 1.  The explicit term is
+// the collocated cross-viscosity flux with the source term, the same operator as
+// collocated_AB3's CalcFluxTerm_FD (func_fluxes.h:86-117) and collocated_SRK's
+// ExplicitTerm (func_global.h:270-307); gradient and divergence + pressure solve as in
+// collocated_SRK/func_global.h:218-262.
+// ---------------------------------------------------------------------------
+struct SrkBufs {
+    char *kuhat, *bufv, *gradv, *nu1, *mujt, *qj, *bufs, *muj, *pjhat, *pj;
+    size_t vb, sb;
+};
+static SrkBufs srk_bufs(tc_handle* h, size_t eb) {
+    SrkBufs b;
+    const int S = h->srk.S;
+    b.vb = (size_t)3 * h->g.N * eb;
+    b.sb = (size_t)h->g.N * eb;
+    char* p = (char*)h->srk.buf;
+    b.kuhat = p;
+    p += S * b.vb;
+    b.bufv = p;
+    p += b.vb;
+    b.gradv = p;
+    p += b.vb;
+    b.nu1 = p;
+    p += b.vb;
+    b.mujt = p;
+    p += S * b.sb;
+    b.qj = p;
+    p += S * b.sb;
+    b.bufs = p;
+    p += b.sb;
+    b.muj = p;
+    p += b.sb;
+    b.pjhat = p;
+    p += b.sb;
+    b.pj = p;
+    return b;
+}
+static size_t srk_bytes(const tc_handle* h, int S, size_t eb) {
+    return ((size_t)(S + 3) * 3 + (size_t)2 * S + 4) * (size_t)h->g.N * eb;
+}
+
+template <typename T>
+struct SrkOps {
+    tc_handle* h;
+    void lin(void* out, long long n, std::initializer_list<std::pair<double, const void*>> terms, double post = 1.0) {
+        std::vector<std::pair<double, const void*>> v(terms);
+        lin_v(out, n, v, post);
+    }
+    void lin_v(void* out, long long n, const std::vector<std::pair<double, const void*>>& v, double post = 1.0) {
+        LinComb<T> a{};
+        a.out = (T*)out;
+        a.nt = (int)v.size();
+        for (int k = 0; k < a.nt; k++) {
+            a.c[k] = v[k].first;
+            a.x[k] = (const T*)v[k].second;
+        }
+        a.post = post;
+        a.n = n;
+        launch_lincomb<T>(a, h->st);
+        h->launches += 1;
+    }
+    void explicit_term(const void* v, void* out) {
+        FluxArgs<T> fa{};
+        fa.g = h->g;
+        fa.m = mesh_dev<T>(h);
+        fa.vel = cvec<T>((void*)v, h->g.N);
+        fa.fout = vec<T>(out, h->g.N);
+        fa.nu_t = nullptr;
+        fa.order = 0;
+        launch_flux_coll<T>(fa, h->st);
+        h->launches += 1;
+    }
+    void gradient(const void* p, void* out) {
+        CorrArgs<T> ca{};
+        ca.g = h->g;
+        ca.m = mesh_dev<T>(h);
+        ca.p = (const T*)p;
+        ca.vout = vec<T>(out, h->g.N);
+        ca.grad_only = 1;
+        launch_correct<T>(ca, h->st);
+        h->launches += 1;
+    }
+};
+
+template <typename T>
+static int srk_step_impl(tc_handle* h, double tau) {
+    const auto& s = h->srk;
+    const int S = s.S;
+    const long long N = h->g.N, N3 = 3 * N;
+    const SrkBufs b = srk_bufs(h, sizeof(T));
+    auto KH = [&](int j) { return (void*)(b.kuhat + j * b.vb); };
+    auto MT = [&](int j) { return (void*)(b.mujt + j * b.sb); };
+    auto QJ = [&](int j) { return (void*)(b.qj + j * b.sb); };
+    void* vel = h->vel[0];
+    void* pres = h->pres[0];
+    void* dpdt = h->pres[1];
+    const double ass = s.BI[S * S - 1], inv_ass = 1. / ass, tau_stage = tau * ass, inv_tau_stage = 1. / tau_stage;
+    const double alpha = s.alpha_tau / tau;
+    const bool ck = s.type == TC_IMEX_CK, atype = s.type == TC_IMEX_A;
+    SrkOps<T> op{h};
+    if (!atype) {  // func_global.h:324-328
+        op.explicit_term(vel, KH(0));
+        op.gradient(pres, b.gradv);
+        op.lin(KH(0), N3, {{1.0, KH(0)}, {-1.0, b.gradv}});
+    }
+    if (ck) op.lin(b.nu1, N3, {{1.0, KH(0)}, {alpha, vel}});  // func_global.h:329-332
+    const int j0 = atype ? 0 : 1;
+    std::vector<std::pair<double, const void*>> t;
+    for (int i = j0; i < S; i++) {
+        // stage velocity u = u_n + tau sum_j aE_ij Kuhat_j (func_global.h:340-347)
+        t.assign({{1.0, vel}});
+        for (int j = 0; j < i; j++) t.push_back({tau * s.BE[i * S + j], KH(j)});
+        op.lin_v(b.bufv, N3, t);
+        op.explicit_term(b.bufv, KH(i));
+        // right-hand side of the pressure system (func_global.h:356-380)
+        const double ck0 = ck ? (1. - s.alpha_tau * s.BI[i * S]) : 1.0;
+        if (s.stab == 0) {
+            t.assign({{ck0, pres}});
+            for (int j = j0; j < i; j++) t.push_back({inv_ass * s.BI[i * S + j], MT(j)});
+            op.lin_v(b.muj, N, t);
+            op.lin(b.bufs, N, {{1.0, b.muj}, {-(alpha * tau_stage), pres}});
+        } else {
+            t.assign({{tau_stage * ck0, dpdt}});
+            for (int j = j0; j < i; j++) t.push_back({inv_ass * s.BI[i * S + j], MT(j)});
+            op.lin_v(b.muj, N, t);
+            t.assign({{1.0, pres}});
+            if (ck) t.push_back({tau * s.BI[i * S], dpdt});
+            for (int j = j0; j < i; j++) t.push_back({tau * s.BI[i * S + j], QJ(j)});
+            op.lin_v(b.pjhat, N, t);
+            op.lin(b.bufs, N, {{1.0, b.muj}, {1.0, b.pjhat}, {-(alpha * tau_stage * tau_stage), dpdt}});
+        }
+        op.gradient(b.bufs, b.gradv);
+        t.assign({{1.0, KH(i)}, {-1.0, b.gradv}, {alpha, vel}});
+        if (ck) t.push_back({-s.d[i], b.nu1});
+        op.lin_v(b.bufv, N3, t);  // func_global.h:383-386
+        poisson<T>(h, b.bufv, nullptr, MT(i));  // UnapplyGradient
+        op.lin(b.pj, N, {{1.0, MT(i)}, {1.0, b.bufs}});  // func_global.h:391-395
+        if (s.stab) op.lin(MT(i), N, {{1.0, MT(i)}, {-(alpha * tau_stage * tau_stage), dpdt}});
+        else op.lin(MT(i), N, {{1.0, MT(i)}, {-(alpha * tau_stage), pres}});
+        if (s.stab) op.lin(QJ(i), N, {{1.0, b.pj}, {-1.0, b.pjhat}}, inv_tau_stage);
+        op.gradient(b.pj, b.gradv);
+        op.lin(KH(i), N3, {{1.0, KH(i)}, {-1.0, b.gradv}});
+    }
+    // final solution (func_global.h:400-407)
+    t.assign({{1.0, vel}});
+    for (int j = 0; j < S; j++) t.push_back({tau * s.BE[S * S + j], KH(j)});
+    op.lin_v(vel, N3, t);
+    TC_CUDA(cudaMemcpyAsync(pres, b.pj, b.sb, cudaMemcpyDeviceToDevice, h->st));
+    if (s.stab) TC_CUDA(cudaMemcpyAsync(dpdt, QJ(S - 1), b.sb, cudaMemcpyDeviceToDevice, h->st));
+    h->fused_valid = false;
+    return check_launch("tc_srk_step");
+}
+
+extern "C" int tc_srk_init(tc_handle* h, int imex_type, int nstages, const double* butcher_e, const double* butcher_i,
+                           int stab_type, double alpha_tau) {
+    if (!h || !butcher_e || !butcher_i) return fail(TC_E_ARG, "tc_srk_init: null argument");
+    if (h->g.scheme != TC_SCHEME_COLLOC || h->g.visc_type != TC_VISC_CROSS || h->nu_t)
+        return fail(TC_E_ARG, "tc_srk_init: needs the collocated scheme with cross viscosity and no turbulence model");
+    if (nstages < 1 || nstages > TC_SRK_MAX_STAGES || imex_type < TC_IMEX_A || imex_type > TC_IMEX_CK ||
+        stab_type < 0 || stab_type > 1)
+        return fail(TC_E_ARG, "tc_srk_init: bad method type, stage count or StabType");
+    const int S = nstages;
+    if (butcher_i[S * S - 1] == 0.0) return fail(TC_E_ARG, "tc_srk_init: a_ss of the implicit table is zero");
+    cudaSetDevice(h->prm.device);
+    const size_t eb = h->fp64 ? sizeof(double) : sizeof(float);
+    if (h->srk.buf) {
+        cudaFree(h->srk.buf);
+        h->srk.buf = nullptr;
+    }
+    if (cudaMalloc(&h->srk.buf, srk_bytes(h, S, eb)) != cudaSuccess) {
+        cudaGetLastError();
+        h->srk.buf = nullptr;
+        h->srk.S = 0;
+        return fail(TC_E_NOMEM, "tc_srk_init: stage buffers");
+    }
+    TC_CUDA(cudaMemsetAsync(h->srk.buf, 0, srk_bytes(h, S, eb), h->st));
+    auto& s = h->srk;
+    s.S = S;
+    s.type = imex_type;
+    s.stab = stab_type;
+    s.alpha_tau = alpha_tau;
+    for (int k = 0; k < S * (S + 1); k++) {
+        s.BE[k] = butcher_e[k];
+        s.BI[k] = butcher_i[k];
+    }
+    // coefficients d of the CK formulation (collocated_SRK/imex.cpp:37-46)
+    const double a_ss = s.BI[S * S - 1];
+    s.d[0] = 1.;
+    for (int j = 1; j < S; j++) {
+        s.d[j] = 0.;
+        for (int k = 0; k < j; k++) s.d[j] -= s.BI[j * S + k] * s.d[k] / a_ss;
+    }
+    h->g.norm_srk = 1;  // the SRK pressure normalisation (collocated_SRK/func_global.h:130-137)
+    return TC_OK;
+}
+
+extern "C" int tc_srk_step(tc_handle* h, double t, double tau) {
+    (void)t;  // the explicit term of the reference does not depend on time
+    if (!h) return fail(TC_E_ARG, "tc_srk_step: null handle");
+    if (h->srk.S == 0) return fail(TC_E_STATE, "tc_srk_step: tc_srk_init first");
+    if (!(tau > 0)) return fail(TC_E_ARG, "tc_srk_step: tau must be positive");
+    cudaSetDevice(h->prm.device);
+    return TC_DISPATCH(h, srk_step_impl, h, tau);
+}
+
 extern "C" int tc_op_turb_visc(tc_handle* h, const double* v, double* nt) {
     if (h) h->fused_valid = false;
     TC_OPCHK(h, v, nt);

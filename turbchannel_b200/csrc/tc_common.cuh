@@ -17,6 +17,10 @@ struct Geom {
     int NXH;      // NX/2 + 1 : kx range of the half spectrum
     int scheme, visc_type, turb, stab_type, fd_mode, low_modes;
     double visc, sour_dpdx, inv_ls, hx, hy, inv_hx, inv_hy, area;
+    // collocated pressure normalisation: 0 shift sum(p vol) hx hy / area
+    // (collocated_AB3/func_global.h:163-170), 1 shift sum(p vol) / area
+    // (collocated_SRK/func_global.h:130-137)
+    int norm_srk = 0;
 };
 
 // Mesh-derived arrays (device pointers into one allocation).  Staggered arrays
