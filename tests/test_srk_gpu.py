@@ -22,7 +22,7 @@ sys.path.insert(0, os.path.join(os.path.dirname(__file__), "..", "oracle"))
 
 pytestmark = pytest.mark.gpu
 
-CASES = [("ARS_343", 1), ("ARS_232", 0), ("ARK3", 1), ("ARK4", 0), ("BHR_553", 1), ("MARS_343", 0)]
+CASES = [("ARS_343", 1), ("ARS_232", 0), ("ARK3", 1), ("ARK4", 0), ("BHR_553", 1), ("MARS_343", 0), ("ARS_232:A", 1)]
 TOL = {0: dict(v=1e-10, p=1e-8), 1: dict(v=2e-4, p=5e-2)}
 
 
@@ -45,7 +45,10 @@ def test_srk_steps_match_oracle(name, stab, precision):
     rng = np.random.default_rng(32)
     p = 1e-2 * rng.standard_normal(N)
     q = 1e-2 * rng.standard_normal(N) if stab else np.zeros(N)
-    m = imex.METHODS[name]()
+    base, _, kind = name.partition(":")
+    m = imex.METHODS[base]()
+    if kind == "A":  # the type-A formulation (no explicit pre-stage)
+        m.kind = imex.A
     O = op.Oracle(orc, zz, "f64")
     so = SrkOracle(O, orc, zz, m.kind, m.S, m.E, m.I, stab, m.alpha_tau(stab))
     S = tb.Solver(prod, zz)

@@ -241,7 +241,7 @@ struct tc_handle {
         int S = 0, type = 0, stab = 1;
         double BE[TC_SRK_MAX_STAGES * (TC_SRK_MAX_STAGES + 1)] = {}, BI[TC_SRK_MAX_STAGES * (TC_SRK_MAX_STAGES + 1)] = {};
         double d[TC_SRK_MAX_STAGES] = {}, alpha_tau = 0;
-        void* buf = nullptr;  // one allocation: kuhat[S], bufv, gradv, nu1 (vectors); mujt[S], qj[S], bufs, muj, pjhat, pj
+        void* buf = nullptr;  // one allocation: kuhat[S], bufv, nu1 (vectors); mujt[S], qj[S], bufs, muj, pjhat, pj
     } srk;
     // instrumentation
     unsigned long long launches = 0;
@@ -1197,7 +1197,7 @@ extern "C" int tc_pressure_solve_device(tc_handle* h, const void* rhs, void* p) 
 // collocated_SRK/func_global.h:218-262.
 // ---------------------------------------------------------------------------
 struct SrkBufs {
-    char *kuhat, *bufv, *gradv, *nu1, *mujt, *qj, *bufs, *muj, *pjhat, *pj;
+    char *kuhat, *bufv, *nu1, *mujt, *qj, *bufs, *muj, *pjhat, *pj;
     size_t vb, sb;
 };
 static SrkBufs srk_bufs(tc_handle* h, size_t eb) {
@@ -1209,8 +1209,6 @@ static SrkBufs srk_bufs(tc_handle* h, size_t eb) {
     b.kuhat = p;
     p += S * b.vb;
     b.bufv = p;
-    p += b.vb;
-    b.gradv = p;
     p += b.vb;
     b.nu1 = p;
     p += b.vb;
@@ -1228,7 +1226,7 @@ static SrkBufs srk_bufs(tc_handle* h, size_t eb) {
     return b;
 }
 static size_t srk_bytes(const tc_handle* h, int S, size_t eb) {
-    return ((size_t)(S + 3) * 3 + (size_t)2 * S + 4) * (size_t)h->g.N * eb;
+    return ((size_t)(S + 2) * 3 + (size_t)2 * S + 4) * (size_t)h->g.N * eb;
 }
 
 template <typename T>
@@ -1262,13 +1260,15 @@ struct SrkOps {
         launch_flux_coll<T>(fa, h->st);
         h->launches += 1;
     }
-    void gradient(const void* p, void* out) {
+    // out = rhs - G p (the correction kernel with tob = 1; out may alias rhs)
+    void grad_sub(const void* rhs, const void* p, void* out) {
         CorrArgs<T> ca{};
         ca.g = h->g;
         ca.m = mesh_dev<T>(h);
+        ca.rhs = cvec<T>((void*)rhs, h->g.N);
         ca.p = (const T*)p;
         ca.vout = vec<T>(out, h->g.N);
-        ca.grad_only = 1;
+        ca.tob = (T)1;
         launch_correct<T>(ca, h->st);
         h->launches += 1;
     }
@@ -1292,8 +1292,7 @@ static int srk_step_impl(tc_handle* h, double tau) {
     SrkOps<T> op{h};
     if (!atype) {  // func_global.h:324-328
         op.explicit_term(vel, KH(0));
-        op.gradient(pres, b.gradv);
-        op.lin(KH(0), N3, {{1.0, KH(0)}, {-1.0, b.gradv}});
+        op.grad_sub(KH(0), pres, KH(0));
     }
     if (ck) op.lin(b.nu1, N3, {{1.0, KH(0)}, {alpha, vel}});  // func_global.h:329-332
     const int j0 = atype ? 0 : 1;
@@ -1321,17 +1320,16 @@ static int srk_step_impl(tc_handle* h, double tau) {
             op.lin_v(b.pjhat, N, t);
             op.lin(b.bufs, N, {{1.0, b.muj}, {1.0, b.pjhat}, {-(alpha * tau_stage * tau_stage), dpdt}});
         }
-        op.gradient(b.bufs, b.gradv);
-        t.assign({{1.0, KH(i)}, {-1.0, b.gradv}, {alpha, vel}});
+        op.grad_sub(KH(i), b.bufs, b.bufv);  // func_global.h:381-386
+        t.assign({{1.0, b.bufv}, {alpha, vel}});
         if (ck) t.push_back({-s.d[i], b.nu1});
-        op.lin_v(b.bufv, N3, t);  // func_global.h:383-386
+        op.lin_v(b.bufv, N3, t);
         poisson<T>(h, b.bufv, nullptr, MT(i));  // UnapplyGradient
         op.lin(b.pj, N, {{1.0, MT(i)}, {1.0, b.bufs}});  // func_global.h:391-395
         if (s.stab) op.lin(MT(i), N, {{1.0, MT(i)}, {-(alpha * tau_stage * tau_stage), dpdt}});
         else op.lin(MT(i), N, {{1.0, MT(i)}, {-(alpha * tau_stage), pres}});
         if (s.stab) op.lin(QJ(i), N, {{1.0, b.pj}, {-1.0, b.pjhat}}, inv_tau_stage);
-        op.gradient(b.pj, b.gradv);
-        op.lin(KH(i), N3, {{1.0, KH(i)}, {-1.0, b.gradv}});
+        op.grad_sub(KH(i), b.pj, KH(i));
     }
     // final solution (func_global.h:400-407)
     t.assign({{1.0, vel}});
