@@ -168,7 +168,7 @@ int tc_set_diag_fusion(tc_handle* h, int mode);
  * count S <= TC_SRK_MAX_STAGES, Butcher tables of (S+1) x S row-major values (last row
  * b), StabType 0 (Du + Sp = 0) or 1 (Du + S dp/dt = 0) and alpha_tau (the reference
  * uses half the method's alpha_tau_max).  It allocates the stage buffers (S+2 vectors,
- * 2S+4 scalars of the working precision) and switches the handle's pressure
+ * 2S+3 scalars of the working precision) and switches the handle's pressure
  * normalisation to collocated_SRK's (shift sum(p vol)/area, func_global.h:130-137).
  * tc_srk_step advances ring level 0 (velocity, pressure) by tau, with dp/dt (StabType
  * 1) in the pressure slot of level 1 (the reference's qressure); t is accepted for the

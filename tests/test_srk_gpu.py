@@ -29,13 +29,24 @@ TOL = {0: dict(v=1e-10, p=1e-8), 1: dict(v=2e-4, p=5e-2)}
 @pytest.mark.parametrize("precision", [0, 1])
 @pytest.mark.parametrize("name,stab", CASES)
 def test_srk_steps_match_oracle(name, stab, precision):
+    _srk_case(name, stab, precision, 32, 16, 17)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("name,stab", [("ARS_343", 1), ("ARK3", 0)])
+def test_srk_steps_match_oracle_ragged(name, stab, precision):
+    """NX, NY = 36, 18: a y-length without a compiled register transform (the pressure
+    solve's fallback kernels) and a non-power-of-two x-length."""
+    _srk_case(name, stab, precision, 36, 18, 11)
+
+
+def _srk_case(name, stab, precision, NX, NY, NZ):
     import oracle_py as op
     from srk_oracle import SrkOracle
 
     import turbchannel_b200 as tb
     from turbchannel_b200 import imex
 
-    NX, NY, NZ = 32, 16, 17
     prod, orc, zz = make_case(scheme=COLLOC, NX=NX, NY=NY, NZ=NZ, precision=precision)
     N, NXY = NX * NY * NZ, NX * NY
     v = 0.3 * seeded_field(N, NXY, seed=31, wall_w_zero=False)

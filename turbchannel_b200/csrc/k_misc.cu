@@ -773,4 +773,39 @@ void launch_lincomb(const LinComb<T>& a, cudaStream_t s) {
 template void launch_lincomb<double>(const LinComb<double>&, cudaStream_t);
 template void launch_lincomb<float>(const LinComb<float>&, cudaStream_t);
 
+template <typename T>
+__global__ void __launch_bounds__(256) k_srk_scal(SrkScal<T> a) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride) {
+        const T x = a.stab ? a.dpdt[i] : a.p[i];
+        if (a.mode == 0) {
+            T muj = (T)a.c0 * x;
+            for (int j = 0; j < a.nj; j++) muj += (T)a.cm[j] * a.mujt[j][i];
+            if (a.stab) {
+                T pjhat = a.p[i];
+                if (a.cpd != 0.0) pjhat += (T)a.cpd * x;
+                for (int j = 0; j < a.nj; j++) pjhat += (T)a.cq[j] * a.qj[j][i];
+                a.pjhat[i] = pjhat;
+                a.bufs[i] = muj + pjhat - (T)a.cb * x;
+            } else {
+                a.bufs[i] = muj - (T)a.cb * x;
+            }
+        } else {
+            const T m = a.mujt_i[i];
+            const T pj = m + a.bufs[i];
+            a.pj[i] = pj;
+            a.mujt_i[i] = m - (T)a.cb * x;
+            if (a.stab) a.qj_i[i] = (T)a.inv * (pj - a.pjhat[i]);
+        }
+    }
+}
+
+template <typename T>
+void launch_srk_scal(const SrkScal<T>& a, cudaStream_t s) {
+    const long long nb = std::min<long long>((a.n + 255) / 256, 148LL * 16);
+    k_srk_scal<T><<<(unsigned)std::max<long long>(nb, 1), 256, 0, s>>>(a);
+}
+template void launch_srk_scal<double>(const SrkScal<double>&, cudaStream_t);
+template void launch_srk_scal<float>(const SrkScal<float>&, cudaStream_t);
+
 }  // namespace tc

@@ -218,6 +218,28 @@ struct LinComb {
 };
 template <typename T> void launch_lincomb(const LinComb<T>& a, cudaStream_t s);
 
+// Pressure bookkeeping of one SRK stage (collocated_SRK/func_global.h:356-380 and
+// :391-395), one pass each.  rhs (mode 0): muj = c0 x + sum_j cm_j mujt_j with x = p
+// (StabType 0) or dp/dt (1); StabType 1 also pjhat = p + cpd dp/dt + sum_j cq_j qj_j;
+// bufs = muj + pjhat - cb dp/dt (1) or muj - cb p (0).  post (mode 1): pj = mujt_i +
+// bufs; mujt_i -= cb (dp/dt or p); StabType 1 also qj_i = inv (pj - pjhat).
+template <typename T>
+struct SrkScal {
+    int mode, stab, nj;
+    const T* p;
+    const T* dpdt;
+    const T* mujt[TC_LIN_MAX];
+    const T* qj[TC_LIN_MAX];
+    double c0, cm[TC_LIN_MAX], cq[TC_LIN_MAX], cpd, cb, inv;
+    T* bufs;
+    T* pjhat;
+    T* pj;
+    T* mujt_i;
+    T* qj_i;
+    long long n;
+};
+template <typename T> void launch_srk_scal(const SrkScal<T>& a, cudaStream_t s);
+
 struct RunCtl {
     unsigned iters, max_iters;
     double cfl, cfl_min, cfl_max;

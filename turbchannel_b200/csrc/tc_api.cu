@@ -241,7 +241,7 @@ struct tc_handle {
         int S = 0, type = 0, stab = 1;
         double BE[TC_SRK_MAX_STAGES * (TC_SRK_MAX_STAGES + 1)] = {}, BI[TC_SRK_MAX_STAGES * (TC_SRK_MAX_STAGES + 1)] = {};
         double d[TC_SRK_MAX_STAGES] = {}, alpha_tau = 0;
-        void* buf = nullptr;  // one allocation: kuhat[S], bufv, nu1 (vectors); mujt[S], qj[S], bufs, muj, pjhat, pj
+        void* buf = nullptr;  // one allocation: kuhat[S], bufv, nu1 (vectors); mujt[S], qj[S], bufs, pjhat, pj
     } srk;
     // instrumentation
     unsigned long long launches = 0;
@@ -1197,7 +1197,7 @@ extern "C" int tc_pressure_solve_device(tc_handle* h, const void* rhs, void* p) 
 // collocated_SRK/func_global.h:218-262.
 // ---------------------------------------------------------------------------
 struct SrkBufs {
-    char *kuhat, *bufv, *nu1, *mujt, *qj, *bufs, *muj, *pjhat, *pj;
+    char *kuhat, *bufv, *nu1, *mujt, *qj, *bufs, *pjhat, *pj;
     size_t vb, sb;
 };
 static SrkBufs srk_bufs(tc_handle* h, size_t eb) {
@@ -1218,15 +1218,13 @@ static SrkBufs srk_bufs(tc_handle* h, size_t eb) {
     p += S * b.sb;
     b.bufs = p;
     p += b.sb;
-    b.muj = p;
-    p += b.sb;
     b.pjhat = p;
     p += b.sb;
     b.pj = p;
     return b;
 }
 static size_t srk_bytes(const tc_handle* h, int S, size_t eb) {
-    return ((size_t)(S + 2) * 3 + (size_t)2 * S + 4) * (size_t)h->g.N * eb;
+    return ((size_t)(S + 2) * 3 + (size_t)2 * S + 3) * (size_t)h->g.N * eb;
 }
 
 template <typename T>
@@ -1303,32 +1301,40 @@ static int srk_step_impl(tc_handle* h, double tau) {
         for (int j = 0; j < i; j++) t.push_back({tau * s.BE[i * S + j], KH(j)});
         op.lin_v(b.bufv, N3, t);
         op.explicit_term(b.bufv, KH(i));
-        // right-hand side of the pressure system (func_global.h:356-380)
+        // right-hand side of the pressure system (func_global.h:356-380), one pass
         const double ck0 = ck ? (1. - s.alpha_tau * s.BI[i * S]) : 1.0;
-        if (s.stab == 0) {
-            t.assign({{ck0, pres}});
-            for (int j = j0; j < i; j++) t.push_back({inv_ass * s.BI[i * S + j], MT(j)});
-            op.lin_v(b.muj, N, t);
-            op.lin(b.bufs, N, {{1.0, b.muj}, {-(alpha * tau_stage), pres}});
-        } else {
-            t.assign({{tau_stage * ck0, dpdt}});
-            for (int j = j0; j < i; j++) t.push_back({inv_ass * s.BI[i * S + j], MT(j)});
-            op.lin_v(b.muj, N, t);
-            t.assign({{1.0, pres}});
-            if (ck) t.push_back({tau * s.BI[i * S], dpdt});
-            for (int j = j0; j < i; j++) t.push_back({tau * s.BI[i * S + j], QJ(j)});
-            op.lin_v(b.pjhat, N, t);
-            op.lin(b.bufs, N, {{1.0, b.muj}, {1.0, b.pjhat}, {-(alpha * tau_stage * tau_stage), dpdt}});
+        SrkScal<T> sc{};
+        sc.stab = s.stab;
+        sc.p = (const T*)pres;
+        sc.dpdt = (const T*)dpdt;
+        sc.n = N;
+        sc.bufs = (T*)b.bufs;
+        sc.pjhat = (T*)b.pjhat;
+        sc.mode = 0;
+        sc.nj = i - j0;
+        for (int j = j0; j < i; j++) {
+            sc.mujt[j - j0] = (const T*)MT(j);
+            sc.qj[j - j0] = (const T*)QJ(j);
+            sc.cm[j - j0] = inv_ass * s.BI[i * S + j];
+            sc.cq[j - j0] = tau * s.BI[i * S + j];
         }
+        sc.c0 = s.stab ? tau_stage * ck0 : ck0;
+        sc.cpd = (s.stab && ck) ? tau * s.BI[i * S] : 0.0;
+        sc.cb = s.stab ? alpha * tau_stage * tau_stage : alpha * tau_stage;
+        launch_srk_scal<T>(sc, h->st);
+        h->launches += 1;
         op.grad_sub(KH(i), b.bufs, b.bufv);  // func_global.h:381-386
         t.assign({{1.0, b.bufv}, {alpha, vel}});
         if (ck) t.push_back({-s.d[i], b.nu1});
         op.lin_v(b.bufv, N3, t);
         poisson<T>(h, b.bufv, nullptr, MT(i));  // UnapplyGradient
-        op.lin(b.pj, N, {{1.0, MT(i)}, {1.0, b.bufs}});  // func_global.h:391-395
-        if (s.stab) op.lin(MT(i), N, {{1.0, MT(i)}, {-(alpha * tau_stage * tau_stage), dpdt}});
-        else op.lin(MT(i), N, {{1.0, MT(i)}, {-(alpha * tau_stage), pres}});
-        if (s.stab) op.lin(QJ(i), N, {{1.0, b.pj}, {-1.0, b.pjhat}}, inv_tau_stage);
+        sc.mode = 1;  // func_global.h:391-395: pj, mujt_i, qj_i in one pass
+        sc.pj = (T*)b.pj;
+        sc.mujt_i = (T*)MT(i);
+        sc.qj_i = (T*)QJ(i);
+        sc.inv = inv_tau_stage;
+        launch_srk_scal<T>(sc, h->st);
+        h->launches += 1;
         op.grad_sub(KH(i), b.pj, KH(i));
     }
     // final solution (func_global.h:400-407)
