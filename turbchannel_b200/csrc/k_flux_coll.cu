@@ -14,6 +14,7 @@
 namespace tc {
 
 constexpr int CTX = 32, CTY = 8;
+constexpr int CPLANES = 128;  // planes whose constants a CTA keeps in shared memory
 
 template <typename T>
 struct CRing {
@@ -127,6 +128,21 @@ __global__ void __launch_bounds__(CTX* CTY, 2) k_flux_coll(FluxArgs<T> a, int tz
     const T inv_tau = a.inv_tau;
     const double* cDZ = a.m.dDZ;
     double ub = 0.0;
+    // per-plane constants of the CTA's planes, once in double: 2 / (DZ[z-1] + DZ[z]),
+    // visc inv_hz / DZ[z], visc inv_hz / DZ[z-1] (cross viscosity); the per-node work
+    // then has no double arithmetic (measured: the kernel is instruction-bound)
+    __shared__ T pc[3][CPLANES];
+    for (int k = threadIdx.x; k < ze - zb && k < CPLANES; k += blockDim.x) {
+        const int z = zb + k;
+        if (z == 0 || z == NZ - 1) {
+            pc[0][k] = pc[1][k] = pc[2][k] = T(0);
+        } else {
+            const double ihz = 2. / (cDZ[z - 1] + cDZ[z]);
+            pc[0][k] = (T)ihz;
+            pc[1][k] = (T)(g.visc * ihz / cDZ[z]);
+            pc[2][k] = (T)(g.visc * ihz / cDZ[z - 1]);
+        }
+    }
 
     for (int z = zb; z < ze; z++) {
         if (z + 1 < ze && z + 2 < NZ) load_plane(z + 2);
@@ -139,7 +155,8 @@ __global__ void __launch_bounds__(CTX* CTY, 2) k_flux_coll(FluxArgs<T> a, int tz
             T f[3] = {0, 0, 0};
             const bool wall = (z == 0 || z == NZ - 1);
             if (!wall) {
-                const T inv_hz = (T)(2. / (cDZ[z - 1] + cDZ[z]));
+                const int kz = z - zb;
+                const T inv_hz = kz < CPLANES ? pc[0][kz] : (T)(2. / (cDZ[z - 1] + cDZ[z]));
                 const T invh[3] = {ihx, ihy, inv_hz};
 #pragma unroll
                 for (int d = 0; d < 3; d++) {
@@ -169,7 +186,10 @@ __global__ void __launch_bounds__(CTX* CTY, 2) k_flux_coll(FluxArgs<T> a, int tz
                         const T u0 = A(c, 0, 0, 0);
                         f[c] += visc * ihx * ihx * (A(c, 1, 0, 0) + A(c, -1, 0, 0) - T(2.) * u0);
                         f[c] += visc * ihy * ihy * (A(c, 0, 1, 0) + A(c, 0, -1, 0) - T(2.) * u0);
-                        f[c] += visc * (T)(((double)A(c, 0, 0, 1) - u0) / cDZ[z] - ((double)u0 - A(c, 0, 0, -1)) / cDZ[z - 1]) * inv_hz;
+                        if (kz < CPLANES)
+                            f[c] += pc[1][kz] * (A(c, 0, 0, 1) - u0) - pc[2][kz] * (u0 - A(c, 0, 0, -1));
+                        else
+                            f[c] += visc * (T)(((double)A(c, 0, 0, 1) - u0) / cDZ[z] - ((double)u0 - A(c, 0, 0, -1)) / cDZ[z - 1]) * inv_hz;
                     }
                 }
                 f[0] += (T)g.sour_dpdx;
