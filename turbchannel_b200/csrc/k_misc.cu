@@ -765,8 +765,52 @@ __global__ void __launch_bounds__(256) k_lincomb(LinComb<T> a) {
     }
 }
 
+// The same combination over 16-byte vectors (n a multiple of the vector width, every
+// pointer 16-byte aligned): identical arithmetic per element, a quarter (float) or half
+// (double) of the load instructions.
+template <typename T>
+__global__ void __launch_bounds__(256) k_lincomb_v(LinComb<T> a) {
+    constexpr int W = 16 / sizeof(T);
+    using V = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+    const long long nv = a.n / W;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += stride) {
+        T acc[W];
+        {
+            const V x = reinterpret_cast<const V*>(a.x[0])[i];
+            const T* xe = reinterpret_cast<const T*>(&x);
+#pragma unroll
+            for (int w = 0; w < W; w++) acc[w] = (T)a.c[0] * xe[w];
+        }
+        for (int k = 1; k < a.nt; k++) {
+            const V x = reinterpret_cast<const V*>(a.x[k])[i];
+            const T* xe = reinterpret_cast<const T*>(&x);
+            const T c = (T)a.c[k];
+#pragma unroll
+            for (int w = 0; w < W; w++) acc[w] += c * xe[w];
+        }
+        if (a.post != 1.0) {
+#pragma unroll
+            for (int w = 0; w < W; w++) acc[w] = (T)a.post * acc[w];
+        }
+        V o;
+        T* oe = reinterpret_cast<T*>(&o);
+#pragma unroll
+        for (int w = 0; w < W; w++) oe[w] = acc[w];
+        reinterpret_cast<V*>(a.out)[i] = o;
+    }
+}
+
 template <typename T>
 void launch_lincomb(const LinComb<T>& a, cudaStream_t s) {
+    constexpr int W = 16 / sizeof(T);
+    bool vec = a.n % W == 0 && (reinterpret_cast<uintptr_t>(a.out) & 15) == 0;
+    for (int k = 0; k < a.nt; k++) vec = vec && (reinterpret_cast<uintptr_t>(a.x[k]) & 15) == 0;
+    if (vec) {
+        const long long nb = std::min<long long>((a.n / W + 255) / 256, 148LL * 16);
+        k_lincomb_v<T><<<(unsigned)std::max<long long>(nb, 1), 256, 0, s>>>(a);
+        return;
+    }
     const long long nb = std::min<long long>((a.n + 255) / 256, 148LL * 16);
     k_lincomb<T><<<(unsigned)std::max<long long>(nb, 1), 256, 0, s>>>(a);
 }
