@@ -43,11 +43,18 @@ WORKLOAD = dict(scheme=1, NX=384, NY=384, NZ=256, Lx=2 * math.pi, Ly=math.pi, Re
 PHASE_WORDS = {"turb": 2, "flux": 21, "div_xfft": 4, "yfft": 2, "zsolve": 2, "iyfft": 2, "ixfft": 2, "correct": 7}
 STEP_WORDS = 40
 FALLBACK_HBM_GBS = 6650.0
-# DRAM bytes per cell of one launch (dram__bytes_read.sum + dram__bytes_write.sum) from
-# the ncu captures summarised in profiles/flux_pair_vv4_192x192x128.md (float kernel) and
-# profiles/flux_vv4_192x128x192.md (double kernel), 4.7 M cells, inputs larger than L2;
-# traffic grows with the cell count, so it is scaled to the grid.
-TRAFFIC_BYTES_PER_CELL = {("flux", 4): (286.44e6 + 90.22e6) / 4718592, ("flux", 8): (591.3e6 + 208.6e6) / 4718592}
+# DRAM bytes per cell of one launch of a phase's kernels (dram__bytes_read.sum +
+# dram__bytes_write.sum from one ncu capture with inputs larger than L2, divided by the
+# captured grid's cells; traffic grows with the cell count, so it is scaled to the grid).
+# The captures, their grids and commands are recorded in profiles/traffic_per_cell.json.
+def traffic_per_cell() -> dict:
+    path = os.path.join(ROOT, "profiles", "traffic_per_cell.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return {(e["phase"], int(e["word_bytes"])): float(e["bytes_per_cell"]) for e in d["captures"]}
+    except (OSError, ValueError, KeyError):
+        return {}
 
 
 def peaks():
@@ -174,7 +181,7 @@ def roofline_for(arm, peak_gbs, word_bytes):
     dom = max(per, key=lambda k: per[k])
     bytes_alg = PHASE_WORDS[dom] * word_bytes * N
     ach = bytes_alg / (per[dom] * 1e-3) / 1e9
-    tpc = TRAFFIC_BYTES_PER_CELL.get((dom, word_bytes))
+    tpc = traffic_per_cell().get((dom, word_bytes))
     roof = {"kernel": dom, "bound": "hbm", "achieved": round(ach, 1), "peak": peak_gbs, "unit": "GB/s",
             "frac": round(ach / peak_gbs, 4), "traffic": None if tpc is None else round(tpc * N),
             "bytes_per_launch_alg": bytes_alg, "ms_per_launch": round(per[dom], 5)}
@@ -225,24 +232,59 @@ def e2e_arm(arm, steps, device):
     diag_ms = e0.elapsed_time(e1) / nd
     diag_bytes = p["NZ"] * 19 * 8
     field_bytes = 4 * N * 8
-    return dict(value=N * steps / (ms * 1e-3), unit="cell-steps/s", ms_per_step=ms / steps,
+    return dict(value=N * steps / (ms * 1e-3), unit="cell-steps/s", ms_per_step=ms / steps, steps=steps,
+                amortised=f"one state upload and one download over the {steps} steps; per-step diagnostics copy",
                 h2d_bytes_per_step=field_bytes // steps, d2h_bytes_per_step=diag_bytes + field_bytes // steps,
                 diagnostics_ms=round(diag_ms, 4))
 
 
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+# The reference's own CPU path at the bench workload's size, compiled from its sources by
+# `make -C oracle ref` (the 384 x 384 x 256 build uses the compile-time index-wrap
+# generalisation of oracle/ref/index_wrap.h; nothing else of the reference changes).
+REF_CPU_LIB = "stag_vv4_dns_c4_f64"
+
+
 def cpu_baseline(small=False, budget_s=20.0, max_steps=3):
-    """The oracle (CPU restatement of the reference path, OpenMP over all host
-    threads) on a bounded sample of the same workload."""
+    """The reference's CPU path (oracle/_ref, OpenMP over all host threads) on a bounded
+    sample of the same workload; the oracle (its CPU restatement, pinned to it) where that
+    build is absent or for the --small grid.  Constant flow rate as the oracle's driver
+    applies it after each step."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle_py as op
 
     w = dict(WORKLOAD)
     if small:
         w.update(NX=96, NY=96, NZ=64)
-    op.set_threads(os.cpu_count() or 1)
+    threads = os.cpu_count() or 1
+    op.set_threads(threads)
     p, zz = op.channel_params(w["scheme"], w["NX"], w["NY"], w["NZ"], w["Lx"], w["Ly"], w["Re_b"], w["gamma"])
-    O = op.Oracle(p, zz, "f64")
-    O.init_channel(0, seed=12345, amp=0.1, project=True)
+    kind = "reference" if (not small and op.ref_available(REF_CPU_LIB)) else "port"
+    if kind == "reference":
+        O = op.RefLib(REF_CPU_LIB)
+        O.L.ref_set_threads(threads)
+        O.setup(p, zz)
+        import ref_gpu_time as rg
+
+        v = rg.seeded_field(p, zz, w["scheme"])
+        O.set_level(0, v, np.zeros(v.shape[0]))
+        del v
+        O.project(0)
+        what = f"the reference's own CPU path (oracle/_ref/libref_{REF_CPU_LIB}.so)"
+    else:
+        O = op.Oracle(p, zz, "f64")
+        O.init_channel(0, seed=12345, amp=0.1, project=True)
+        what = "the oracle (CPU restatement of the reference's path)"
     tau = w["tau"]
     O.step(0.0, tau, 0, 1, cfr=1.0)  # untimed: first-touch of the solver's buffers
     cur, it, n = 1, 1, 0
@@ -254,9 +296,38 @@ def cpu_baseline(small=False, budget_s=20.0, max_steps=3):
             break
     dt = time.perf_counter() - t0
     N = w["NX"] * w["NY"] * w["NZ"]
-    return {"value": N * n / dt, "unit": "cell-steps/s", "cores": op.get_threads(), "kind": "port",
+    del O
+    return {"value": N * n / dt, "unit": "cell-steps/s", "cores": threads, "kind": kind, "cpu": cpu_model(),
             "sample": f"{n} SBDF step(s) of the full {w['NX']}x{w['NZ']}x{w['NY']} VV4 grid after 1 untimed step, "
-                      f"FP64, {op.get_threads()} OpenMP threads, {dt:.1f} s"}
+                      f"FP64, {what}, {threads} OpenMP threads, {dt:.1f} s"}
+
+
+def workload_config(w: dict, world: int) -> dict:
+    """The `config` object of both arms' lines (the same workload, whatever the precision)."""
+    return {"workload": f"staggered VV4 DNS {w['NX']}x{w['NZ']}x{w['NY']} (x, wall-normal, span) cells, "
+                        "Re_b 21900, 2pi x 2 x pi, tanh 2.2, dt 0.0008, constant flow rate",
+            "grid": [w["NX"], w["NY"], w["NZ"]], "cells": w["NX"] * w["NY"] * w["NZ"],
+            "parallelism": "replicas only" if world > 1 else "1 GPU",
+            "l2": "inputs larger than L2 (one field level 450 MB f32 / 900 MB f64)"}
+
+
+def reference_gpu(steps: int, warmup: int, device: int, precisions=("f64", "f32"), config="vv4_c4"):
+    """The reference's own GPU path (its data_cuda solver: lambda kernels, cuFFT, Thrust),
+    compiled from its sources into oracle/_ref, timed on this GPU by oracle/ref_gpu_time.py
+    in a child process (its own CUDA context; the reference exits on a CUDA error)."""
+    out = {}
+    script = os.path.join(ROOT, "oracle", "ref_gpu_time.py")
+    for prec in precisions:
+        try:
+            r = subprocess.run([sys.executable, script, "--config", config, "--precision", prec, "--steps",
+                                str(steps), "--warmup", str(warmup), "--device", str(device)],
+                               capture_output=True, text=True, timeout=600)
+            lines = [x for x in r.stdout.splitlines() if x.startswith("{")]
+            out[prec] = json.loads(lines[-1]) if lines else {"unavailable": f"no output (rc {r.returncode}): "
+                                                                            f"{(r.stdout + r.stderr)[-300:]}"}
+        except (subprocess.TimeoutExpired, OSError, ValueError) as e:
+            out[prec] = {"unavailable": f"{type(e).__name__}: {e}"[:300]}
+    return out
 
 
 def aggregate_value(world: int, cells: int, steps: int, ms_max: float) -> float:
@@ -295,9 +366,9 @@ class Dist:
 
 
 def run_reference(args, world, rank):
-    """Reference arm: the reference's own CPU path timed on the host cores.  The
-    reference cannot be compiled at 384 (its periodic index wrap needs powers of
-    two), so the CPU restatement of that path (the oracle) is timed."""
+    """Reference arm: the reference's own CPU path (its data_cpu solver, compiled from its
+    sources into oracle/_ref at 384 x 384 x 256) timed on all host cores; the oracle port
+    only where that build is absent."""
     if rank != 0:
         return
     w = dict(WORKLOAD)
@@ -307,8 +378,7 @@ def run_reference(args, world, rank):
     line = {"impl": "reference", "metric": METRIC, "value": base["value"], "unit": "cell-steps/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"staggered VV4 DNS {w['NX']}x{w['NZ']}x{w['NY']} (x, wall-normal, span), "
-                                   f"Re_b 21900, dt 0.0008, constant flow rate"},
+            "config": workload_config(w, world),
             "cpu_baseline": base, "e2e": {"value": base["value"], "unit": "cell-steps/s", "h2d_bytes_per_step": 0,
                                          "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -323,6 +393,8 @@ def main():
     ap.add_argument("--small", action="store_true", help="96x64x96 grid (quick check, not a bench number)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip timing the reference's own GPU path on this GPU")
     ap.add_argument("--only", choices=["mixed", "fp64"], help="time one precision only (profiling)")
     ap.add_argument("--grid", type=int, nargs=3, metavar=("NX", "NY", "NZ"),
                     help="override the grid (profiling runs; not a bench number)")
@@ -383,6 +455,14 @@ def main():
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         base = cpu_baseline(small=args.small)
+    ref_gpu = None
+    if rank == 0 and world == 1 and not args.no_reference_gpu and not args.small and not GRID:
+        ref_gpu = reference_gpu(args.steps, args.warmup, local)
+        for prec, ours in (("f64", fp64["ms_per_step"] if fp64 else None), ("f32", mixed["ms"] / args.steps)):
+            r = ref_gpu.get(prec, {})
+            if ours and "ms_per_step" in r:
+                # the reference's step time over ours (FP64 against FP64, its FP32 against our mixed form)
+                r["reference_ms_over_ours"] = round(r["ms_per_step"] / ours, 3)
 
     if rank == 0:
         w = WORKLOAD if not args.small else dict(WORKLOAD, NX=96, NY=96, NZ=64)
@@ -394,15 +474,14 @@ def main():
             "warmup": args.warmup, "ms_per_step": mixed["ms"] / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded MT19937-64 noise on the laminar profile, projected divergence-free)",
-            "config": {"workload": f"staggered VV4 DNS {w['NX']}x{w['NZ']}x{w['NY']} (x, wall-normal, span) cells, "
-                                   "Re_b 21900, 2pi x 2 x pi, tanh 2.2, dt 0.0008, constant flow rate, "
-                                   "mixed precision (f32 storage/stencils/FFT, f64 low-k solves, forcing, reductions)",
-                       "grid": [w["NX"], w["NY"], w["NZ"]], "cells": N, "parallelism": "replicas only" if world > 1 else "1 GPU",
-                       "l2": "inputs larger than L2 (one field level 450 MB f32 / 900 MB f64)"},
+            "config": workload_config(w, world),
+            "precision_form": "mixed: f32 storage/stencils/FFT, f64 low-k solves, forcing, reductions "
+                              "(the plain FP64 form under \"fp64\")",
             "roofline": roof, "step_roofline": step_roof, "phases_ms": per_phase,
             "cpu_baseline": base, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
             "fp64": fp64, "mixed_vs_fp64": (value / fp64["value"]) if fp64 else None,
             "bulk_velocity_after": ub_mixed,
+            "reference_gpu": ref_gpu,
         }
         print(json.dumps(line), flush=True)
     if dist_ctx:

@@ -140,7 +140,11 @@ int tc_set_turb_model(tc_handle* h, int kind, const void* weights);
 
 /* Diagnostics (FP64 accumulation), synchronous.
  * data::CalcIntegral / CalcKineticEnergy / CalcCFL / CalcProfiles
- * (staggered/func_global.h:678-808). */
+ * (staggered/func_global.h:678-808).  A NaN or Inf anywhere in the level's u, v, w,
+ * p or nu_t makes these calls (and tc_diagnostics) return TC_E_NUMERIC, with the
+ * outputs still written and the plane named in tc_last_error(); the reference reports
+ * nothing here (its only numeric signal is the -1e50 written for a singular pivot,
+ * staggered/func_global.h:169). */
 int tc_integral(tc_handle* h, int level, double out[3]);
 int tc_kinetic_energy(tc_handle* h, int level, double* out);
 int tc_cfl(tc_handle* h, int level, double tau, int mode, double* out);
@@ -205,8 +209,10 @@ int tc_get_nu_t(tc_handle* h, double* nu_t);
  * allocates nothing: the z-solve's elimination coefficients live in a static device
  * array of 32 MiB shared by all calls on a device, so the z-solve's
  * (NX/2+1)*NY*NZ*c*8 bytes (c = 3 for VV4, 1 otherwise) must fit (else TC_E_ARG),
- * and calls whose launches overlap in time race on it.  The first call on a device
- * looks the array up (and may load the module): make it before any stream capture. */
+ * and calls whose launches overlap in time race on it.  tc_create loads the module
+ * that holds the array on the handle's device, so its 32 MiB are taken from device
+ * memory when the handle is created (create handles before handing the rest of HBM
+ * to a pool); each call then only looks the array's address up. */
 int tc_op_pressure_solve_static(tc_handle* h, const void* rhs, void* p);
 
 /* Seeded channel initial field on level `level`: u = 1.5(1 - y^2) + noise, v, w =

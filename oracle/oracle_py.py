@@ -281,6 +281,9 @@ class RefLib:
         L.ref_get_mesh.argtypes = [C.c_char_p, _dp]
         L.ref_get_mesh.restype = C.c_int
         L.ref_set_threads.argtypes = [C.c_int]
+        if self.kind != 2:
+            L.ref_cfr_shift.argtypes = [C.c_int, C.c_double]
+            L.ref_project.argtypes = [C.c_int]
         self.NZ = None
 
     def setup(self, p: dict, zz: np.ndarray):
@@ -328,8 +331,16 @@ class RefLib:
         self.L.ref_get_nu_t(nt)
         return nt
 
-    def step(self, t, tau, cur, order):
+    def step(self, t, tau, cur, order, cfr=None):
+        """The reference's data::Step; with cfr, then the oracle driver's constant flow
+        rate shift of u (staggered builds only: ref_cfr_shift)."""
         self.L.ref_step(t, tau, cur, order)
+        if cfr is not None:
+            self.L.ref_cfr_shift((cur + 1) % 4, C.c_double(cfr))
+
+    def project(self, l):
+        """Level l made divergence-free with the reference's own operators (staggered)."""
+        self.L.ref_project(l)
 
     def _v2s(self, fn, v, n):
         out = np.zeros(n)

@@ -12,6 +12,9 @@
 #ifndef REF_DOUBLE
 #define REF_DOUBLE 1
 #endif
+#ifndef REF_GENERAL_WRAP
+#define REF_GENERAL_WRAP 0
+#endif
 #ifndef REF_GALERKIN
 #define REF_GALERKIN 1
 #endif
@@ -27,8 +30,12 @@
 #define ENABLE_TURB_VISC REF_GALERKIN
 #define VISC_TERM_GALERKIN REF_GALERKIN
 
+#if REF_GENERAL_WRAP
+#include "index_wrap.h" /* NX, NY of any size (sizes that are not powers of two) */
+#else
 #define NX REF_NX
 #define NY REF_NY
+#endif
 #define NZ_MAX REF_NZMAX
 
 #define BLK_1D 256

@@ -15,6 +15,9 @@
 #ifndef REF_DOUBLE
 #define REF_DOUBLE 1
 #endif
+#ifndef REF_GENERAL_WRAP
+#define REF_GENERAL_WRAP 0
+#endif
 #ifndef REF_TURB
 #define REF_TURB 0
 #endif
@@ -39,8 +42,12 @@ enum struct tViscApproximation { CROSS, NAIVE, GALERKIN };
 #define CONV_VV 1
 #define CONV_APPR_TYPE REF_CONV
 
+#if REF_GENERAL_WRAP
+#include "index_wrap.h" /* NX, NY of any size (sizes that are not powers of two) */
+#else
 #define NX REF_NX
 #define NY REF_NY
+#endif
 #define NXY (NX * NY)
 #define NZ_MAX REF_NZMAX
 

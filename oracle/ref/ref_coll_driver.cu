@@ -144,4 +144,141 @@ void ref_profiles(int l, double* out) {
         o[9] = a.nu_t; o[10] = 0.; o[11] = 0.;
     }
 }
+
+/* ---------------------------------------------------------------------------
+ * The reference's own GPU solver (data_cuda::data of collocated_AB3/main.cpp:114-178:
+ * lambda Forall kernels, the shared-memory flux kernel, cuFFT, Thrust), set up as
+ * collocated_AB3/main.cpp:264-300 does and stepped as its time loop does
+ * (main.cpp:405-440).  Used to time the reference's GPU path on the same device as
+ * the product; the CPU object's field buffers are not allocated here.
+ * ------------------------------------------------------------------------- */
+static data_cuda::data G;
+static int g_gpu_ready = 0;
+
+__global__ void refgpu_subtract(real3* v, const real3* g, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) v[i] -= g[i];
+}
+
+int refgpu_setup_colloc(int nz, const double* zz, double visc, double sour_dpdx, double inv_ls, double hx, double hy,
+                        double area, int turb, int stab_type, int fd_mode, int device) {
+    if (nz > NZ_MAX || nz < 4 || g_gpu_ready) return 1;
+    if (cudaSetDevice(device) != cudaSuccess) return 2;
+    for (int i = 0; i < nz; i++) data_cpu::ZZ[i] = zz[i];
+    for (int i = 0; i < nz - 1; i++) data_cpu::DZ[i] = data_cpu::ZZ[i + 1] - data_cpu::ZZ[i];
+    main_params& MD = D;
+    MD.StabType = stab_type;
+    MD.visc = visc;
+    MD.sour_dpdx = sour_dpdx;
+    MD.inv_length_scale = inv_ls;
+    MD.EnableTurbVisc = turb;
+    MD.NZ = nz;
+    MD.N3D = NX * NY * nz;
+    MD.hx = hx;
+    MD.hy = hy;
+    MD.inv_hx = 1. / MD.hx;
+    MD.inv_hy = 1. / MD.hy;
+    MD.area = area;
+    MD.xmin = 0.;
+    MD.ymin = 0.;
+    MD.FDmode = fd_mode;
+    *(static_cast<main_params*>(&G)) = *(static_cast<main_params*>(&D));
+    G.alloc_all();
+    cudaMemcpyToSymbol(data_cuda::D, &G, sizeof(data_cuda::data));
+    G.InitFourier();
+    cudaMemcpyToSymbol(data_cuda::D, &G, sizeof(data_cuda::data));
+    cudaMemcpyToSymbol(data_cuda::DZ, data_cpu::DZ, sizeof(double) * nz);
+    cudaMemcpyToSymbol(data_cuda::ZZ, data_cpu::ZZ, sizeof(double) * nz);
+    double* A = data_cpu::MAT_A;
+    A[0] = 0.;
+    for (int j = 1; j < nz; j++) A[j] = D.hx * D.hy / data_cpu::DZ[j - 1];
+    if (D.FDmode) { A[1] *= 0.5; A[nz - 1] *= 0.5; }
+    cudaMemcpyToSymbol(data_cuda::MAT_A, data_cpu::MAT_A, sizeof(double) * nz);
+    for (int l = 0; l < 4; l++) {
+        cudaMemset((void*)G.vel[l], 0, sizeof(real3) * D.N3D);
+        cudaMemset((void*)G.flux[l], 0, sizeof(real3) * D.N3D);
+        cudaMemset((void*)G.pres[l], 0, sizeof(real) * D.N3D);
+    }
+    cudaMemset((void*)G.divv, 0, sizeof(real) * D.N3D);
+    if (G.nu_t) cudaMemset((void*)G.nu_t, 0, sizeof(real) * D.N3D);
+    g_gpu_ready = cudaDeviceSynchronize() == cudaSuccess;
+    return g_gpu_ready ? 0 : 3;
+}
+
+int refgpu_set_level(int l, const double* vel, const double* p) {
+    if (!g_gpu_ready) return 1;
+    std::vector<real3> a(vel ? D.N3D : 0);
+    std::vector<real> b(p ? D.N3D : 0);
+    if (vel) { put3(a.data(), vel); cudaMemcpy(G.vel[l], a.data(), sizeof(real3) * D.N3D, cudaMemcpyHostToDevice); }
+    if (p) { put1(b.data(), p); cudaMemcpy(G.pres[l], b.data(), sizeof(real) * D.N3D, cudaMemcpyHostToDevice); }
+    return cudaDeviceSynchronize() == cudaSuccess ? 0 : 2;
+}
+int refgpu_get_level(int l, double* vel, double* p) {
+    if (!g_gpu_ready) return 1;
+    std::vector<real3> a(vel ? D.N3D : 0);
+    std::vector<real> b(p ? D.N3D : 0);
+    if (vel) { cudaMemcpy(a.data(), G.vel[l], sizeof(real3) * D.N3D, cudaMemcpyDeviceToHost); get3(vel, a.data()); }
+    if (p) { cudaMemcpy(b.data(), G.pres[l], sizeof(real) * D.N3D, cudaMemcpyDeviceToHost); get1(p, b.data()); }
+    return cudaDeviceSynchronize() == cudaSuccess ? 0 : 2;
+}
+
+/* v -= grad(L^-1 div v) with the GPU object's own operators (flux[(l+1)%4] is the
+ * scratch gradient). */
+int refgpu_project(int l) {
+    if (!g_gpu_ready) return 1;
+    real3* g = G.flux[(l + 1) % 4];
+    G.UnapplyGradient(G.vel[l], G.pres[l]);
+    G.ApplyGradient(G.pres[l], g);
+    refgpu_subtract<<<(D.N3D + 255) / 256, 256>>>(G.vel[l], g, D.N3D);
+    cudaMemset((void*)G.pres[l], 0, sizeof(real) * D.N3D);
+    return cudaDeviceSynchronize() == cudaSuccess ? 0 : 2;
+}
+
+/* `nsteps` steps of the reference's time loop (order ramped as main.cpp:409 does),
+ * timed with CUDA events on the default stream; with_diag adds the loop's per-step
+ * CalcIntegral, CalcVelocityProfile (+ the av_u copy) and CalcCFL (main.cpp:414-439). */
+double refgpu_run(int nsteps, double tau, int with_diag, int* cur, int* it) {
+    if (!g_gpu_ready) return -1.0;
+    std::vector<real9> prof(D.NZ);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaDeviceSynchronize();
+    cudaEventRecord(e0, 0);
+    for (int s = 0; s < nsteps; s++) {
+        const int order = *it + 1 < 3 ? *it + 1 : 3;
+        G.Step(*it * tau, tau, *cur, order);
+        *cur = (*cur + 1) % 4;
+        *it += 1;
+        if (with_diag) {
+            volatile double fr = G.CalcIntegral(G.vel[*cur])[0];
+            (void)fr;
+            G.CalcVelocityProfile(G.vel[*cur]);
+            cudaMemcpy(prof.data(), G.av_u, sizeof(real9) * D.NZ, cudaMemcpyDeviceToHost);
+            volatile double cfl = G.CalcCFL(G.vel[*cur], (real)tau, 3);
+            (void)cfl;
+        }
+    }
+    cudaEventRecord(e1, 0);
+    cudaEventSynchronize(e1);
+    float ms = -1.f;
+    const cudaError_t err = cudaGetLastError();
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return err == cudaSuccess ? (double)ms : -1.0;
+}
+
+int refgpu_integral(int l, double* out) {
+    if (!g_gpu_ready) return 1;
+    real3 r = G.CalcIntegral(G.vel[l]);
+    for (int c = 0; c < 3; c++) out[c] = r[c];
+    return 0;
+}
+
+void refgpu_free(void) {
+    if (!g_gpu_ready) return;
+    G.dealloc_all();
+    g_gpu_ready = 0;
+}
 }

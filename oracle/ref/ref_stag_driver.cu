@@ -150,4 +150,161 @@ void ref_profiles(int l, double* out) {
         o[9] = a.nu_t; o[10] = a.p; o[11] = a.pp;
     }
 }
+
+/* ---------------------------------------------------------------------------
+ * The reference's own GPU solver, data_cuda::data of staggered/func_cuda.cpp
+ * (lambda Forall kernels, cuFFT D2Z/Z2D, Thrust reductions), set up as
+ * staggered/main.cpp:209-262 does (the CPU object holds the parameters and mesh
+ * data; the GPU object gets a copy of them, its own buffers and the constant-memory
+ * image), and stepped as its time loop does (main.cpp:306-340).  Used to time the
+ * reference's GPU path on the same device as the product.  The GPU object holds
+ * device buffers only; the CPU object's field buffers are not allocated here.
+ * ------------------------------------------------------------------------- */
+extern "C++" void CopyDataToDevice(const data_cuda::data&);  // staggered/func_cuda.cpp
+static data_cuda::data G;
+static int g_gpu_ready = 0;
+
+__global__ void refgpu_subtract(real3* v, const real3* g, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) v[i] -= g[i];
+}
+
+int refgpu_setup(int nz, const double* zz, double visc, double sour_dpdx, double inv_ls, double hx, double hy,
+                 double area, int device) {
+    if (nz > NZ_MAX || nz < 6 || g_gpu_ready) return 1;
+    if (cudaSetDevice(device) != cudaSuccess) return 2;
+    D.NZ = nz;
+    D.N3D = NX * NY * nz;
+    D.visc = visc;
+    D.sour_dpdx = sour_dpdx;
+    D.inv_length_scale = inv_ls;
+    D.hx = hx;
+    D.hy = hy;
+    D.inv_hx = 1. / D.hx;
+    D.inv_hy = 1. / D.hy;
+    D.area = area;
+    D.xmin = 0.;
+    D.ymin = 0.;
+    for (int i = 0; i <= nz; i++) D.ZZ[i] = zz[i];
+    D.InitDerivativeMeshData();
+    *(static_cast<main_params*>(&G)) = *(static_cast<main_params*>(&D));
+    G.alloc_all();
+    CopyDataToDevice(G);
+    G.InitFourier();
+    for (int l = 0; l < 4; l++) {
+        cudaMemset((void*)G.vel[l], 0, sizeof(real3) * D.N3D);
+        cudaMemset((void*)G.flux[l], 0, sizeof(real3) * D.N3D);
+        cudaMemset((void*)G.pres[l], 0, sizeof(real) * D.N3D);
+    }
+    cudaMemset((void*)G.divv, 0, sizeof(real) * D.N3D);
+    if (G.nu_t) cudaMemset((void*)G.nu_t, 0, sizeof(real) * D.N3D);
+    g_gpu_ready = cudaDeviceSynchronize() == cudaSuccess;
+    return g_gpu_ready ? 0 : 3;
+}
+
+/* Host AoS double <-> the GPU object's level `l` (real3 / real in `real`). */
+int refgpu_set_level(int l, const double* vel, const double* p) {
+    if (!g_gpu_ready) return 1;
+    std::vector<real3> a(vel ? D.N3D : 0);
+    std::vector<real> b(p ? D.N3D : 0);
+    if (vel) { put3(a.data(), vel); cudaMemcpy(G.vel[l], a.data(), sizeof(real3) * D.N3D, cudaMemcpyHostToDevice); }
+    if (p) { put1(b.data(), p); cudaMemcpy(G.pres[l], b.data(), sizeof(real) * D.N3D, cudaMemcpyHostToDevice); }
+    return cudaDeviceSynchronize() == cudaSuccess ? 0 : 2;
+}
+int refgpu_get_level(int l, double* vel, double* p) {
+    if (!g_gpu_ready) return 1;
+    std::vector<real3> a(vel ? D.N3D : 0);
+    std::vector<real> b(p ? D.N3D : 0);
+    if (vel) { cudaMemcpy(a.data(), G.vel[l], sizeof(real3) * D.N3D, cudaMemcpyDeviceToHost); get3(vel, a.data()); }
+    if (p) { cudaMemcpy(b.data(), G.pres[l], sizeof(real) * D.N3D, cudaMemcpyDeviceToHost); get1(p, b.data()); }
+    return cudaDeviceSynchronize() == cudaSuccess ? 0 : 2;
+}
+
+/* Project level `l` divergence-free with the GPU object's own operators, as
+ * staggered/selftest.cpp:224-226 does: v -= grad(L^-1 div v) (flux[(l+1)%4] is the
+ * scratch gradient). */
+int refgpu_project(int l) {
+    if (!g_gpu_ready) return 1;
+    real3* g = G.flux[(l + 1) % 4];
+    G.UnapplyGradient(G.vel[l], G.pres[l]);
+    G.ApplyGradient(G.pres[l], g);
+    refgpu_subtract<<<(D.N3D + 255) / 256, 256>>>(G.vel[l], g, D.N3D);
+    cudaMemset((void*)G.pres[l], 0, sizeof(real) * D.N3D);
+    return cudaDeviceSynchronize() == cudaSuccess ? 0 : 2;
+}
+
+/* `nsteps` steps of the reference's time loop from ring level *cur (order ramped
+ * from *it as main.cpp:308 does), timed with CUDA events on the default stream that
+ * the reference launches on.  with_diag != 0 adds the loop's per-step diagnostics
+ * (CalcIntegral, CalcProfiles + the av_u device->host copy, CalcCFL:
+ * main.cpp:313-338).  Returns the elapsed milliseconds, or a negative value on a
+ * CUDA error. */
+double refgpu_run(int nsteps, double tau, int with_diag, int* cur, int* it) {
+    if (!g_gpu_ready) return -1.0;
+    std::vector<real9<real>> prof(D.NZ);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaDeviceSynchronize();
+    cudaEventRecord(e0, 0);
+    for (int s = 0; s < nsteps; s++) {
+        const int order = *it + 1 < 3 ? *it + 1 : 3;
+        G.Step(*it * tau, tau, *cur, order);
+        *cur = (*cur + 1) % 4;
+        *it += 1;
+        if (with_diag) {
+            volatile real3 fr = G.CalcIntegral(G.vel[*cur]);
+            (void)fr;
+            G.CalcProfiles(G.vel[*cur], G.pres[*cur]);
+            cudaMemcpy(prof.data(), G.av_u, sizeof(real9<real>) * D.NZ, cudaMemcpyDeviceToHost);
+            volatile real cfl = G.CalcCFL(G.vel[*cur], (real)tau, 3);
+            (void)cfl;
+        }
+    }
+    cudaEventRecord(e1, 0);
+    cudaEventSynchronize(e1);
+    float ms = -1.f;
+    const cudaError_t err = cudaGetLastError();
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return err == cudaSuccess ? (double)ms : -1.0;
+}
+
+int refgpu_integral(int l, double* out) {
+    if (!g_gpu_ready) return 1;
+    real3 r = G.CalcIntegral(G.vel[l]);
+    for (int c = 0; c < 3; c++) out[c] = r[c];
+    return 0;
+}
+
+void refgpu_free(void) {
+    if (!g_gpu_ready) return;
+    G.dealloc_all();
+    g_gpu_ready = 0;
+}
+
+/* Project level `l` of the CPU object divergence-free with the reference's own
+ * operators (staggered/selftest.cpp:224-226; flux[(l+1)%4] is the scratch gradient). */
+void ref_project(int l) {
+    real3* g = D.flux[(l + 1) % 4];
+    D.UnapplyGradient(D.vel[l], D.pres[l]);
+    D.ApplyGradient(D.pres[l], g);
+    real3* v = D.vel[l];
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < D.N3D; i++) v[i] -= g[i];
+    memset((void*)D.pres[l], 0, sizeof(real) * D.N3D);
+    memset((void*)g, 0, sizeof(real3) * D.N3D);
+}
+
+/* Constant flow rate for the reference's CPU object, as the oracle's driver applies
+ * it after each step (shift u uniformly so that the bulk velocity is `target`;
+ * the reference itself forces with a constant sour_dpdx). */
+void ref_cfr_shift(int l, double target) {
+    const real3 I = D.CalcIntegral(D.vel[l]);
+    const real du = (real)((target - I[0] / D.area));
+    real3* v = D.vel[l];
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < D.N3D; i++) v[i][0] += du;
+}
 }

@@ -408,3 +408,40 @@ def test_full_size_configurations_match_oracle(name, precision):
     assert rel_err(vs, vo) < tol, rel_err(vs, vo)
     assert rel_err(ps, po) < 20 * tol, rel_err(ps, po)
     S.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("name", ["vv4_dns", "hw2_les", "coll_cross"])
+def test_diagnostics_report_non_finite_values(name, precision):
+    """A NaN or Inf in a level makes the diagnostics return TC_E_NUMERIC (host-made
+    fields only: the bad value is planted on the host, nothing faults on the device)."""
+    import ctypes as C
+
+    import turbchannel_b200 as tb
+
+    prod, _, zz = make_case(precision=precision, **CASES[name])
+    S = tb.Solver(prod, zz)
+    NXY = S.NX * S.NY
+    coll = CASES[name]["scheme"] == COLLOC
+    v = seeded_field(S.N, NXY, seed=9, amp=0.1, wall_w_zero=not coll)
+    p = np.random.default_rng(10).standard_normal(S.N)
+    S.upload_level(0, v, p)
+    S.CalcIntegral(0)  # a finite level passes
+    cells = [(S.N // 2 + 3, 0, np.nan), (NXY + 5, 2, np.inf), (S.N - 7, 1, -np.inf)]
+    for cell, comp, bad in cells:
+        vb = v.copy()
+        vb[cell, comp] = bad
+        S.upload_level(1, vb, p)
+        out3 = (C.c_double * 3)()
+        d = C.c_double(0)
+        assert S.L.tc_integral(S.h, 1, out3) == -4, (cell, comp)
+        assert b"non-finite" in S.L.tc_last_error()
+        assert S.L.tc_kinetic_energy(S.h, 1, C.byref(d)) == -4
+        assert S.L.tc_cfl(S.h, 1, C.c_double(1e-3), 3, C.byref(d)) == -4
+    pb = p.copy()
+    pb[S.N // 3] = np.nan
+    S.upload_level(2, v, pb)
+    prof = np.zeros(S.NZ * 12)
+    assert S.L.tc_profiles(S.h, 2, prof.ctypes.data_as(C.c_void_p)) == -4
+    assert b"sum p" in S.L.tc_last_error()
+    S.close()

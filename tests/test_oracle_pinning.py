@@ -56,8 +56,10 @@ def test_oracle_matches_reference_golden(path):
         assert rel_err(got, d[name]) < tol, name
 
 
+# The *_w48 / *_w36 variants are built with the index-wrap generalisation
+# (oracle/ref/index_wrap.h) at sizes that are not powers of two (48 x 24, 36 x 18).
 REF_VARIANTS = ["stag_hw2_dns_f64", "stag_hw2_les_f64", "stag_vv4_dns_f64", "stag_vv4_les_f64", "coll_gal_f64",
-                "coll_cross_f64", "stag_vv4_les_f32", "coll_gal_f32"]
+                "coll_cross_f64", "stag_vv4_les_f32", "coll_gal_f32", "stag_vv4_dns_w48_f64", "stag_hw2_les_w36_f64"]
 
 
 @pytest.mark.parametrize("variant", REF_VARIANTS)

@@ -352,12 +352,12 @@ void launch_divergence(const DivArgs<T>& a, cudaStream_t s) {
 
 // ---------------------------------------------------------------------------
 // Per-plane diagnostics in double: one CTA per z-plane.
-// planes[z*16 + k]: 0..2 sum u, v, w_c; 3..8 sum uu, vv, w_cw_c, uv, uw_c, vw_c;
-// 9 sum nu_t; 10 sum p; 11 sum pp; 12 sum w (raw); 13 sum w^2 (raw);
-// 14..15 max CFL convective / viscous part; 16.. unused.  (CalcProfiles,
+// planes[z*TC_DIAG_STRIDE + k]: 0..2 sum u, v, w_c; 3..8 sum uu, vv, w_cw_c, uv, uw_c,
+// vw_c; 9 sum nu_t; 10 sum p; 11 sum pp; 12 sum w (raw); 13 sum w^2 (raw); 14..15
+// unused (0); 16..18 max CFL convective / viscous / both.  (CalcProfiles,
 // CalcIntegral, CalcKineticEnergy, CalcCFL: staggered/func_global.h:678-808.)
 // ---------------------------------------------------------------------------
-constexpr int NDIAG = 16;
+constexpr int NDIAG = NDIAG_SUMS;
 static_assert(NDIAG + 3 == TC_DIAG_STRIDE, "diagnostics layout");
 
 // Stage 1: CTA (z, s) reduces chunk s of plane z into part[(z*S + s)*STRIDE + k];

@@ -152,6 +152,7 @@ struct DiagArgs {
     double* part;    // NZ x diag_chunks() x TC_DIAG_STRIDE partial sums
 };
 constexpr int TC_DIAG_STRIDE = 19;
+constexpr int NDIAG_SUMS = 16;  // planes[z][0..15] are sums, [16..18] CFL maxima
 
 template <typename T> void launch_flux_stag(const FluxArgs<T>& a, cudaStream_t s);
 template <typename T> void launch_flux_coll(const FluxArgs<T>& a, cudaStream_t s);

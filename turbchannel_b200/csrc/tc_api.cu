@@ -403,6 +403,8 @@ static void fill_flux_pair_consts(const Geom& g, const HostMesh& hm, std::vector
     }
 }
 
+static int static_zscr(void** out);
+
 extern "C" int tc_create(const tc_params* prm, const double* zz, tc_handle** out) {
     if (!prm || !zz || !out) return fail(TC_E_ARG, "tc_create: null argument");
     *out = nullptr;
@@ -458,6 +460,17 @@ extern "C" int tc_create(const tc_params* prm, const double* zz, tc_handle** out
         free_all(h);
         delete h;
         return fail(TC_E_CUDA, "tc_create: stream creation failed");
+    }
+    {
+        // loads the module holding tc_op_pressure_solve_static's scratch array on this
+        // device now, so that array's memory is reserved before the caller's own pools
+        void* scr = nullptr;
+        if (static_zscr(&scr)) {
+            const std::string msg = "tc_create: " + g_err;
+            free_all(h);
+            delete h;
+            return fail(TC_E_CUDA, msg);
+        }
     }
     if ((long long)3 * g.N >= 4294967296LL) {
         free_all(h);
@@ -1039,6 +1052,23 @@ static void reduce_planes(const tc_handle* h, double integral[3], double* ke, do
     }
 }
 
+// The plane sums of the diagnostics pass add every u, v, w, p (and nu_t) of the level,
+// so a NaN or Inf anywhere in it makes one of them non-finite (the CFL maxima use fmax,
+// which skips NaN, so they are not enough).  The outputs are still written.
+static int check_planes_finite(const tc_handle* h, const char* who) {
+    static const char* const names[NDIAG_SUMS] = {"sum u", "sum v", "sum w", "sum uu", "sum vv", "sum ww",
+                                                  "sum uv", "sum uw", "sum vw", "sum nu_t", "sum p", "sum pp",
+                                                  "sum w (raw)", "sum ww (raw)", "", ""};
+    for (int z = 0; z < h->g.NZ; z++) {
+        const double* s = h->planes_h + (size_t)z * TC_DIAG_STRIDE;
+        for (int k = 0; k < NDIAG_SUMS; k++)
+            if (!std::isfinite(s[k]))
+                return fail(TC_E_NUMERIC, std::string(who) + ": non-finite value in the level (plane z = " +
+                                              std::to_string(z) + ", " + names[k] + " = " + std::to_string(s[k]) + ")");
+    }
+    return TC_OK;
+}
+
 extern "C" int tc_diagnostics(tc_handle* h, int level, double tau, double integral[3], double* cfl, double* profiles) {
     if (!h || level < 0 || level > 3) return fail(TC_E_ARG, "tc_diagnostics: bad handle or level");
     cudaSetDevice(h->prm.device);
@@ -1047,7 +1077,7 @@ extern "C" int tc_diagnostics(tc_handle* h, int level, double tau, double integr
     double c[3];
     reduce_planes(h, integral, nullptr, c, profiles);
     if (cfl) *cfl = c[2];
-    return TC_OK;
+    return check_planes_finite(h, "tc_diagnostics");
 }
 extern "C" int tc_integral(tc_handle* h, int level, double out[3]) {
     return tc_diagnostics(h, level, 0.0, out, nullptr, nullptr);
@@ -1058,7 +1088,7 @@ extern "C" int tc_kinetic_energy(tc_handle* h, int level, double* out) {
     int rc = TC_DISPATCH(h, diag_run, h, level, 0.0);
     if (rc) return rc;
     reduce_planes(h, nullptr, out, nullptr, nullptr);
-    return TC_OK;
+    return check_planes_finite(h, "tc_kinetic_energy");
 }
 extern "C" int tc_cfl(tc_handle* h, int level, double tau, int mode, double* out) {
     if (!h || !out || level < 0 || level > 3 || mode < 1 || mode > 3) return fail(TC_E_ARG, "tc_cfl: bad argument");
@@ -1068,7 +1098,7 @@ extern "C" int tc_cfl(tc_handle* h, int level, double tau, int mode, double* out
     double c[3];
     reduce_planes(h, nullptr, nullptr, c, nullptr);
     *out = c[mode - 1];
-    return TC_OK;
+    return check_planes_finite(h, "tc_cfl");
 }
 extern "C" int tc_profiles(tc_handle* h, int level, double* out) {
     if (!out) return fail(TC_E_ARG, "tc_profiles: null output");
@@ -1478,9 +1508,13 @@ extern "C" int tc_init_channel(tc_handle* h, int level, unsigned long long seed,
 // precomputed at creation instead); that elimination's coefficients live in a
 // file-scope static device array (below), not in a buffer of the handle.
 //
-// * Setup: the first call on a device looks the array up with cudaGetSymbolAddress
-//   (which may load this module into the context), so it should come before any
-//   stream capture; later calls on that device only read the cached address.
+// * Setup: tc_create looks the array up with cudaGetSymbolAddress on the handle's
+//   device.  With CUDA's lazy module loading that lookup is what loads this module into
+//   the context, and loading it is what gives the 32 MiB array its device memory, so
+//   the array is reserved when the handle is created, not inside the first
+//   tc_op_pressure_solve_static call: create the handle before a caller's pool takes
+//   the remaining HBM.  Every call looks the address up again (cheap once the module is
+//   loaded), so no address outlives a context (e.g. after cudaDeviceReset).
 // * Size limit: the z-solve needs (NX/2+1)*NY*NZ*c*8 bytes (c = 3 for VV4, 1
 //   otherwise); problems above TC_STATIC_ZSCR_BYTES (32 MiB) are rejected with
 //   TC_E_ARG.
@@ -1493,21 +1527,13 @@ extern "C" int tc_init_channel(tc_handle* h, int level, unsigned long long seed,
 static constexpr size_t TC_STATIC_ZSCR_BYTES = (size_t)32 << 20;
 static __device__ __align__(256) unsigned char g_static_zscr[TC_STATIC_ZSCR_BYTES];
 
-static std::mutex g_static_mu;
-static void* g_static_zscr_ptr[64] = {};
-
-// Address of g_static_zscr on device `dev` (which must be current).
-static int static_zscr(int dev, void** out) {
-    if (dev < 0 || dev >= 64) return fail(TC_E_ARG, "static z-solve scratch: device index out of range");
-    std::lock_guard<std::mutex> lk(g_static_mu);
-    if (!g_static_zscr_ptr[dev]) {
-        void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_static_zscr);
-        if (e != cudaSuccess || !p)
-            return fail(TC_E_CUDA, std::string("cudaGetSymbolAddress(static z-solve scratch): ") + cudaGetErrorString(e));
-        g_static_zscr_ptr[dev] = p;
-    }
-    *out = g_static_zscr_ptr[dev];
+// Address of g_static_zscr on the current device.
+static int static_zscr(void** out) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_static_zscr);
+    if (e != cudaSuccess || !p)
+        return fail(TC_E_CUDA, std::string("cudaGetSymbolAddress(static z-solve scratch): ") + cudaGetErrorString(e));
+    *out = p;
     return TC_OK;
 }
 
@@ -1544,7 +1570,7 @@ extern "C" int tc_op_pressure_solve_static(tc_handle* h, const void* rhs, void* 
                                   "static array's " + std::to_string(TC_STATIC_ZSCR_BYTES) + " bytes");
     TC_CUDA(cudaSetDevice(h->prm.device));
     void* scr = nullptr;
-    const int rc = static_zscr(h->prm.device, &scr);
+    const int rc = static_zscr(&scr);
     if (rc) return rc;
     return TC_DISPATCH(h, poisson_static, h, rhs, p, scr);
 }
