@@ -2,7 +2,7 @@
 // SiLU, softplus) with BF16 weights and activations on the tensor cores
 // (mma.sync m16n8k16, FP32 accumulation).  One warp evaluates a tile of 16 samples.
 //
-// Arithmetic (the CPU oracle oracle/mlp_oracle.py restates it, roundings included):
+// Arithmetic (the CPU oracle oracle/les_oracle.py restates it, roundings included):
 //   xb = bf16(x)                       x: 6 features, padded with zeros to 16
 //   z1 = W1^T xb + b1,  h1 = silu(z1),  h1b = bf16(h1)
 //   z2 = W2^T h1b + b2, h2 = silu(z2),  h2b = bf16(h2)
