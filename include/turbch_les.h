@@ -60,6 +60,13 @@ int tc_mlp_grad(tc_mlp* m, const float* features, const float* targets, long lon
 /* out[n] = nu_t / nu for n feature rows. */
 int tc_mlp_forward(tc_mlp* m, const float* features, long long n, float* out);
 
+/* Where a run with TC_TURB_MLP on a staggered grid evaluates the closure (no counterpart
+ * in the reference, whose Smagorinsky nu_t is a separate pass, staggered/func_global.h:
+ * 875-890).  mode 0 (default): a separate pass writes nu_t, the flux kernel reads it;
+ * 1: the flux kernel evaluates the network itself for the planes it stages (tile plus a
+ * one-cell halo) and also writes nu_t.  Both give the same nu_t and step. */
+int tc_set_mlp_fusion(tc_handle* h, int mode);
+
 #ifdef __cplusplus
 }
 #endif

@@ -37,3 +37,16 @@ def seeded_field(N, NXY, seed=7, amp=1.0, wall_w_zero=True):
     if wall_w_zero:
         v[:NXY, 2] = 0.0
     return v
+
+
+def within(label, err, tol):
+    """err < tol as a test check; with TC_ERROR_LOG set, also appends the measured error
+    (label, err, tol) to that file as a JSON line (how the tolerances were sized)."""
+    import json
+    import os
+
+    path = os.environ.get("TC_ERROR_LOG")
+    if path:
+        with open(path, "a") as f:
+            f.write(json.dumps({"label": label, "err": float(err), "tol": float(tol)}) + "\n")
+    return err < tol

@@ -11,7 +11,7 @@ Tolerances (relative to the max-norm of the oracle result):
 import numpy as np
 import pytest
 
-from cases import COLLOC, HW2, VV4, make_case, rel_err, seeded_field
+from cases import COLLOC, HW2, VV4, make_case, rel_err, seeded_field, within
 
 pytestmark = pytest.mark.gpu
 
@@ -57,12 +57,13 @@ def test_operators(name, precision):
         nt = 1e-3 * np.abs(np.random.default_rng(5).standard_normal(S.N))
         S.set_nu_t(nt)
         O.set_nu_t(nt)
-    assert rel_err(S.ExplicitTerm(v), O.explicit_term(v)) < tol * 10
-    assert rel_err(S.ApplyGradient(p), O.apply_gradient(p)) < tol
-    assert rel_err(S.ApplyDivergence(v), O.apply_divergence(v)) < tol
-    assert rel_err(S.UnapplyGradient(v), O.unapply_gradient(v)) < tol * 10
+    L = f"op/{name}/p{precision}"
+    assert within(L + "/explicit", rel_err(S.ExplicitTerm(v), O.explicit_term(v)), tol * 10)
+    assert within(L + "/grad", rel_err(S.ApplyGradient(p), O.apply_gradient(p)), tol)
+    assert within(L + "/div", rel_err(S.ApplyDivergence(v), O.apply_divergence(v)), tol)
+    assert within(L + "/unapply", rel_err(S.UnapplyGradient(v), O.unapply_gradient(v)), tol * 10)
     rhs = O.apply_divergence(v)
-    assert rel_err(S.LinearSystemSolveFFT(rhs), O.pressure_solve(rhs)) < tol * 10
+    assert within(L + "/psolve", rel_err(S.LinearSystemSolveFFT(rhs), O.pressure_solve(rhs)), tol * 10)
     if CASES[name].get("turb"):
         vs = 0.3 * seeded_field(S.N, NXY, seed=9, wall_w_zero=not coll)
         got = S.RecalcTurbVisc(vs)
@@ -70,7 +71,7 @@ def test_operators(name, precision):
         want = O.get_nu_t()
         if coll:  # elements of the top node plane are not defined
             got, want = got[:-NXY], want[:-NXY]
-        assert rel_err(got, want) < tol * 10
+        assert within(L + "/nu_t", rel_err(got, want), tol * 10)
 
 
 def _run_steps(S, O, nsteps, tau, cfr=None):
@@ -98,17 +99,18 @@ def test_steps(name, precision):
     cur = _run_steps(S, O, 6, tau)
     vs, ps = S.download_level(cur)
     vo, po = O.get_level(cur)
-    assert rel_err(vs, vo) < tol
-    assert rel_err(ps, po) < tol * 20
+    L = f"step/{name}/p{precision}"
+    assert within(L + "/vel", rel_err(vs, vo), tol)
+    assert within(L + "/pres", rel_err(ps, po), tol * 20)
     # flux history used by the next step
     for lvl in range(4):
-        assert rel_err(S.download_flux(lvl), O.get_flux(lvl)) < tol * 20
+        assert within(L + "/flux", rel_err(S.download_flux(lvl), O.get_flux(lvl)), tol * 20)
     # diagnostics
     I, cfl, prof = S.diagnostics(cur, tau)
-    assert rel_err(I, O.integral(cur)) < tol * 10
-    assert abs(cfl - O.cfl(cur, tau)) / O.cfl(cur, tau) < tol * 10
-    assert rel_err(prof, O.profiles(cur)) < tol * 10
-    assert abs(S.CalcKineticEnergy(cur) - O.kinetic_energy(cur)) / O.kinetic_energy(cur) < tol * 10
+    assert within(L + "/integral", rel_err(I, O.integral(cur)), tol * 10)
+    assert within(L + "/cfl", abs(cfl - O.cfl(cur, tau)) / O.cfl(cur, tau), tol * 10)
+    assert within(L + "/profiles", rel_err(prof, O.profiles(cur)), tol * 10)
+    assert within(L + "/ke", abs(S.CalcKineticEnergy(cur) - O.kinetic_energy(cur)) / O.kinetic_energy(cur), tol * 10)
 
 
 @pytest.mark.parametrize("name", ["hw2_dns", "vv4_les", "coll_gal_stab1"])
@@ -360,9 +362,10 @@ def test_config1_hundred_steps_match_oracle(precision):
     vs, ps = S.download_level(cur)
     vo, po = O.get_level(cur)
     tv, tp = (1e-9, 1e-9) if precision == 0 else (2e-3, 5e-2)
-    assert rel_err(vs, vo) < tv, rel_err(vs, vo)
-    assert rel_err(ps, po) < tp, rel_err(ps, po)
-    assert abs(S.CalcKineticEnergy(cur) - O.kinetic_energy(cur)) <= tv * O.kinetic_energy(cur)
+    L = f"config1/p{precision}"
+    assert within(L + "/vel", rel_err(vs, vo), tv), rel_err(vs, vo)
+    assert within(L + "/pres", rel_err(ps, po), tp), rel_err(ps, po)
+    assert within(L + "/ke", abs(S.CalcKineticEnergy(cur) - O.kinetic_energy(cur)) / O.kinetic_energy(cur), tv)
     S.close()
 
 
@@ -405,8 +408,9 @@ def test_full_size_configurations_match_oracle(name, precision):
     tol = TOL[precision]["step"]
     vs, ps = S.download_level(cur)
     vo, po = O.get_level(cur)
-    assert rel_err(vs, vo) < tol, rel_err(vs, vo)
-    assert rel_err(ps, po) < 20 * tol, rel_err(ps, po)
+    L = f"full/{name}/p{precision}"
+    assert within(L + "/vel", rel_err(vs, vo), tol), rel_err(vs, vo)
+    assert within(L + "/pres", rel_err(ps, po), 20 * tol), rel_err(ps, po)
     S.close()
 
 

@@ -207,3 +207,62 @@ def test_collocated_run_with_learned_closure_matches_oracle_nu_t():
     v2, p2 = S.download_level(10 % 4)
     assert np.all(np.isfinite(v2)) and np.all(np.isfinite(p2))
     S.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("shape", [(HW2, 32, 16, 24), (HW2, 54, 18, 9), (VV4, 36, 18, 20), (HW2, 64, 24, 40)])
+def test_closure_fused_into_flux_matches_separate_pass(shape, precision):
+    """tc_set_mlp_fusion(h, 1): the flux kernel evaluates the network for the planes it
+    stages (tile plus a one-cell halo).  Against the separate pass (k_turb_mlp, then the
+    flux kernel) over six steps.  The arithmetic is the same, but the compiler may fuse
+    multiply-adds differently in the two kernels: FP64 agrees to 1e-10 (relative to the
+    max-norm) in nu_t and the fields; in mixed precision a float-rounding difference can
+    move a feature across a BF16 rounding boundary of the network, so nu_t agrees to 1e-3
+    in the 2-norm and the fields to the mixed step tolerance (2e-4 velocity, 4e-3
+    pressure).  nu_t of the first step also against the oracle's features and network
+    (1e-2 in the 2-norm, as the separate-pass test).  Shapes cover partial tiles in x and
+    y (54 x 18, 36 x 18), one z-chunk (9 planes) and several (40), and VV4's wider
+    stencil."""
+    import turbchannel_b200 as tb
+
+    scheme, NX, NY, NZ = shape
+    prod, _, zz = make_case(scheme=scheme, NX=NX, NY=NY, NZ=NZ, precision=precision, turb=1)
+    m = tb.Mlp(seed=21)
+    P = m.params
+    m.close()
+    runs = []
+    for fuse in (0, 1):
+        S = tb.Solver(prod, zz)
+        S.set_turb_model(tb.TURB_MLP, P)
+        S.set_mlp_fusion(fuse)
+        S.init_channel(0, seed=5, amp=0.2, project=True)
+        tau, cur = 2e-3, 0
+        nts = []
+        for it in range(6):
+            S.Step(it * tau, tau, cur, min(it + 1, 3))
+            cur = (cur + 1) % 4
+            nts.append(S.get_nu_t())
+        v, p = S.download_level(cur)
+        runs.append((v, p, nts))
+        S.close()
+    (v0, p0, n0), (v1, p1, n1) = runs
+    for a, b in zip(n0, n1):
+        if precision == 0:
+            assert rel_err(b, a) < 1e-10
+        else:
+            assert np.linalg.norm(b - a) / np.linalg.norm(a) < 1e-3
+    tv, tp = (1e-10, 1e-10) if precision == 0 else (2e-4, 4e-3)
+    assert rel_err(v1, v0) < tv and rel_err(p1, p0) < tp
+    # the first step's nu_t is the closure of the initial field: against the oracle
+    S = tb.Solver(prod, zz)
+    S.init_channel(0, seed=5, amp=0.2, project=True)
+    v, _ = S.download_level(0)
+    S.close()
+    Fo = lo.box_filter(v, np.zeros(len(v)), NX, NY, NZ, 1)
+    utau = prod["inv_length_scale"] * prod["visc"]
+    G = lo.gradient(Fo[0:3], prod["hx"], prod["hy"], np.asarray(zz))
+    zc = 0.5 * (zz[:-1] + zz[1:])
+    d = np.minimum(zc - zz[0], zz[-1] - zc)[:, None, None]
+    X = lo.features_from_gradient(G, prod["visc"], utau, d).reshape(-1, 6).astype(np.float32)
+    want = prod["visc"] * lo.mlp_forward(P, X)
+    assert np.linalg.norm(n1[0] - want) / np.linalg.norm(want) < 1e-2

@@ -58,6 +58,6 @@ def test_report_renders():
         w = {k: (v.tolist() if isinstance(v, np.ndarray) else v) for k, v in d.items()}
         runs.append({"name": f"{name}_seed{seed}", "seed": seed, "steps": 10, "wall_ms_per_step": 1.0,
                      "windows": {"5": w, "10": w}})
-    txt = ps.report(None, {"kind": "long", "runs": runs, "window": 5, "stat_steps": 10, "dt": 8e-4,
+    txt = ps.report(None, {"kind": "long", "runs": runs, "windows": [5], "stat_steps": 10, "dt": 8e-4,
                            "spinup": [1, 1]})
     assert "mixed_seed1 vs fp64_seed1" in txt and "fp64_seed2 vs fp64_seed1" in txt

@@ -49,7 +49,7 @@ EXPORTS = [
 # Every entry point declared in include/turbch_les.h (learned LES closure).
 EXPORTS_LES = [
     "tc_les_filter", "tc_les_samples", "tc_mlp_create", "tc_mlp_destroy", "tc_mlp_get_params", "tc_mlp_set_params",
-    "tc_mlp_set_data", "tc_mlp_train", "tc_mlp_grad", "tc_mlp_forward",
+    "tc_mlp_set_data", "tc_mlp_train", "tc_mlp_grad", "tc_mlp_forward", "tc_set_mlp_fusion",
 ]
 MLP_NPAR = 4673
 NPHASE = 8
@@ -109,6 +109,7 @@ def load_library(path: str = LIB_PATH):
     L.tc_phase_times.argtypes = [vp, vp, C.POINTER(C.c_int)]
     L.tc_launch_count.argtypes = [vp, C.POINTER(C.c_ulonglong)]
     L.tc_set_diag_fusion.argtypes = [vp, ip]
+    L.tc_set_mlp_fusion.argtypes = [vp, ip]
     L.tc_srk_init.argtypes = [vp, ip, ip, vp, vp, ip, C.c_double]
     L.tc_srk_step.argtypes = [vp, C.c_double, C.c_double]
     ll = C.c_longlong
@@ -257,6 +258,10 @@ class Solver:
         """kind TURB_NONE / TURB_SMAGORINSKY / TURB_MLP (weights: MLP_NPAR float parameters)."""
         w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float32)
         self._check(self.L.tc_set_turb_model(self.h, kind, None if w is None else _ptr(w)))
+
+    def set_mlp_fusion(self, mode: int):
+        """1: the learned closure is evaluated inside the flux kernel; 0: a separate pass."""
+        self._check(self.L.tc_set_mlp_fusion(self.h, mode))
 
     # ---- learned closure: training data ----
     def les_filter(self, level: int, width: int = 4, width_z: int = 1):

@@ -9,23 +9,12 @@
 // from the RHS in the same pass (collocated_AB3/func_global.h:436-437).
 #include <algorithm>
 
+#include "flux_ring.cuh"
 #include "kernels.cuh"
 
 namespace tc {
 
-constexpr int CTX = 32, CTY = 8;
 constexpr int CPLANES = 128;  // planes whose constants a CTA keeps in shared memory
-
-template <typename T>
-struct CRing {
-    static constexpr int H = 1, PW = CTX + 2, PH = CTY + 2, PL = PW * PH, RS = 4;
-    const T* ring;
-    int zs, tx, ty;
-    __device__ __forceinline__ T operator()(int c, int dx, int dy, int dz) const {
-        const int slot = (zs + dz) & (RS - 1);
-        return ring[((slot * 3 + c) * PH + ty + 1 + dy) * PW + tx + 1 + dx];
-    }
-};
 
 // Galerkin viscous term, collocated_AB3/func_fluxes.h:21-85 (without the final
 // 1/(hx hy hz) factor).  NUT(ex, ey, ez) = nu_t of the element with lower corner at
@@ -94,10 +83,11 @@ __device__ __forceinline__ void visc_galerkin(const ACC& A, const NUT& nut, int 
     }
 }
 
-template <typename T, int VISC, bool LES, int ORDER, bool STAB1>
-__global__ void __launch_bounds__(CTX* CTY, 2) k_flux_coll(FluxArgs<T> a, int tz) {
-    using ACC = CRing<T>;
-    constexpr int PW = ACC::PW, PL = ACC::PL, RS = ACC::RS;
+// CY: nodes per thread along y (the tile is 32 x 8 CY nodes): two for float, one for double.
+template <typename T, int VISC, bool LES, int ORDER, bool STAB1, bool VEC, int CY>
+__global__ void __launch_bounds__(STX* STY, 2) k_flux_coll(FluxArgs<T> a, int tz) {
+    using ACC = RingAcc<T, 1, CY>;
+    constexpr int RS = ACC::RS;
     extern __shared__ __align__(16) unsigned char smraw[];
     T* ring = reinterpret_cast<T*>(smraw);
     __shared__ double sbuf[32];
@@ -105,32 +95,25 @@ __global__ void __launch_bounds__(CTX* CTY, 2) k_flux_coll(FluxArgs<T> a, int tz
     const Geom& g = a.g;
     const int NX = g.NX, NY = g.NY, NZ = g.NZ;
     const size_t NXY = (size_t)NX * NY;
-    const int tx = threadIdx.x % CTX, ty = threadIdx.x / CTX;
-    const int x0 = blockIdx.x * CTX, y0 = blockIdx.y * CTY;
+    const int tx = threadIdx.x % STX, tyt = threadIdx.x / STX;
+    const int x0 = blockIdx.x * STX, y0 = blockIdx.y * (STY * CY);
     const int zb = blockIdx.z * tz, ze = min(NZ, zb + tz);
-    const int ix = x0 + tx, iy = y0 + ty;
-    const bool active = ix < NX && iy < NY;
+    const int ix = x0 + tx;
 
-    auto load_plane = [&](int z) {
-        T* dst = ring + (z & (RS - 1)) * 3 * PL;
-        for (int e = threadIdx.x; e < 3 * PL; e += blockDim.x) {
-            const int c = e / PL, r = e - c * PL, py = r / PW, px = r - py * PW;
-            const int gx = wrapi(x0 - 1 + px, NX), gy = wrapi(y0 - 1 + py, NY);
-            cp_async<sizeof(T)>(dst + e, a.vel.c[c] + (size_t)z * NXY + (size_t)gy * NX + gx);
-        }
-    };
-    for (int z = max(0, zb - 1); z <= min(NZ - 1, zb + 1); z++) load_plane(z);
+    TileCopy<T, 1, CY, VEC> cp;
+    cp.init(x0, y0, NX, NY, g.N);
+    const T* vbase = a.vel.c[0];  // the three components are consecutive blocks of N
+    for (int z = max(0, zb - 1); z <= min(NZ - 1, zb + 1); z++) cp.load(ring, vbase, z, NXY);
     cp_async_commit();
 
     const int xm = wrapi(ix - 1, NX), xp = wrapi(ix + 1, NX);
-    const int ym = wrapi(iy - 1, NY), yp = wrapi(iy + 1, NY);
     const T hx = (T)g.hx, hy = (T)g.hy, ihx = (T)g.inv_hx, ihy = (T)g.inv_hy, visc = (T)g.visc;
     const T inv_tau = a.inv_tau;
     const double* cDZ = a.m.dDZ;
     double ub = 0.0;
     // per-plane constants of the CTA's planes, once in double: 2 / (DZ[z-1] + DZ[z]),
     // visc inv_hz / DZ[z], visc inv_hz / DZ[z-1] (cross viscosity); the per-node work
-    // then has no double arithmetic (measured: the kernel is instruction-bound)
+    // then has no double arithmetic
     __shared__ T pc[3][CPLANES];
     for (int k = threadIdx.x; k < ze - zb && k < CPLANES; k += blockDim.x) {
         const int z = zb + k;
@@ -145,18 +128,54 @@ __global__ void __launch_bounds__(CTX* CTY, 2) k_flux_coll(FluxArgs<T> a, int tz
     }
 
     for (int z = zb; z < ze; z++) {
-        if (z + 1 < ze && z + 2 < NZ) load_plane(z + 2);
+        if (z + 1 < ze && z + 2 < NZ) cp.load(ring, vbase, z + 2, NXY);
         cp_async_commit();
+        const bool wall = (z == 0 || z == NZ - 1);
+        // history (and, for StabType 1, p_n around the node) issued before the stencil so
+        // its latency overlaps it
+        T hp[CY][3], hq[CY][3], vp[CY][3], vq[CY][3], pn[CY][6];
+#pragma unroll
+        for (int q = 0; q < CY; q++) {
+            const int iy = y0 + tyt * CY + q;
+            if (ix >= NX || iy >= NY) continue;
+            const size_t id = (size_t)z * NXY + (size_t)iy * NX + ix;
+            if (ORDER >= 2) {
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    hp[q][c] = __ldg(a.fp.c[c] + id);
+                    vp[q][c] = __ldg(a.velp.c[c] + id);
+                    if (ORDER == 3) {
+                        hq[q][c] = __ldg(a.fq.c[c] + id);
+                        vq[q][c] = __ldg(a.velq.c[c] + id);
+                    }
+                }
+            }
+            if (STAB1 && ORDER > 0 && !wall) {
+                const T* p = a.pcur + (size_t)z * NXY;
+                const int ym = wrapi(iy - 1, NY), yp = wrapi(iy + 1, NY);
+                pn[q][0] = __ldg(p + (size_t)iy * NX + xp);
+                pn[q][1] = __ldg(p + (size_t)iy * NX + xm);
+                pn[q][2] = __ldg(p + (size_t)yp * NX + ix);
+                pn[q][3] = __ldg(p + (size_t)ym * NX + ix);
+                pn[q][4] = __ldg(a.pcur + id + NXY);
+                pn[q][5] = __ldg(a.pcur + id - NXY);
+            }
+        }
         cp_async_wait<1>();
         __syncthreads();
-        if (active) {
-            const ACC A{ring, z & (RS - 1), tx, ty};
+        const int kz = z - zb;
+        const T inv_hz = wall ? T(0) : (kz < CPLANES ? pc[0][kz] : (T)(2. / (cDZ[z - 1] + cDZ[z])));
+        ACC A0;
+        A0.set(ring, z & (RS - 1), tx, tyt * CY);
+#pragma unroll
+        for (int q = 0; q < CY; q++) {
+            const int iy = y0 + tyt * CY + q;
+            if (ix >= NX || iy >= NY) continue;
+            ACC A = A0;
+            A.shift_rows(q);
             const size_t id = (size_t)z * NXY + (size_t)iy * NX + ix;
             T f[3] = {0, 0, 0};
-            const bool wall = (z == 0 || z == NZ - 1);
             if (!wall) {
-                const int kz = z - zb;
-                const T inv_hz = kz < CPLANES ? pc[0][kz] : (T)(2. / (cDZ[z - 1] + cDZ[z]));
                 const T invh[3] = {ihx, ihy, inv_hz};
 #pragma unroll
                 for (int d = 0; d < 3; d++) {
@@ -171,6 +190,7 @@ __global__ void __launch_bounds__(CTX* CTY, 2) k_flux_coll(FluxArgs<T> a, int tz
                     }
                 }
                 if (VISC == TC_VISC_GALERKIN) {
+                    const int ym = wrapi(iy - 1, NY);
                     auto nut = [&](int ex, int ey, int ez) -> T {
                         if (!LES) return T(0);
                         const int xx = ex < 0 ? xm : ix, yy = ey < 0 ? ym : iy;
@@ -199,10 +219,9 @@ __global__ void __launch_bounds__(CTX* CTY, 2) k_flux_coll(FluxArgs<T> a, int tz
             if (ORDER > 0) {
                 T gp[3] = {0, 0, 0};
                 if (STAB1 && !wall) {
-                    const T* p = a.pcur;
-                    gp[0] = T(0.5) * ihx * (p[(size_t)z * NXY + (size_t)iy * NX + xp] - p[(size_t)z * NXY + (size_t)iy * NX + xm]);
-                    gp[1] = T(0.5) * ihy * (p[(size_t)z * NXY + (size_t)yp * NX + ix] - p[(size_t)z * NXY + (size_t)ym * NX + ix]);
-                    gp[2] = T(0.5) * (p[id + NXY] - p[id - NXY]) / a.m.cellh[z];
+                    gp[0] = T(0.5) * ihx * (pn[q][0] - pn[q][1]);
+                    gp[1] = T(0.5) * ihy * (pn[q][2] - pn[q][3]);
+                    gp[2] = T(0.5) * (pn[q][4] - pn[q][5]) / a.m.cellh[z];
                 }
                 T r[3];
 #pragma unroll
@@ -211,11 +230,10 @@ __global__ void __launch_bounds__(CTX* CTY, 2) k_flux_coll(FluxArgs<T> a, int tz
                     if (ORDER == 1) {
                         r[c] = f[c] + inv_tau * vn;
                     } else if (ORDER == 2) {
-                        r[c] = (T(2.) * f[c] - a.fp.c[c][id]) + inv_tau * (2 * vn - T(0.5) * a.velp.c[c][id]);
+                        r[c] = (T(2.) * f[c] - hp[q][c]) + inv_tau * (2 * vn - T(0.5) * vp[q][c]);
                     } else {
-                        r[c] = ((3 * f[c] - 3 * a.fp.c[c][id]) + a.fq.c[c][id]) +
-                               inv_tau * ((3 * vn - T(1.5) * a.velp.c[c][id]) +
-                                          T(0.33333333333333333333) * a.velq.c[c][id]);
+                        r[c] = ((3 * f[c] - 3 * hp[q][c]) + hq[q][c]) +
+                               inv_tau * ((3 * vn - T(1.5) * vp[q][c]) + T(0.33333333333333333333) * vq[q][c]);
                     }
                     if (STAB1) r[c] -= gp[c];
                     a.rhs.c[c][id] = r[c];
@@ -231,20 +249,29 @@ __global__ void __launch_bounds__(CTX* CTY, 2) k_flux_coll(FluxArgs<T> a, int tz
     }
 }
 
-static void flux_coll_shape(const Geom& g, dim3& grid, int& tz) {
-    const int tiles = ((g.NX + CTX - 1) / CTX) * ((g.NY + CTY - 1) / CTY);
+// nodes per thread along y: two for float, one for double (register budget of 2 CTAs/SM)
+template <typename T>
+constexpr int coll_cy() { return sizeof(T) == 4 ? 2 : 1; }
+
+static void flux_coll_shape(const Geom& g, int cy, dim3& grid, int& tz) {
+    const int ty = STY * cy;
+    const int tiles = ((g.NX + STX - 1) / STX) * ((g.NY + ty - 1) / ty);
     int nch = std::max(1, (148 * 8 + tiles - 1) / tiles);
     tz = std::max(4, (g.NZ + nch - 1) / nch);
-    grid = dim3((g.NX + CTX - 1) / CTX, (g.NY + CTY - 1) / CTY, (g.NZ + tz - 1) / tz);
+    grid = dim3((g.NX + STX - 1) / STX, (g.NY + ty - 1) / ty, (g.NZ + tz - 1) / tz);
 }
 
 template <typename T, int VISC, bool LES, int ORDER, bool STAB1>
 static void run(const FluxArgs<T>& a, cudaStream_t s) {
-    constexpr size_t smem = sizeof(T) * 4 * 3 * (CTX + 2) * (CTY + 2);
+    constexpr int CY = coll_cy<T>();
+    constexpr size_t smem = sizeof(T) * 4 * 3 * RingAcc<T, 1, CY>::PL;
+    const bool vec = a.g.NX % (16 / (int)sizeof(T)) == 0;
+    auto kern = vec ? k_flux_coll<T, VISC, LES, ORDER, STAB1, true, CY> : k_flux_coll<T, VISC, LES, ORDER, STAB1, false, CY>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     dim3 grid;
     int tz;
-    flux_coll_shape(a.g, grid, tz);
-    k_flux_coll<T, VISC, LES, ORDER, STAB1><<<grid, CTX * CTY, smem, s>>>(a, tz);
+    flux_coll_shape(a.g, CY, grid, tz);
+    kern<<<grid, STX * STY, smem, s>>>(a, tz);
 }
 
 template <typename T, int VISC, bool LES>

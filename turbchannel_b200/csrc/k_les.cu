@@ -164,44 +164,6 @@ __global__ void __launch_bounds__(256) k_les_features(const float* __restrict__ 
     Yo[c] = (float)(nus / nu);
 }
 
-// The closure's inputs in float (the run's inference path; the training samples use
-// les_features in double): same invariants, then rounded to BF16 by the network.
-__device__ __forceinline__ void les_features_f(const float G[3][3], float sc, float yplus, float* f) {
-    float S[3][3], O[3][3];
-#pragma unroll
-    for (int i = 0; i < 3; i++)
-#pragma unroll
-        for (int j = 0; j < 3; j++) {
-            S[i][j] = 0.5f * (G[i][j] + G[j][i]) * sc;
-            O[i][j] = 0.5f * (G[i][j] - G[j][i]) * sc;
-        }
-    float S2[3][3], O2[3][3];
-#pragma unroll
-    for (int i = 0; i < 3; i++)
-#pragma unroll
-        for (int j = 0; j < 3; j++) {
-            S2[i][j] = S[i][0] * S[0][j] + S[i][1] * S[1][j] + S[i][2] * S[2][j];
-            O2[i][j] = O[i][0] * O[0][j] + O[i][1] * O[1][j] + O[i][2] * O[2][j];
-        }
-    float l1 = 0, l2 = 0, l3 = 0, l4 = 0, l5 = 0;
-#pragma unroll
-    for (int i = 0; i < 3; i++)
-#pragma unroll
-        for (int j = 0; j < 3; j++) {
-            l1 += S[i][j] * S[j][i];
-            l2 += O[i][j] * O[j][i];
-            l3 += S2[i][j] * S[j][i];
-            l4 += O2[i][j] * S[j][i];
-            l5 += O2[i][j] * S2[j][i];
-        }
-    f[0] = asinhf(l1);
-    f[1] = asinhf(l2);
-    f[2] = asinhf(l3);
-    f[3] = asinhf(l4);
-    f[4] = asinhf(l5);
-    f[5] = 0.25f * log1pf(yplus);
-}
-
 // nu_t of a run from the learned closure.  P: packed FP32 parameters.  Each warp takes
 // 32 cells at a time: every lane gathers its cell's velocity gradient (differences in
 // T, then float) and features, then two 16-row tiles go through the network on the

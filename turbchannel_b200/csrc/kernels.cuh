@@ -188,6 +188,9 @@ void launch_les_filter(const T* u, const T* v, const T* w, const T* p, const dou
 void launch_les_features(const float* F, const Geom& g, int fw, int fz, const double* ZZ, float* X, float* Y,
                          cudaStream_t s);
 template <typename T> void launch_turb_mlp(const TurbArgs<T>& a, const float* P, cudaStream_t s);
+// the staggered step flux (orders 1..3, NAIVE viscosity) with the learned closure's
+// inference fused in; also writes nu_t of every cell to nu_out (k_flux_mlp.cu)
+template <typename T> void launch_flux_mlp(const FluxArgs<T>& a, const float* P, T* nu_out, cudaStream_t s);
 void launch_mlp_grad(const float* P, const float* X, const float* Y, long long n, float* part, float* grad,
                      cudaStream_t s);
 void launch_mlp_adam(float* P, float* M, float* V, const float* grad, float lr, int step, cudaStream_t s);

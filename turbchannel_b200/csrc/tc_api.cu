@@ -229,6 +229,7 @@ struct tc_handle {
     float* mlp_params = nullptr;  // learned closure (TC_TURB_MLP): packed FP32 parameters
     // diagnostics fused into the step's correction (tc_set_diag_fusion)
     int diag_fuse = 0;             // 0 off (default), 1 always, 2 when the caller reads every step's diagnostics
+    int mlp_fuse = 0;              // TC_TURB_MLP: 1 = closure evaluated inside the flux kernel (k_flux_mlp)
     bool diag_follow = false;      // mode 2: the last step's output level was read
     bool fused_valid = false, fused_used = false;
     int fused_level = -1, last_out = -1;
@@ -788,9 +789,10 @@ static int step_impl(tc_handle* h, double tau, int cur, int order) {
     const bool coll = g.scheme == TC_SCHEME_COLLOC;
     const bool stab1 = coll && g.stab_type == 1;
     const bool les = h->nu_t && (h->turb_kind == TC_TURB_SMAGORINSKY || h->turb_kind == TC_TURB_MLP);
+    const bool mlp_in_flux = les && h->turb_kind == TC_TURB_MLP && h->mlp_fuse && !coll;
     const size_t eb = h->ev_used;
     mark(h, 0, eb);
-    if (les) {
+    if (les && !mlp_in_flux) {
         turb_visc<T>(h, h->vel[cur]);
         h->launches += 1;
     }
@@ -814,6 +816,7 @@ static int step_impl(tc_handle* h, double tau, int cur, int order) {
     fa.ticket = h->ticket;
     fa.ub_out = cfr ? h->red : nullptr;
     if (coll) launch_flux_coll<T>(fa, h->st);
+    else if (mlp_in_flux) launch_flux_mlp<T>(fa, h->mlp_params, (T*)h->nu_t, h->st);
     else launch_flux_stag<T>(fa, h->st);
     h->launches += 1;
     mark(h, 2, eb);
@@ -1827,6 +1830,12 @@ extern "C" int tc_mlp_forward(tc_mlp* m, const float* features, long long n, flo
     cudaFree(X);
     cudaFree(O);
     if (e != cudaSuccess) return fail(TC_E_CUDA, std::string("tc_mlp_forward: ") + cudaGetErrorString(e));
+    return TC_OK;
+}
+
+extern "C" int tc_set_mlp_fusion(tc_handle* h, int mode) {
+    if (!h || mode < 0 || mode > 1) return fail(TC_E_ARG, "tc_set_mlp_fusion: bad handle or mode");
+    h->mlp_fuse = mode;
     return TC_OK;
 }
 

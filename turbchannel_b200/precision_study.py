@@ -15,7 +15,8 @@ short: both precisions from the same state, side by side, dt 0.0008; after 3, 10
 long: the turbulent statistics.  Each run: spin-up (dt 0.0006 through the transition,
     where the CFL number of the explicit convection peaks, then dt 0.0008), then
     statistics at dt 0.0008 accumulated on the device (tc_stats_accumulate every
-    `--stat-every` steps) over the first `--window` steps and over all `--stat-steps`.
+    `--stat-every` steps) over the first W steps for each W of `--windows` and over all
+    `--stat-steps`.
     Runs: FP64 and mixed from seed 12345, and FP64 and mixed from seed 12346.  Beyond a
     few thousand steps the trajectories of any two runs separate (the flow is chaotic), so
     their statistics differ by sampling error; FP64(12345) against FP64(12346) measures
@@ -144,7 +145,7 @@ def long_run(precision: int, seed: int, args, log) -> dict:
     S.stats_reset()
     windows = {}
     done = 0
-    for target in sorted({args.window, args.stat_steps}):
+    for target in sorted({*args.windows, args.stat_steps}):
         while done < target:
             n = min(args.stat_every, target - done)
             advance(n, args.dt, False)
@@ -175,7 +176,7 @@ def long(args) -> dict:
             with open(args.out + ".partial", "w") as f:
                 json.dump({"kind": "long", "runs": runs}, f)
     return {"kind": "long", "grid": list(args.grid), "dt": args.dt, "dt_transition": args.dt_a,
-            "spinup": [args.spinup_a, args.spinup_b], "stat_steps": args.stat_steps, "window": args.window,
+            "spinup": [args.spinup_a, args.spinup_b], "stat_steps": args.stat_steps, "windows": args.windows,
             "stat_every": args.stat_every, "vortex": args.vortex, "runs": runs}
 
 
@@ -200,6 +201,13 @@ def compare(a: dict, b: dict) -> dict:
     return out
 
 
+def pooled(ws: list) -> dict:
+    """Equal-weight mean of several runs' window statistics."""
+    out = {k: np.mean([np.asarray(w[k]) for w in ws], axis=0) for k in STATS}
+    out["Re_tau"] = float(np.mean([w["Re_tau"] for w in ws]))
+    return out
+
+
 def report(short_res: dict | None, long_res: dict | None) -> str:
     L = []
     if short_res:
@@ -219,7 +227,8 @@ def report(short_res: dict | None, long_res: dict | None) -> str:
             if "failed" in r:
                 L.append(f"Run {r['name']} failed: {r['failed']}\n")
         seeds = sorted({r["seed"] for r in long_res["runs"]})
-        for w in sorted({str(long_res["window"]), str(long_res["stat_steps"])}, key=int):
+        wins = long_res.get("windows", [long_res.get("window")])
+        for w in sorted({*(str(x) for x in wins if x), str(long_res["stat_steps"])}, key=int):
             L.append(f"### Statistics over {w} steps at dt {long_res['dt']} (after {sum(long_res['spinup'])} "
                      f"spin-up steps)\n")
             L.append("| pair | mean U max (L2) | u'u' | v'v' | w'w' | u'w' | p_rms | Re_tau |")
@@ -228,10 +237,15 @@ def report(short_res: dict | None, long_res: dict | None) -> str:
             if len(seeds) > 1:
                 pairs += [(f"fp64_seed{seeds[1]}", f"fp64_seed{seeds[0]}"),
                           (f"mixed_seed{seeds[1]}", f"mixed_seed{seeds[0]}")]
+            wstats = {n: r["windows"][w] for n, r in runs.items()}
+            if len(seeds) > 1 and all(f"{k}_seed{s}" in runs for k in ("fp64", "mixed") for s in seeds):
+                for k in ("fp64", "mixed"):  # the seeds' statistics averaged: half the sampling variance
+                    wstats[f"{k}_pooled"] = pooled([wstats[f"{k}_seed{s}"] for s in seeds])
+                pairs.append(("mixed_pooled", "fp64_pooled"))
             for a, b in pairs:
-                if a not in runs or b not in runs:
+                if a not in wstats or b not in wstats:
                     continue
-                c = compare(runs[a]["windows"][w], runs[b]["windows"][w])
+                c = compare(wstats[a], wstats[b])
                 cells = [f"{c['U']['max_rel']:.2%} ({c['U']['l2_rel']:.2%})"] + \
                         [f"{c[k]['max_rel']:.1%}" for k in STATS[1:]] + [f"{c['Re_tau']:.2%}"]
                 L.append(f"| {a} vs {b} | " + " | ".join(cells) + " |")
@@ -261,7 +275,8 @@ def main():
     ap.add_argument("--spinup-a", type=int, default=20000)
     ap.add_argument("--spinup-b", type=int, default=10000)
     ap.add_argument("--stat-steps", type=int, default=25000)
-    ap.add_argument("--window", type=int, default=5000)
+    ap.add_argument("--windows", type=int, nargs="+", default=[5000],
+                    help="also report the statistics over the first W steps of the window")
     ap.add_argument("--stat-every", type=int, default=5)
     args = ap.parse_args()
     if args.mode == "report":
