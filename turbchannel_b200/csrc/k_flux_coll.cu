@@ -108,7 +108,7 @@ __global__ void __launch_bounds__(STX* STY, 2) k_flux_coll(FluxArgs<T> a, int tz
 
     const int xm = wrapi(ix - 1, NX), xp = wrapi(ix + 1, NX);
     const T hx = (T)g.hx, hy = (T)g.hy, ihx = (T)g.inv_hx, ihy = (T)g.inv_hy, visc = (T)g.visc;
-    const T inv_tau = a.inv_tau;
+    const T inv_tau = a.inv_tau, it2 = T(0.5) * a.inv_tau, it6 = a.inv_tau * T(0.16666666666666666667);
     const double* cDZ = a.m.dDZ;
     double ub = 0.0;
     // per-plane constants of the CTA's planes, once in double: 2 / (DZ[z-1] + DZ[z]),
@@ -133,7 +133,7 @@ __global__ void __launch_bounds__(STX* STY, 2) k_flux_coll(FluxArgs<T> a, int tz
         const bool wall = (z == 0 || z == NZ - 1);
         // history (and, for StabType 1, p_n around the node) issued before the stencil so
         // its latency overlaps it
-        T hp[CY][3], hq[CY][3], vp[CY][3], vq[CY][3], pn[CY][6];
+        T hp[CY][3], hq[CY][3], vq[CY][3], pn[CY][6];
 #pragma unroll
         for (int q = 0; q < CY; q++) {
             const int iy = y0 + tyt * CY + q;
@@ -143,7 +143,6 @@ __global__ void __launch_bounds__(STX* STY, 2) k_flux_coll(FluxArgs<T> a, int tz
 #pragma unroll
                 for (int c = 0; c < 3; c++) {
                     hp[q][c] = __ldg(a.fp.c[c] + id);
-                    vp[q][c] = __ldg(a.velp.c[c] + id);
                     if (ORDER == 3) {
                         hq[q][c] = __ldg(a.fq.c[c] + id);
                         vq[q][c] = __ldg(a.velq.c[c] + id);
@@ -214,9 +213,10 @@ __global__ void __launch_bounds__(STX* STY, 2) k_flux_coll(FluxArgs<T> a, int tz
                 }
                 f[0] += (T)g.sour_dpdx;
             }
+            if (ORDER == 0) {
 #pragma unroll
-            for (int c = 0; c < 3; c++) a.fout.c[c][id] = f[c];
-            if (ORDER > 0) {
+                for (int c = 0; c < 3; c++) a.fout.c[c][id] = f[c];
+            } else {
                 T gp[3] = {0, 0, 0};
                 if (STAB1 && !wall) {
                     gp[0] = T(0.5) * ihx * (pn[q][0] - pn[q][1]);
@@ -227,15 +227,10 @@ __global__ void __launch_bounds__(STX* STY, 2) k_flux_coll(FluxArgs<T> a, int tz
 #pragma unroll
                 for (int c = 0; c < 3; c++) {
                     const T vn = A(c, 0, 0, 0);
-                    if (ORDER == 1) {
-                        r[c] = f[c] + inv_tau * vn;
-                    } else if (ORDER == 2) {
-                        r[c] = (T(2.) * f[c] - hp[q][c]) + inv_tau * (2 * vn - T(0.5) * vp[q][c]);
-                    } else {
-                        r[c] = ((3 * f[c] - 3 * hp[q][c]) + hq[q][c]) +
-                               inv_tau * ((3 * vn - T(1.5) * vp[q][c]) + T(0.33333333333333333333) * vq[q][c]);
-                    }
+                    r[c] = sbdf_rhs<ORDER, T>(f[c], vn, ORDER >= 2 ? hp[q][c] : T(0), ORDER == 3 ? hq[q][c] : T(0),
+                                              ORDER == 3 ? vq[q][c] : T(0), inv_tau, it6);
                     if (STAB1) r[c] -= gp[c];
+                    a.fout.c[c][id] = f[c] + it2 * vn;  // A_n
                     a.rhs.c[c][id] = r[c];
                 }
                 ub += (double)r[0] * (double)a.m.cellh[z];

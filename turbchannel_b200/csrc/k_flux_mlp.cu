@@ -218,20 +218,19 @@ __global__ void __launch_bounds__(FMX* FMY, 1) k_flux_mlp(FluxArgs<T> a, const f
     mz.ihx = (T)g.inv_hx;
     mz.ihy = (T)g.inv_hy;
     mz.visc = (T)g.visc;
-    const T inv_tau = a.inv_tau;
+    const T inv_tau = a.inv_tau, it2 = T(0.5) * a.inv_tau, it6 = a.inv_tau * T(0.16666666666666666667);
     const T visc = (T)g.visc;
     double ub = 0.0;
 
     for (int z = zb; z < ze; z++) {
         if (z + 1 < ze && z + 4 < NZ) cp.load(ring, vbase, z + 4, NXY);
         cp_async_commit();
-        T hp[3], hq[3], vp[3], vq[3];
+        T hp[3], hq[3], vq[3];
         if (ORDER >= 2 && own) {
             const size_t id = (size_t)z * NXY + (size_t)iy * NX + ix;
 #pragma unroll
             for (int c = 0; c < 3; c++) {
                 hp[c] = __ldg(a.fp.c[c] + id);
-                vp[c] = __ldg(a.velp.c[c] + id);
                 if (ORDER == 3) {
                     hq[c] = __ldg(a.fq.c[c] + id);
                     vq[c] = __ldg(a.velq.c[c] + id);
@@ -269,18 +268,14 @@ __global__ void __launch_bounds__(FMX* FMY, 1) k_flux_mlp(FluxArgs<T> a, const f
             f[2] = (T(0) + cf[2]) + vf[2];
             if (z == 0) f[2] = 0;
             const size_t id = (size_t)z * NXY + (size_t)iy * NX + ix;
-#pragma unroll
-            for (int c = 0; c < 3; c++) a.fout.c[c][id] = f[c];
-            if (ORDER > 0) {
+            {
                 T r[3];
 #pragma unroll
                 for (int c = 0; c < 3; c++) {
                     const T vn = A(c, 0, 0, 0);
-                    if (ORDER == 1) r[c] = f[c] + inv_tau * vn;
-                    else if (ORDER == 2) r[c] = (T(2.) * f[c] - hp[c]) + inv_tau * (2 * vn - T(0.5) * vp[c]);
-                    else
-                        r[c] = ((3 * f[c] - 3 * hp[c]) + hq[c]) +
-                               inv_tau * ((3 * vn - T(1.5) * vp[c]) + T(0.33333333333333333333) * vq[c]);
+                    r[c] = sbdf_rhs<ORDER, T>(f[c], vn, ORDER >= 2 ? hp[c] : T(0), ORDER == 3 ? hq[c] : T(0),
+                                              ORDER == 3 ? vq[c] : T(0), inv_tau, it6);
+                    a.fout.c[c][id] = f[c] + it2 * vn;  // A_n
                     a.rhs.c[c][id] = r[c];
                 }
                 ub += (double)r[0] * (double)a.m.DZ[z];

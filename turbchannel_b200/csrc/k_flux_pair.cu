@@ -9,7 +9,12 @@
 // the other accesses load anyway), the arithmetic of both cells is one packed
 // instruction, and the history/outputs move as 8-byte global accesses.  The
 // stencils are the ones of stencil_stag.cuh, instantiated with the pair type F2.
-// Used for the CROSS (DNS) viscosity; every other variant keeps k_flux_stag.
+// Used for the CROSS (DNS) viscosity; every other variant keeps k_flux_stag.  Its flux
+// history is the reference's F_n (the other flux kernels keep A_n = F_n + v_n/(2 tau), see
+// sbdf_rhs): measured at 384x384x256, reading A_{n-1}, A_{n-2}, v_{n-2} instead of F_{n-1},
+// F_{n-2}, v_{n-1}, v_{n-2} moved 20% fewer bytes but took 0.741 against 0.702 ms -- at 254
+// registers the compiler re-read stencil values from shared memory (+24% shared loads,
+// +8% instructions), and staging the history in shared memory instead took 0.987 ms.
 #include <algorithm>
 
 #include "kernels.cuh"
@@ -389,8 +394,12 @@ static void run_pair_order(const FluxArgs<float>& a, cudaStream_t s) {
 
 // The pair kernel covers the CROSS viscosity with NX % 4 == 0 (16-byte tile chunks);
 // returns false for every other case.
+bool flux_pair_covers(const Geom& g) {
+    return g.scheme != TC_SCHEME_COLLOC && g.visc_type == TC_VISC_CROSS && g.NX % 4 == 0;
+}
+
 bool launch_flux_stag_pair(const FluxArgs<float>& a, cudaStream_t s) {
-    if (a.g.visc_type != TC_VISC_CROSS || a.g.NX % 4 != 0) return false;
+    if (!flux_pair_covers(a.g)) return false;
     if (a.g.scheme == TC_SCHEME_VV4) run_pair_order<TC_SCHEME_VV4>(a, s);
     else run_pair_order<TC_SCHEME_HW2>(a, s);
     return true;

@@ -79,14 +79,14 @@ __global__ void __launch_bounds__(STX* STY, 2) k_flux_stag(FluxArgs<T> a, int tz
     mz.ihy = (T)g.inv_hy;
     mz.visc = (T)g.visc;
     const int xm = wrapi(ix - 1, NX), xp = wrapi(ix + 1, NX);
-    const T inv_tau = a.inv_tau;
+    const T inv_tau = a.inv_tau, it2 = T(0.5) * a.inv_tau, it6 = a.inv_tau * T(0.16666666666666666667);
     double ub = 0.0;
 
     for (int z = zb; z < ze; z++) {
         if (z + 1 < ze && z + H + 1 < NZ) cp.load(ring, vbase, z + H + 1, NXY);
         cp_async_commit();
         // history of this thread's cells, issued before the stencil so its latency overlaps it
-        T hp[CY][3], hq[CY][3], vp[CY][3], vq[CY][3];
+        T hp[CY][3], hq[CY][3], vq[CY][3];
         if (ORDER >= 2) {
 #pragma unroll
             for (int q = 0; q < CY; q++) {
@@ -96,10 +96,11 @@ __global__ void __launch_bounds__(STX* STY, 2) k_flux_stag(FluxArgs<T> a, int tz
 #pragma unroll
                     for (int c = 0; c < 3; c++) {
                         hp[q][c] = __ldg(a.fp.c[c] + id);
-                        vp[q][c] = __ldg(a.velp.c[c] + id);
                         if (ORDER == 3) {
                             hq[q][c] = __ldg(a.fq.c[c] + id);
                             vq[q][c] = __ldg(a.velq.c[c] + id);
+                        } else {
+                            hq[q][c] = vq[q][c] = T(0);
                         }
                     }
                 }
@@ -127,17 +128,17 @@ __global__ void __launch_bounds__(STX* STY, 2) k_flux_stag(FluxArgs<T> a, int tz
             if (z == 0) f[2] = 0;
             const size_t id = (size_t)z * NXY + (size_t)iy * NX + ix;
 #pragma unroll
-            for (int c = 0; c < 3; c++) a.fout.c[c][id] = f[c];
-            if (ORDER > 0) {
+            if (ORDER == 0) {
+#pragma unroll
+                for (int c = 0; c < 3; c++) a.fout.c[c][id] = f[c];
+            } else {
                 T r[3];
 #pragma unroll
                 for (int c = 0; c < 3; c++) {
                     const T vn = A(c, 0, 0, 0);
-                    if (ORDER == 1) r[c] = f[c] + inv_tau * vn;
-                    else if (ORDER == 2) r[c] = (T(2.) * f[c] - hp[q][c]) + inv_tau * (2 * vn - T(0.5) * vp[q][c]);
-                    else
-                        r[c] = ((3 * f[c] - 3 * hp[q][c]) + hq[q][c]) +
-                               inv_tau * ((3 * vn - T(1.5) * vp[q][c]) + T(0.33333333333333333333) * vq[q][c]);
+                    r[c] = sbdf_rhs<ORDER, T>(f[c], vn, ORDER >= 2 ? hp[q][c] : T(0), ORDER == 3 ? hq[q][c] : T(0),
+                                              ORDER == 3 ? vq[q][c] : T(0), inv_tau, it6);
+                    a.fout.c[c][id] = f[c] + it2 * vn;  // A_n
                     a.rhs.c[c][id] = r[c];
                 }
                 ub += (double)r[0] * (double)a.m.DZ[z];

@@ -25,8 +25,10 @@ template <typename T>
 struct FluxArgs {
     Geom g;
     MeshDev<T> m;
+    // vel = v_n (stencil), velq = v_{n-2}; fp, fq = the flux ring's levels n-1, n-2, which
+    // hold A_m = F_m + v_m / (2 tau) (sbdf_rhs); velp (v_{n-1}) is not read by the step
     CV3<T> vel, velp, velq, fp, fq;
-    V3<T> fout, rhs;
+    V3<T> fout, rhs;  // fout: A_n (orders 1..3) or F_n (order 0); rhs: the SBDF right-hand side
     const T* nu_t;
     const T* pcur;
     T inv_tau;
@@ -35,6 +37,23 @@ struct FluxArgs {
     unsigned* ticket;
     double* ub_out;
 };
+
+// SBDF right-hand side (staggered/func_global.h:910-932) with the flux history kept as
+// A_m = F_m + v_m / (2 tau) instead of F_m: since
+//   3 F_{n-1} + (3/2) v_{n-1} / tau = 3 A_{n-1} and F_{n-2} + v_{n-2} / (3 tau) =
+//   A_{n-2} - v_{n-2} / (6 tau) (order 3), F_{n-1} + v_{n-1} / (2 tau) = A_{n-1} (order 2),
+// the combination reads one array per history level plus v_{n-2} -- 3 words per cell
+// fewer than F_{n-1}, F_{n-2}, v_{n-1}, v_{n-2} -- and the new level A_n = F_n + v_n/(2 tau)
+// is written in place of F_n.  b = F_n + v_n / tau.
+//   order 1: b;   order 2: 2 b - A_{n-1};   order 3: 3 b - 3 A_{n-1} + A_{n-2} - v_{n-2}/(6 tau)
+// it = 1/tau, it6 = 1/(6 tau) (in the working precision).
+template <int ORDER, typename V>
+__device__ __forceinline__ V sbdf_rhs(V f, V vn, V ap, V aq, V vq, V it, V it6) {
+    const V b = f + it * vn;
+    if (ORDER == 1) return b;
+    if (ORDER == 2) return V(2) * b - ap;
+    return (V(3) * b - V(3) * ap) + (aq - it6 * vq);
+}
 
 // Divergence of the RHS fused with the forward real FFT along x.  Output: half
 // spectrum spec[z][kx][y] (kx = 0..NX/2, y fastest).  src_scalar != nullptr: the
@@ -157,6 +176,7 @@ constexpr int NDIAG_SUMS = 16;  // planes[z][0..15] are sums, [16..18] CFL maxim
 template <typename T> void launch_flux_stag(const FluxArgs<T>& a, cudaStream_t s);
 template <typename T> void launch_flux_coll(const FluxArgs<T>& a, cudaStream_t s);
 bool launch_flux_stag_pair(const FluxArgs<float>& a, cudaStream_t s);  // k_flux_pair.cu; false: not covered
+bool flux_pair_covers(const Geom& g);  // the float pair kernel takes the step (its history is plain F)
 template <typename T> int launch_div_xfft(const DivFftArgs<T>& a, cudaStream_t s);  // returns launches
 template <typename T> void launch_yfft(const YFftArgs<T>& a, cudaStream_t s);
 template <typename T> void launch_zsolve(const ZSolveArgs<T>& a, cudaStream_t s, cudaStream_t side, cudaEvent_t fork,

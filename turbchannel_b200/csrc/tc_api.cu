@@ -192,6 +192,11 @@ struct tc_handle {
     size_t esz = 8;
     void* vel[4] = {};
     void* flux[4] = {};
+    // The flux ring's level l holds A_l = F_l + hist_it[l] v_l / 2 (sbdf_rhs in kernels.cuh):
+    // hist_it[l] is the 1/tau (in the working precision) of the step that wrote it; 0 =
+    // plain F (a new handle, a checkpoint of the first format).
+    double hist_it[4] = {0.0, 0.0, 0.0, 0.0};
+    bool hist_a = true;  // false: the step's flux kernel keeps plain F (k_flux_pair), hist_it stays 0
     void* pres[4] = {};
     void* nu_t = nullptr;
     void* ptmp = nullptr;
@@ -449,6 +454,7 @@ extern "C" int tc_create(const tc_params* prm, const double* zz, tc_handle** out
     g.inv_hx = 1. / p.hx; g.inv_hy = 1. / p.hy; g.area = p.area;
     h->fp64 = p.precision == TC_FP64;
     h->esz = h->fp64 ? 8 : 4;
+    h->hist_a = h->fp64 || !flux_pair_covers(g);
     h->turb_kind = p.turb_model;
     if (plan_fft(p.NX, h->px) || plan_fft(p.NY, h->py)) {
         delete h;
@@ -672,11 +678,42 @@ static int down_scal(tc_handle* h, const void* src, double* dst) {
 
 #define TC_DISPATCH(h, fn, ...) ((h)->fp64 ? fn<double>(__VA_ARGS__) : fn<float>(__VA_ARGS__))
 
+// Brings flux level l to A_l = F_l + it v_l / 2 (one pass, only when the step's 1/tau
+// differs from the one the level was written with: the reference restarts the BDF
+// order after a change of tau, so a continuing order meets this only after a checkpoint
+// of the first format or a caller that changes tau without restarting).
+template <typename T>
+static void rebase_hist(tc_handle* h, int l, double it) {
+    if (!h->hist_a) it = 0.0;
+    if (h->hist_it[l] == it) return;
+    LinComb<T> lc{};
+    lc.out = (T*)h->flux[l];
+    lc.x[0] = (const T*)h->flux[l];
+    lc.c[0] = 1.0;
+    lc.x[1] = (const T*)h->vel[l];
+    lc.c[1] = 0.5 * (it - h->hist_it[l]);
+    lc.post = 1.0;
+    lc.nt = 2;
+    lc.n = 3 * h->g.N;
+    launch_lincomb<T>(lc, h->st);
+    h->launches += 1;
+    h->hist_it[l] = it;
+}
+
+// Before a caller may change v_l (upload, zero-copy pointers, a new initial field), flux
+// level l goes back to plain F_l, so the history means what the reference's would.
+static void hist_plain(tc_handle* h, int l) {
+    if (h->hist_it[l] == 0.0) return;
+    if (h->fp64) rebase_hist<double>(h, l, 0.0);
+    else rebase_hist<float>(h, l, 0.0);
+}
+
 extern "C" int tc_upload_level(tc_handle* h, int level, const double* vel, const double* p) {
     if (!h || level < 0 || level > 3) return fail(TC_E_ARG, "tc_upload_level: bad handle or level");
     if (h) h->fused_valid = false;
     cudaSetDevice(h->prm.device);
     int rc = TC_OK;
+    if (vel) hist_plain(h, level);
     if (vel) rc = TC_DISPATCH(h, up_vec, h, vel, h->vel[level]);
     if (!rc && p) rc = TC_DISPATCH(h, up_scal, h, p, h->pres[level]);
     if (!rc) TC_CUDA(cudaStreamSynchronize(h->st));
@@ -693,11 +730,24 @@ extern "C" int tc_download_level(tc_handle* h, int level, double* vel, double* p
 extern "C" int tc_download_flux(tc_handle* h, int level, double* f) {
     if (!h || level < 0 || level > 3 || !f) return fail(TC_E_ARG, "tc_download_flux: bad argument");
     cudaSetDevice(h->prm.device);
-    return TC_DISPATCH(h, down_vec, h, h->flux[level], f);
+    int rc = TC_DISPATCH(h, down_vec, h, h->flux[level], f);
+    if (rc || h->hist_it[level] == 0.0) return rc;
+    // the reference's F_l = A_l - v_l / (2 tau)
+    const size_t n = 3 * (size_t)h->g.N;
+    std::vector<double> v(n);
+    rc = TC_DISPATCH(h, down_vec, h, h->vel[level], v.data());
+    if (rc) return rc;
+    const double c = 0.5 * h->hist_it[level];
+    for (size_t i = 0; i < n; i++) f[i] -= c * v[i];
+    return TC_OK;
 }
 extern "C" int tc_device_level(tc_handle* h, int level, void** vel, void** p) {
     if (h) h->fused_valid = false;  // the caller may write the level
     if (!h || level < 0 || level > 3) return fail(TC_E_ARG, "tc_device_level: bad handle or level");
+    if (vel) {
+        cudaSetDevice(h->prm.device);
+        hist_plain(h, level);
+    }
     if (vel) *vel = h->vel[level];
     if (p) *p = h->pres[level];
     return TC_OK;
@@ -815,9 +865,14 @@ static int step_impl(tc_handle* h, double tau, int cur, int order) {
     fa.ub_partial = h->red + 2;
     fa.ticket = h->ticket;
     fa.ub_out = cfr ? h->red : nullptr;
+    const double itd = (double)inv_tau;
+    if (order >= 2) rebase_hist<T>(h, prv, itd);
+    if (order == 3) rebase_hist<T>(h, pr2, itd);
     if (coll) launch_flux_coll<T>(fa, h->st);
     else if (mlp_in_flux) launch_flux_mlp<T>(fa, h->mlp_params, (T*)h->nu_t, h->st);
     else launch_flux_stag<T>(fa, h->st);
+    h->hist_it[cur] = h->hist_a ? itd : 0.0;
+    h->hist_it[nxt] = 0.0;  // that level now holds the right-hand side (the reference's flux[next]), not an A
     h->launches += 1;
     mark(h, 2, eb);
     void* pdest = stab1 ? h->ptmp : h->pres[nxt];
@@ -1465,6 +1520,7 @@ static int project_level(tc_handle* h, int level) {
 extern "C" int tc_init_channel(tc_handle* h, int level, unsigned long long seed, double amp, int project) {
     if (!h || level < 0 || level > 3) return fail(TC_E_ARG, "tc_init_channel: bad handle or level");
     cudaSetDevice(h->prm.device);
+    hist_plain(h, level);
     const Geom& g = h->g;
     const size_t N = (size_t)g.N;
     std::vector<double> v(3 * N), p(N, 0.0);
@@ -1860,7 +1916,8 @@ struct CkptHeader {
     int32_t version, scheme, precision, NX, NY, NZ, current_field, forcing_mode;
     double t, forcing_value, sour_dpdx, last_tau, last_bd0, last_du;
     int64_t N;
-    char pad[256 - 8 - 8 * 4 - 6 * 8 - 8];
+    double hist_it[4];  // version 2: the 1/tau baked into each flux level (A = F + it v / 2)
+    char pad[256 - 8 - 8 * 4 - 6 * 8 - 8 - 4 * 8];
 };
 static_assert(sizeof(CkptHeader) == 256, "checkpoint header size");
 
@@ -1910,7 +1967,8 @@ extern "C" int tc_checkpoint_save(tc_handle* h, const char* path, int current_fi
     CkptHeader hd;
     memset(&hd, 0, sizeof(hd));
     memcpy(hd.magic, TC_CKPT_MAGIC, 8);
-    hd.version = 1;
+    hd.version = 2;
+    for (int l = 0; l < 4; l++) hd.hist_it[l] = h->hist_it[l];
     hd.scheme = h->prm.scheme;
     hd.precision = h->prm.precision;
     hd.NX = h->g.NX;
@@ -1942,7 +2000,8 @@ extern "C" int tc_checkpoint_load(tc_handle* h, const char* path, int* current_f
     FileCloser fc{fopen(path, "rb")};
     if (!fc.f) return fail(TC_E_ARG, std::string("tc_checkpoint_load: cannot open ") + path);
     CkptHeader hd;
-    if (fread(&hd, sizeof(hd), 1, fc.f) != 1 || memcmp(hd.magic, TC_CKPT_MAGIC, 8) != 0 || hd.version != 1)
+    if (fread(&hd, sizeof(hd), 1, fc.f) != 1 || memcmp(hd.magic, TC_CKPT_MAGIC, 8) != 0 || hd.version < 1 ||
+        hd.version > 2)
         return fail(TC_E_ARG, "tc_checkpoint_load: not a checkpoint of this library");
     if (hd.scheme != h->prm.scheme || hd.precision != h->prm.precision || hd.NX != h->g.NX || hd.NY != h->g.NY ||
         hd.NZ != h->g.NZ || hd.N != h->g.N || hd.current_field < 0 || hd.current_field > 3)
@@ -1956,6 +2015,7 @@ extern "C" int tc_checkpoint_load(tc_handle* h, const char* path, int* current_f
     h->g.sour_dpdx = hd.sour_dpdx;
     h->last_tau = hd.last_tau;
     h->last_bd0 = hd.last_bd0;
+    for (int l = 0; l < 4; l++) h->hist_it[l] = hd.version >= 2 ? hd.hist_it[l] : 0.0;  // version 1: plain F
     TC_CUDA(cudaMemcpy(h->red + 1, &hd.last_du, sizeof(double), cudaMemcpyHostToDevice));
     h->fused_valid = false;
     if (current_field) *current_field = hd.current_field;
@@ -2081,6 +2141,18 @@ extern "C" int tc_run_graph(tc_handle* h, double tau, int current_field, int nst
         cudaGetLastError();
         return fail(TC_E_NOMEM, "tc_run_graph: allocation failed");
     }
+    {
+        // the graph's order-3 steps read flux levels current-1 and current-2 as written with
+        // this tau: bring them there outside the graph
+        const double itd = h->fp64 ? (double)(1. / tau) : (double)(float)(1. / tau);
+        if (h->fp64) {
+            rebase_hist<double>(h, (current_field + 3) % 4, itd);
+            rebase_hist<double>(h, (current_field + 2) % 4, itd);
+        } else {
+            rebase_hist<float>(h, (current_field + 3) % 4, itd);
+            rebase_hist<float>(h, (current_field + 2) % 4, itd);
+        }
+    }
     if (!h->run_exec || h->run_tau != tau || h->run_cur != current_field || h->run_every != check_every ||
         h->run_mode != cfl_mode) {
         int rc = run_graph_build(h, tau, current_field, check_every, cfl_mode);
@@ -2093,6 +2165,10 @@ extern "C" int tc_run_graph(tc_handle* h, double tau, int current_field, int nst
     TC_CUDA(cudaStreamSynchronize(h->st));
     h->fused_valid = false;
     h->last_out = current_field;
+    {  // every level was rewritten by the graph's steps (at least check_every >= 4 of them)
+        const double itd = h->fp64 ? (double)(1. / tau) : (double)(float)(1. / tau);
+        for (int l = 0; l < 4; l++) h->hist_it[l] = h->hist_a ? itd : 0.0;
+    }
     if (steps_done) *steps_done = (int)c.iters * check_every;
     if (cfl) *cfl = c.cfl;
     return TC_OK;
