@@ -96,6 +96,10 @@ def run_dns(args, log):
     tau, cur = args.dt, 0
     prof, nprof = np.zeros(args.nz), 0
     samples = {cz: ([], []) for cz in args.coarsen}
+    # resolved statistics of the filtered DNS on each LES grid, from the snapshots: per coarse
+    # plane the sums of the filtered u, v, w and of their products (plane means, then time)
+    fstat = {cz: np.zeros((args.nz // cz[1], 6)) for cz in args.coarsen}
+    nfs = 0
     rng = np.random.default_rng(1)
     t0 = time.time()
     total = args.dns_steps + args.stat_steps
@@ -111,6 +115,13 @@ def run_dns(args, log):
                 if args.snap_dir:  # the filtered snapshot of the first LES grid, 10 fields
                     r0, rz0 = args.coarsen[0]
                     np.save(os.path.join(args.snap_dir, f"snap_{k:07d}.npy"), S.les_filter(cur, r0, rz0))
+                for (r, rz) in args.coarsen:
+                    F = S.les_filter(cur, r, rz).astype(np.float64)
+                    ub, vb, wb = F[0], F[1], F[2]
+                    fstat[(r, rz)] += np.stack([ub.mean(axis=(1, 2)), vb.mean(axis=(1, 2)), wb.mean(axis=(1, 2)),
+                                                (ub * ub).mean(axis=(1, 2)), (wb * wb).mean(axis=(1, 2)),
+                                                (ub * wb).mean(axis=(1, 2))], axis=1)
+                nfs += 1
                 for (r, rz), (Xs, Ys) in samples.items():
                     X, Y = S.les_samples(cur, r, rz)
                     sel = rng.random(len(Y)) < args.sample_frac * r * r * rz / 64
@@ -122,7 +133,8 @@ def run_dns(args, log):
     S.sync()
     vel, _ = S.download_level(cur)
     S.close()
-    return dict(params=p, zz=zz, prof=prof / max(nprof, 1), vel=vel, wall_s=time.time() - t0,
+    return dict(params=p, zz=zz, prof=prof / max(nprof, 1), vel=vel, wall_s=time.time() - t0, snapshots=nfs,
+                fstat={cz: v / max(nfs, 1) for cz, v in fstat.items()},
                 samples={cz: (np.concatenate(Xs), np.concatenate(Ys)) for cz, (Xs, Ys) in samples.items()})
 
 
@@ -138,6 +150,7 @@ def run_les(args, model, params, vel0, r, rz, log):
     S.set_forcing(1, 1.0)
     tau, cur = args.les_dt, 0
     prof, wsum = np.zeros(p["NZ"]), 0.0
+    full = np.zeros((p["NZ"], 12))
     total = args.les_steps + args.les_stat_steps
     import torch
 
@@ -152,7 +165,9 @@ def run_les(args, model, params, vel0, r, rz, log):
         cur = (cur + 1) % 4
         t += tau
         if it >= args.les_steps and (it - args.les_steps) % args.stat_every == 0:
-            prof += tau * S.CalcProfiles(cur)[:, 0]
+            pf = S.CalcProfiles(cur)
+            prof += tau * pf[:, 0]
+            full += tau * pf
             wsum += tau
         if it % 10 == 9:  # the reference driver's CFL control (staggered/main.cpp:361-370)
             cfl = S.CalcCFL(cur, tau, 3)
@@ -173,7 +188,35 @@ def run_les(args, model, params, vel0, r, rz, log):
     S.close()
     log(f"LES {args.nx // r}x{args.nz // rz}x{args.ny // r} {model}: Ub {ub:.5f}, {ms:.4f} ms/step "
         f"(with the per-sample profile calls)")
-    return dict(prof=prof / max(wsum, 1e-300), ms_per_step=ms, ub=ub, finite=ok, zz=zz, final_tau=tau)
+    full = full / max(wsum, 1e-300)
+    stress = {"uu": full[:, 3] - full[:, 0] ** 2, "ww": full[:, 5] - full[:, 2] ** 2,
+              "uw": full[:, 7] - full[:, 0] * full[:, 2]}
+    return dict(prof=prof / max(wsum, 1e-300), ms_per_step=ms, ub=ub, finite=ok, zz=zz, final_tau=tau,
+                cells=p["NX"] * p["NY"] * p["NZ"], stress=stress)
+
+
+def summarize(paths: list) -> str:
+    """Markdown table of experiment results (one JSON per run): per LES grid and model the
+    mean-u error and the resolved-stress errors against the filtered DNS, and the cost."""
+    rows = ["| run | LES grid | model | mean u rel. L2 | <u'u'> | <w'w'> | <u'w'> | ms/step | ns/cell-step |",
+            "|---|---|---|---:|---:|---:|---:|---:|---:|"]
+    agg = {}
+    for path in paths:
+        with open(path) as f:
+            res = json.load(f)
+        run = os.path.basename(path).rsplit(".", 1)[0]
+        for case in res["cases"]:
+            g = "x".join(str(v) for v in case["les_grid"])
+            for model, r in case["les"].items():
+                st = r.get("stress_rel_l2_err", {})
+                rows.append(f"| {run} | {g} | {model} | {r['rel_l2_err_mean_u']:.2%} | {st.get('uu', float('nan')):.1%} "
+                            f"| {st.get('ww', float('nan')):.1%} | {st.get('uw', float('nan')):.1%} | "
+                            f"{r['ms_per_step']:.3f} | {r.get('ns_per_cell_step', float('nan')):.3f} |")
+                agg.setdefault((g, model), []).append(r["rel_l2_err_mean_u"])
+    rows += ["", "| LES grid | model | mean u rel. L2: mean over runs | min | max | runs |", "|---|---|---:|---:|---:|---:|"]
+    for (g, model), v in sorted(agg.items()):
+        rows.append(f"| {g} | {model} | {np.mean(v):.2%} | {np.min(v):.2%} | {np.max(v):.2%} | {len(v)} |")
+    return "\n".join(rows)
 
 
 def main():
@@ -211,7 +254,11 @@ def main():
                     help="directory for the box-filtered snapshots (float32 .npy, fields u, v, w, p, uu, vv, ww, uv, "
                          "uw, vw on the first LES grid of --coarsen)")
     ap.add_argument("--out", default="les_experiment.json")
+    ap.add_argument("--summary", nargs="+", metavar="JSON", help="print the markdown summary of finished runs")
     args = ap.parse_args()
+    if args.summary:
+        print(summarize(args.summary))
+        return
     if args.snap_dir:
         os.makedirs(args.snap_dir, exist_ok=True)
     t_start = time.time()
@@ -250,7 +297,11 @@ def main():
         # filtered-DNS mean u profile on the LES cells (dz-weighted average of rz DNS cells)
         wz = dz.reshape(-1, rz)
         ref = (dns["prof"].reshape(-1, rz) * wz).sum(axis=1) / wz.sum(axis=1)
+        fs = dns["fstat"][(r, rz)]  # filtered DNS: resolved <u'u'>, <w'w'>, <u'w'> per LES plane
+        fref = {"uu": fs[:, 3] - fs[:, 0] ** 2, "ww": fs[:, 4] - fs[:, 2] ** 2, "uw": fs[:, 5] - fs[:, 0] * fs[:, 2]}
         case = {"les_grid": [args.nx // r, args.nz // rz, args.ny // r], "filter": [r, rz, r],
+                "snapshots": dns["snapshots"],
+                "filtered_dns_stress": {k: v.tolist() for k, v in fref.items()},
                 "training": {"samples": int(len(Y)), "epochs": args.epochs, "loss_first": float(losses[0]),
                              "loss_last": float(losses[-1]), "heldout_mse": val_mse, "heldout_mse_no_model": zero_mse},
                 "filtered_dns_mean_u": ref.tolist(), "les": {}}
@@ -259,7 +310,11 @@ def main():
             err = out["prof"] - ref
             case["les"][model] = {"rel_l2_err_mean_u": float(np.linalg.norm(err) / np.linalg.norm(ref)),
                                   "max_err_mean_u": float(np.max(np.abs(err))), "ms_per_step": out["ms_per_step"],
-                                  "bulk_velocity": out["ub"], "finite": out["finite"], "mean_u": out["prof"].tolist()}
+                                  "bulk_velocity": out["ub"], "finite": out["finite"], "mean_u": out["prof"].tolist(),
+                                  "ns_per_cell_step": out["ms_per_step"] * 1e6 / out["cells"],
+                                  "stress_rel_l2_err": {k: float(np.linalg.norm(out["stress"][k] - fref[k]) /
+                                                                 max(np.linalg.norm(fref[k]), 1e-300))
+                                                        for k in fref}}
             log(f"  {model}: rel L2 error of the mean u profile {case['les'][model]['rel_l2_err_mean_u']:.4f}")
         res["cases"].append(case)
     with open(args.out, "w") as f:
