@@ -250,179 +250,6 @@ static void xfft_reg_launch(const DivFftArgs<T>& a, const T* src, int rows, cuda
     k<<<dim3(a.g.NY / rows, a.g.NZ), 256, smem, s>>>(a, src, rows, lr);
 }
 
-// ---------------------------------------------------------------------------
-// divergence fused with the forward x-FFT
-// ---------------------------------------------------------------------------
-// Divergence (times the cell height) of four x-adjacent cells x..x+3 of row y, plane z,
-// read straight from the vector RHS: the arithmetic of k_div_quad_z (HW2
-// staggered/func_global.h:306-312, VV4 :325-333, collocated collocated_AB3/func_global.h:
-// 310-325), the w planes loaded for this plane alone.
-template <typename T, int SCHEME>
-__device__ __forceinline__ void div_quad_at(const DivFftArgs<T>& a, int z, int y, int x, T d[4]) {
-    const Geom& g = a.g;
-    const int NX = g.NX, NY = g.NY, NZ = g.NZ;
-    const size_t NXY = (size_t)NX * NY, col = (size_t)y * NX + x;
-    const T *u = a.v.c[0], *v = a.v.c[1], *w = a.v.c[2];
-    const T ihx = (T)g.inv_hx, ihy = (T)g.inv_hy;
-    const int xq = x + 4 == NX ? 0 : x + 4, xm = x == 0 ? NX - 1 : x - 1;
-    const int yp = y + 1 == NY ? 0 : y + 1, ym = y == 0 ? NY - 1 : y - 1;
-    const int ypp = yp + 1 == NY ? 0 : yp + 1;
-    auto ldw = [&](int zz) {
-        Acc4<T> r;
-        if (zz >= 0 && zz < NZ) r = ld4(w + (size_t)zz * NXY + col);
-        else
-#pragma unroll
-            for (int k = 0; k < 4; k++) r.v[k] = T(0);
-        return r;
-    };
-    const size_t pl = (size_t)z * NXY, rb = pl + (size_t)y * NX, id = rb + x;
-    T e[9];  // u at x-1 .. x+7
-    {
-        const Acc4<T> U0 = ld4(u + id), U1 = ld4(u + rb + xq);
-        e[0] = __ldg(u + rb + xm);
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-            e[1 + k] = U0.v[k];
-            e[5 + k] = U1.v[k];
-        }
-    }
-    if constexpr (SCHEME == TC_SCHEME_VV4) {
-        const T C27 = T(0.03703703703703703703);
-        const T dz = a.m.DZ[z], dzw = a.m.DZW[z];
-        const Acc4<T> V0 = ld4(v + id), Vp = ld4(v + pl + (size_t)yp * NX + x),
-                      Vpp = ld4(v + pl + (size_t)ypp * NX + x), Vm = ld4(v + pl + (size_t)ym * NX + x);
-        const Acc4<T> Wm = ldw(z - 1), W0v = ldw(z), Wp = ldw(z + 1), Wpp = ldw(z + 2);
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-            const T W0 = W0v.v[k];
-            const T Wr = z == NZ - 1 ? T(0) : Wp.v[k];
-            const T Wrr = z == NZ - 1 ? W0 : (z == NZ - 2 ? T(0) : Wpp.v[k]);
-            const T Wll = z == 0 ? Wp.v[k] : (z == 1 ? T(0) : Wm.v[k]);
-            const T dudx = ihx * (dz * (e[k + 2] - e[k + 1]) - C27 * dzw * (e[k + 3] - e[k]));
-            const T dvdy = ihy * (dz * (Vp.v[k] - V0.v[k]) - C27 * dzw * (Vpp.v[k] - Vm.v[k]));
-            d[k] = dudx + dvdy + (Wr - W0) - C27 * (Wrr - Wll);
-        }
-    } else if constexpr (SCHEME == TC_SCHEME_HW2) {
-        const T hz = a.m.DZ[z];
-        const Acc4<T> V0 = ld4(v + id), Vp = ld4(v + pl + (size_t)yp * NX + x);
-        const Acc4<T> W0v = ldw(z), Wp = ldw(z + 1);
-#pragma unroll
-        for (int k = 0; k < 4; k++)
-            d[k] = (e[k + 2] - e[k + 1]) * ihx * hz + (Vp.v[k] - V0.v[k]) * ihy * hz +
-                   ((z < NZ - 1) ? (Wp.v[k] - W0v.v[k]) : (-W0v.v[k]));
-    } else {
-        const T hz = a.m.cellh[z], hx = (T)g.hx, hy = (T)g.hy;
-        const Acc4<T> Vp = ld4(v + pl + (size_t)yp * NX + x), Vm = ld4(v + pl + (size_t)ym * NX + x);
-        const Acc4<T> Wm = ldw(z - 1), W0v = ldw(z), Wp = ldw(z + 1);
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-            const T Wa = z == 0 ? Wp.v[k] : (z == NZ - 1 ? W0v.v[k] : Wp.v[k]);
-            const T Wb = z == 0 ? W0v.v[k] : Wm.v[k];
-            T dd = 0;
-            dd += T(0.5) * (e[k + 2] - e[k]) * hy * hz;
-            dd += T(0.5) * (Vp.v[k] - Vm.v[k]) * hx * hz;
-            dd += T(0.5) * (Wa - Wb) * hx * hy;
-            d[k] = dd;
-        }
-    }
-}
-
-// One CTA takes RB y-rows and marches a chunk of z-planes.  Per plane: the divergence of
-// its rows into a shared-memory tile D (coalesced 16-byte row loads of u, v, w, as
-// k_div_quad_z), then the forward real x-FFT of the tile (two rows per complex line, the
-// two-pass register transform of k_xfft_reg reading D instead of global memory), unpacked
-// to spec[z][kx][y].  Against the divergence kernel followed by k_xfft_reg this drops the
-// divergence field's write and re-read (2 words per cell).  The transformed lines reuse
-// D's memory (D is dead after the first pass).
-constexpr int DIVX_NT = 256;
-template <typename T, int N>
-struct DivxShape {
-    static constexpr int RB = sizeof(T) == 4 ? 16 : 8;           // rows per CTA
-    static constexpr int DS = N + (sizeof(T) == 4 ? 12 : 6);     // row stride of D (bank spread, 16-byte rows)
-    static constexpr int NL = RB / 2, ZS = N + 1;
-    static constexpr size_t d_bytes = (size_t)RB * DS * sizeof(T);
-    static constexpr size_t z_bytes = (size_t)NL * ZS * sizeof(cplx<T>);
-    static constexpr size_t smem = (d_bytes > z_bytes ? d_bytes : z_bytes) + (size_t)NL * FftSplit<N>::YL * sizeof(cplx<T>);
-};
-
-template <typename T, int N, int SCHEME>
-__global__ void __launch_bounds__(DIVX_NT) k_divx_reg(DivFftArgs<T> a, int tz) {
-    using SH = DivxShape<T, N>;
-    constexpr int RB = SH::RB, DS = SH::DS, NL = SH::NL, ZS = SH::ZS;
-    constexpr int N1 = FftSplit<N>::N1, N2 = FftSplit<N>::N2, YL = FftSplit<N>::YL, NXH = N / 2 + 1;
-    static_assert(SH::d_bytes % 16 == 0, "16-byte aligned tiles");
-    extern __shared__ __align__(16) unsigned char smraw[];
-    T* D = reinterpret_cast<T*>(smraw);                                                   // [RB][DS]
-    cplx<T>* Zs = reinterpret_cast<cplx<T>*>(smraw);                                      // [NL][ZS], over D
-    cplx<T>* Y = reinterpret_cast<cplx<T>*>(smraw + (SH::d_bytes > SH::z_bytes ? SH::d_bytes : SH::z_bytes));
-    const Geom& g = a.g;
-    const int NY = g.NY, NZ = g.NZ;
-    const int y0 = blockIdx.x * RB, zb = blockIdx.y * tz, ze = min(NZ, zb + tz);
-    for (int z = zb; z < ze; z++) {
-#pragma unroll 2
-        for (int it = threadIdx.x; it < RB * (N / 4); it += DIVX_NT) {
-            const int r = it / (N / 4), x = (it - r * (N / 4)) * 4;
-            T d[4];
-            div_quad_at<T, SCHEME>(a, z, y0 + r, x, d);
-            T* dst = D + r * DS + x;
-            if constexpr (sizeof(T) == 4) {
-                *reinterpret_cast<float4*>(dst) = make_float4(d[0], d[1], d[2], d[3]);
-            } else {
-                reinterpret_cast<double2*>(dst)[0] = make_double2(d[0], d[1]);
-                reinterpret_cast<double2*>(dst)[1] = make_double2(d[2], d[3]);
-            }
-        }
-        __syncthreads();
-        for (int it = threadIdx.x; it < NL * N2; it += DIVX_NT) {
-            const int l = it / N2, n2 = it - l * N2;
-            const T* d0 = D + (2 * l) * DS + n2;
-            cplx<T> v[N1];
-#pragma unroll
-            for (int n1 = 0; n1 < N1; n1++) v[n1] = {d0[n1 * N2], d0[DS + n1 * N2]};
-            fft_pass_a<T, N, -1>(v, n2, a.twx, Y + l * YL);
-        }
-        __syncthreads();
-        for (int it = threadIdx.x; it < NL * N1; it += DIVX_NT) {
-            const int l = it / N1, k1 = it - l * N1;
-            cplx<T> v[N2];
-            fft_pass_b<T, N, -1>(v, k1, Y + l * YL);
-            cplx<T>* zl = Zs + l * ZS + k1;
-#pragma unroll
-            for (int k2 = 0; k2 < N2; k2++) zl[k2 * N1] = v[k2];
-        }
-        __syncthreads();
-        // unpack the two real rows of each line (as k_xfft_reg)
-        for (int e = threadIdx.x; e < NXH * RB; e += DIVX_NT) {
-            const int kx = e / RB, r = e % RB, l = r >> 1;
-            const cplx<T> Zk = Zs[l * ZS + kx], Zm = Zs[l * ZS + (kx == 0 ? 0 : N - kx)];
-            cplx<T> val;
-            if ((r & 1) == 0) val = {T(0.5) * (Zk.x + Zm.x), T(0.5) * (Zk.y - Zm.y)};
-            else val = {T(0.5) * (Zk.y + Zm.y), -T(0.5) * (Zk.x - Zm.x)};
-            a.spec[((size_t)z * NXH + kx) * NY + y0 + r] = val;
-        }
-        __syncthreads();  // D / Zs and Y are rewritten by the next plane
-    }
-}
-
-template <typename T, int N>
-static bool divx_launch(const DivFftArgs<T>& a, cudaStream_t s) {
-    using SH = DivxShape<T, N>;
-    if (a.g.NY % SH::RB != 0) return false;
-    auto k = a.g.scheme == TC_SCHEME_VV4 ? k_divx_reg<T, N, TC_SCHEME_VV4>
-             : a.g.scheme == TC_SCHEME_HW2 ? k_divx_reg<T, N, TC_SCHEME_HW2> : k_divx_reg<T, N, TC_SCHEME_COLLOC>;
-    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SH::smem);
-    int dev = 0, sms = 148, occ = 1;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, DIVX_NT, SH::smem);
-    // z-chunks: about one wave of resident CTAs over the y-blocks
-    const int yb = a.g.NY / SH::RB;
-    const int nch = std::max(1, std::min(a.g.NZ, sms * std::max(1, occ) / yb));
-    const int tz = (a.g.NZ + nch - 1) / nch;
-    k<<<dim3(yb, (a.g.NZ + tz - 1) / tz), DIVX_NT, SH::smem, s>>>(a, tz);
-    return true;
-}
-
 constexpr int DIV_ZC = 4;  // planes per thread of k_div_quad_z
 template <typename T>
 static void div_quad_launch(const DivFftArgs<T>& a, T* out, cudaStream_t s) {
@@ -583,7 +410,6 @@ int launch_div_xfft_reg(const DivFftArgs<T>& a, cudaStream_t s) {
     case n: {                                                \
         const int rows = xfft_reg_rows<T, n>(a.g.NY, false); \
         if (!rows) return 0;                                 \
-        if (vec && divx_launch<T, n>(a, s)) return 1;        \
         if (vec) div_quad_launch<T>(a, a.dtmp, s);           \
         xfft_reg_launch<T, n>(a, vec ? a.dtmp : a.src_scalar, rows, s); \
         return vec ? 2 : 1;                                  \

@@ -638,12 +638,8 @@ void launch_zfactor(const ZSolveArgs<T>& a, cudaStream_t s) {
 // (kx, kh), (kx, NY-kh) that share their factors, so a warp's factor loads fetch each
 // factor row once (two lanes, one address).  Rows are moved R at a time through two
 // register batches: the loads of batch b+1 are issued before batch b is consumed.
-#ifndef ZSOLVE_MPT
-#define ZSOLVE_MPT 1  // modes per thread of k_zsolve_fac
-#endif
-
 template <typename T, int SCHEME>
-__device__ __forceinline__ void zsolve_fac_mode(const ZSolveArgs<T>& a, size_t t) {
+__global__ void __launch_bounds__(128) k_zsolve_fac(ZSolveArgs<T> a) {
     constexpr bool VV = SCHEME == TC_SCHEME_VV4;
     constexpr int R = sizeof(T) == 4 ? 8 : 4;
     using FQ = typename std::conditional<VV, Q4<T>, Q2<T>>::type;
@@ -651,6 +647,7 @@ __device__ __forceinline__ void zsolve_fac_mode(const ZSolveArgs<T>& a, size_t t
     const Geom& g = a.g;
     const int NY = g.NY, NYH1 = NY / 2 + 1;
     const size_t M = (size_t)g.NXH * NY, MH = (size_t)g.NXH * NYH1;
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     const size_t mh = t >> 1;
     if (mh >= MH) return;
     const int kx = (int)(mh / NYH1), kh = (int)(mh - (size_t)kx * NYH1);
@@ -745,15 +742,6 @@ __device__ __forceinline__ void zsolve_fac_mode(const ZSolveArgs<T>& a, size_t t
             run(i0 - R, zb, bb);
         }
     }
-}
-
-// Thread t solves modes t, t + T, ..., t + (mpt - 1) T (T threads in all): with mpt > 1
-// fewer modes are in flight at a time, so less of the forward sweep's output leaves L2
-// before the backward sweep reads it back.  Lanes t, t^1 stay partners (T is even).
-template <typename T, int SCHEME>
-__global__ void __launch_bounds__(128) k_zsolve_fac(ZSolveArgs<T> a, int mpt) {
-    const size_t nt = (size_t)gridDim.x * blockDim.x;
-    for (int k = 0; k < mpt; k++) zsolve_fac_mode<T, SCHEME>(a, (size_t)blockIdx.x * blockDim.x + threadIdx.x + k * nt);
 }
 
 // The low-|k| modes (kx < LM, |ky| < LM) in double from their double factors; mode
@@ -913,8 +901,7 @@ static void zsolve_fac_scheme(const ZSolveArgs<T>& a, cudaStream_t s, cudaStream
     zsolve_low_scheme<T, SCHEME>(a, side);
     cudaEventRecord(join, side);
     const size_t MH = (size_t)a.g.NXH * (a.g.NY / 2 + 1);
-    const size_t nb = (2 * MH + 128 * ZSOLVE_MPT - 1) / (128 * ZSOLVE_MPT);
-    k_zsolve_fac<T, SCHEME><<<(unsigned)nb, 128, 0, s>>>(a, ZSOLVE_MPT);
+    k_zsolve_fac<T, SCHEME><<<(unsigned)((2 * MH + 127) / 128), 128, 0, s>>>(a);
     cudaStreamWaitEvent(s, join, 0);
 }
 
