@@ -5,8 +5,8 @@ variant of the step path.
 Tolerances (relative to the max-norm of the oracle result):
   FP64 : single operators 1e-12, six SBDF steps 1e-10 (differences are round-off
          from FMA contraction, FFT ordering and summation order);
-  MIXED: float storage/stencils/FFTs against the FP64 oracle, 2e-5 per operator and
-         2e-4 after six steps.
+  MIXED: float storage/stencils/FFTs against the FP64 oracle, per check about 3x the
+         largest error measured on a B200 (the MIXED table below).
 """
 import numpy as np
 import pytest
@@ -29,6 +29,22 @@ CASES = {
 }
 
 TOL = {0: dict(op=1e-12, step=1e-10), 1: dict(op=2e-5, step=2e-4)}
+# Mixed precision (float storage, stencils and FFTs against the FP64 oracle): each check's
+# tolerance is about 3x the largest error measured over the cases on a B200 (recorded with
+# TC_ERROR_LOG; e.g. six steps: velocity 9.6e-7, pressure 1.47e-3, flux history 2.9e-5).
+MIXED = {
+    "op/div": 4e-7, "op/grad": 5e-7, "op/explicit": 6e-7, "op/unapply": 2e-6, "op/psolve": 1.5e-6,
+    "op/nu_t": 1.5e-6,
+    "step/vel": 3e-6, "step/pres": 4.5e-3, "step/flux": 1e-4, "step/integral": 1e-6, "step/cfl": 1.2e-6,
+    "step/profiles": 2e-6, "step/ke": 2e-6,
+    "config1/vel": 1.5e-5, "config1/pres": 3.5e-3, "config1/ke": 6e-6,
+    "full/vel": 2e-6, "full/pres": 7.5e-4,
+}
+
+
+def tol_for(check, precision, fp64_tol):
+    """FP64: the given tolerance; mixed: the measured-error-based value of MIXED."""
+    return fp64_tol if precision == 0 else MIXED[check]
 
 
 def _pair(name, precision):
@@ -58,12 +74,14 @@ def test_operators(name, precision):
         S.set_nu_t(nt)
         O.set_nu_t(nt)
     L = f"op/{name}/p{precision}"
-    assert within(L + "/explicit", rel_err(S.ExplicitTerm(v), O.explicit_term(v)), tol * 10)
-    assert within(L + "/grad", rel_err(S.ApplyGradient(p), O.apply_gradient(p)), tol)
-    assert within(L + "/div", rel_err(S.ApplyDivergence(v), O.apply_divergence(v)), tol)
-    assert within(L + "/unapply", rel_err(S.UnapplyGradient(v), O.unapply_gradient(v)), tol * 10)
+    assert within(L + "/explicit", rel_err(S.ExplicitTerm(v), O.explicit_term(v)), tol_for("op/explicit", precision, tol * 10))
+    assert within(L + "/grad", rel_err(S.ApplyGradient(p), O.apply_gradient(p)), tol_for("op/grad", precision, tol))
+    assert within(L + "/div", rel_err(S.ApplyDivergence(v), O.apply_divergence(v)), tol_for("op/div", precision, tol))
+    assert within(L + "/unapply", rel_err(S.UnapplyGradient(v), O.unapply_gradient(v)),
+                  tol_for("op/unapply", precision, tol * 10))
     rhs = O.apply_divergence(v)
-    assert within(L + "/psolve", rel_err(S.LinearSystemSolveFFT(rhs), O.pressure_solve(rhs)), tol * 10)
+    assert within(L + "/psolve", rel_err(S.LinearSystemSolveFFT(rhs), O.pressure_solve(rhs)),
+                  tol_for("op/psolve", precision, tol * 10))
     if CASES[name].get("turb"):
         vs = 0.3 * seeded_field(S.N, NXY, seed=9, wall_w_zero=not coll)
         got = S.RecalcTurbVisc(vs)
@@ -71,7 +89,7 @@ def test_operators(name, precision):
         want = O.get_nu_t()
         if coll:  # elements of the top node plane are not defined
             got, want = got[:-NXY], want[:-NXY]
-        assert within(L + "/nu_t", rel_err(got, want), tol * 10)
+        assert within(L + "/nu_t", rel_err(got, want), tol_for("op/nu_t", precision, tol * 10))
 
 
 def _run_steps(S, O, nsteps, tau, cfr=None):
@@ -100,17 +118,18 @@ def test_steps(name, precision):
     vs, ps = S.download_level(cur)
     vo, po = O.get_level(cur)
     L = f"step/{name}/p{precision}"
-    assert within(L + "/vel", rel_err(vs, vo), tol)
-    assert within(L + "/pres", rel_err(ps, po), tol * 20)
+    assert within(L + "/vel", rel_err(vs, vo), tol_for("step/vel", precision, tol))
+    assert within(L + "/pres", rel_err(ps, po), tol_for("step/pres", precision, tol * 20))
     # flux history used by the next step
     for lvl in range(4):
-        assert within(L + "/flux", rel_err(S.download_flux(lvl), O.get_flux(lvl)), tol * 20)
+        assert within(L + "/flux", rel_err(S.download_flux(lvl), O.get_flux(lvl)), tol_for("step/flux", precision, tol * 20))
     # diagnostics
     I, cfl, prof = S.diagnostics(cur, tau)
-    assert within(L + "/integral", rel_err(I, O.integral(cur)), tol * 10)
-    assert within(L + "/cfl", abs(cfl - O.cfl(cur, tau)) / O.cfl(cur, tau), tol * 10)
-    assert within(L + "/profiles", rel_err(prof, O.profiles(cur)), tol * 10)
-    assert within(L + "/ke", abs(S.CalcKineticEnergy(cur) - O.kinetic_energy(cur)) / O.kinetic_energy(cur), tol * 10)
+    assert within(L + "/integral", rel_err(I, O.integral(cur)), tol_for("step/integral", precision, tol * 10))
+    assert within(L + "/cfl", abs(cfl - O.cfl(cur, tau)) / O.cfl(cur, tau), tol_for("step/cfl", precision, tol * 10))
+    assert within(L + "/profiles", rel_err(prof, O.profiles(cur)), tol_for("step/profiles", precision, tol * 10))
+    assert within(L + "/ke", abs(S.CalcKineticEnergy(cur) - O.kinetic_energy(cur)) / O.kinetic_energy(cur),
+                  tol_for("step/ke", precision, tol * 10))
 
 
 @pytest.mark.parametrize("name", ["hw2_dns", "vv4_les", "coll_gal_stab1"])
@@ -339,7 +358,8 @@ def test_config1_hundred_steps_match_oracle(precision):
     4 pi x 2 x 4/3 pi, Re_b 5600, tanh 1.8, dt 0.002, constant flow rate, 100 steps from
     the seeded field, against the FP64 oracle. FP64: 1e-9 relative on the fields after
     100 steps (round-off of FMA contraction and summation order, grown over the run);
-    mixed: 2e-3 on the velocity, 5e-2 on the pressure (float storage over 100 steps)."""
+    mixed: 1.5e-5 on the velocity, 3.5e-3 on the pressure (about 3x the measured errors
+    of float storage over 100 steps)."""
     import oracle_py as op
     import turbchannel_b200 as tb
 
@@ -361,11 +381,11 @@ def test_config1_hundred_steps_match_oracle(precision):
         cur = (cur + 1) % 4
     vs, ps = S.download_level(cur)
     vo, po = O.get_level(cur)
-    tv, tp = (1e-9, 1e-9) if precision == 0 else (2e-3, 5e-2)
+    tv, tp, tk = (1e-9, 1e-9, 1e-9) if precision == 0 else (MIXED["config1/vel"], MIXED["config1/pres"], MIXED["config1/ke"])
     L = f"config1/p{precision}"
     assert within(L + "/vel", rel_err(vs, vo), tv), rel_err(vs, vo)
     assert within(L + "/pres", rel_err(ps, po), tp), rel_err(ps, po)
-    assert within(L + "/ke", abs(S.CalcKineticEnergy(cur) - O.kinetic_energy(cur)) / O.kinetic_energy(cur), tv)
+    assert within(L + "/ke", abs(S.CalcKineticEnergy(cur) - O.kinetic_energy(cur)) / O.kinetic_energy(cur), tk)
     S.close()
 
 
@@ -384,7 +404,7 @@ FULL_SIZE = {
 def test_full_size_configurations_match_oracle(name, precision):
     """The flow configurations at their full sizes, three SBDF steps (orders 1, 2, 3) from
     the seeded field with constant flow rate, against the FP64 oracle: 1e-10 (FP64) /
-    2e-4 (mixed) relative on the velocity, 20x that on the pressure."""
+    the mixed tolerances of the MIXED table (2e-6 velocity, 7.5e-4 pressure)."""
     import oracle_py as op
     import turbchannel_b200 as tb
 
@@ -409,8 +429,8 @@ def test_full_size_configurations_match_oracle(name, precision):
     vs, ps = S.download_level(cur)
     vo, po = O.get_level(cur)
     L = f"full/{name}/p{precision}"
-    assert within(L + "/vel", rel_err(vs, vo), tol), rel_err(vs, vo)
-    assert within(L + "/pres", rel_err(ps, po), 20 * tol), rel_err(ps, po)
+    assert within(L + "/vel", rel_err(vs, vo), tol_for("full/vel", precision, tol)), rel_err(vs, vo)
+    assert within(L + "/pres", rel_err(ps, po), tol_for("full/pres", precision, 20 * tol)), rel_err(ps, po)
     S.close()
 
 
