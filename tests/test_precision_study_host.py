@@ -58,6 +58,17 @@ def test_report_renders():
         w = {k: (v.tolist() if isinstance(v, np.ndarray) else v) for k, v in d.items()}
         runs.append({"name": f"{name}_seed{seed}", "seed": seed, "steps": 10, "wall_ms_per_step": 1.0,
                      "windows": {"5": w, "10": w}})
-    txt = ps.report(None, {"kind": "long", "runs": runs, "windows": [5], "stat_steps": 10, "dt": 8e-4,
-                           "spinup": [1, 1]})
+    long_res = {"kind": "long", "runs": runs, "windows": [5], "stat_steps": 10, "dt": 8e-4, "dt_transition": 6e-4,
+                "spinup": [1, 1], "grid": [8, 8, NZ], "stat_every": 1}
+    txt = ps.report(None, long_res)
     assert "mixed_seed1 vs fp64_seed1" in txt and "fp64_seed2 vs fp64_seed1" in txt
+    assert "mixed_pooled vs fp64_pooled" in txt
+
+    # the JSON summary carries the same comparisons, rounded, for both windows
+    sm = ps._round(ps.summary(None, long_res))
+    assert set(sm["long"]["windows"]) == {"5", "10"}
+    pr = sm["long"]["windows"]["10"]["pairs"]
+    assert set(pr) == {"mixed_seed1 vs fp64_seed1", "mixed_seed2 vs fp64_seed2", "fp64_seed2 vs fp64_seed1",
+                       "mixed_seed2 vs mixed_seed1", "mixed_pooled vs fp64_pooled"}
+    assert abs(pr["mixed_seed1 vs fp64_seed1"]["U"]["max_rel"] - 0.001) < 1e-6
+    assert sm["long"]["failed"] == {}

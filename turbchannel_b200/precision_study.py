@@ -208,6 +208,73 @@ def pooled(ws: list) -> dict:
     return out
 
 
+def _pairs(long_res: dict) -> tuple[list, list]:
+    """The compared pairs: mixed against FP64 per seed, seed against seed per precision, and
+    the seeds' pooled statistics mixed against FP64."""
+    seeds = sorted({r["seed"] for r in long_res["runs"]})
+    pairs = [(f"mixed_seed{s}", f"fp64_seed{s}") for s in seeds]
+    if len(seeds) > 1:
+        pairs += [(f"fp64_seed{seeds[1]}", f"fp64_seed{seeds[0]}"),
+                  (f"mixed_seed{seeds[1]}", f"mixed_seed{seeds[0]}"),
+                  ("mixed_pooled", "fp64_pooled")]
+    return seeds, pairs
+
+
+def _window_stats(long_res: dict, w: str, seeds: list) -> dict:
+    runs = {r["name"]: r for r in long_res["runs"] if "failed" not in r}
+    wstats = {n: r["windows"][w] for n, r in runs.items()}
+    if len(seeds) > 1 and all(f"{k}_seed{s}" in runs for k in ("fp64", "mixed") for s in seeds):
+        for k in ("fp64", "mixed"):  # the seeds' statistics averaged: half the sampling variance
+            wstats[f"{k}_pooled"] = pooled([wstats[f"{k}_seed{s}"] for s in seeds])
+    return wstats
+
+
+def _windows(long_res: dict) -> list:
+    wins = long_res.get("windows", [long_res.get("window")])
+    return sorted({*(str(x) for x in wins if x), str(long_res["stat_steps"])}, key=int)
+
+
+def summary(short_res: dict | None, long_res: dict | None) -> dict:
+    """The report's numbers as a compact dict (no profiles): per window and pair the relative
+    differences of compare(), per run Re_tau and the centre velocity, and the short study's
+    field errors."""
+    out = {}
+    if short_res:
+        out["short"] = {"grid": short_res["grid"], "dt": short_res["dt"],
+                        "records": [{**{k: r[k] for k in ("steps", "u", "v", "w", "p", "Ub", "KE", "CFL")},
+                                     # V, W, uv, vw average to zero: a difference relative to them says nothing
+                                     "profiles": {k: v for k, v in r["profiles"].items()
+                                                  if k in ("U", "uu", "vv", "ww", "uw", "P", "pp")}}
+                                    for r in short_res["records"]]}
+    if long_res:
+        seeds, pairs = _pairs(long_res)
+        L = {k: long_res[k] for k in ("grid", "dt", "dt_transition", "spinup", "stat_steps", "stat_every")}
+        L["windows"] = {}
+        for w in _windows(long_res):
+            ws = _window_stats(long_res, w, seeds)
+            L["windows"][w] = {
+                "pairs": {f"{a} vs {b}": compare(ws[a], ws[b]) for a, b in pairs if a in ws and b in ws},
+                "runs": {r["name"]: {"Re_tau": r["windows"][w]["Re_tau"],
+                                     "Re_tau_walls": r["windows"][w]["Re_tau_walls"],
+                                     "U_centre": float(np.asarray(r["windows"][w]["U"])[len(r["windows"][w]["U"]) // 2]),
+                                     "steps": r["steps"], "wall_ms_per_step": r["wall_ms_per_step"]}
+                         for r in long_res["runs"] if "failed" not in r}}
+        L["failed"] = {r["name"]: r["failed"] for r in long_res["runs"] if "failed" in r}
+        out["long"] = L
+    return out
+
+
+def _round(x, digits: int = 4):
+    """x with every float rounded to a few significant digits (the summary is read, not reused)."""
+    if isinstance(x, float):
+        return float(f"{x:.{digits}g}")
+    if isinstance(x, dict):
+        return {k: _round(v, digits) for k, v in x.items()}
+    if isinstance(x, (list, tuple)):
+        return [_round(v, digits) for v in x]
+    return x
+
+
 def report(short_res: dict | None, long_res: dict | None) -> str:
     L = []
     if short_res:
@@ -226,22 +293,13 @@ def report(short_res: dict | None, long_res: dict | None) -> str:
         for r in long_res["runs"]:
             if "failed" in r:
                 L.append(f"Run {r['name']} failed: {r['failed']}\n")
-        seeds = sorted({r["seed"] for r in long_res["runs"]})
-        wins = long_res.get("windows", [long_res.get("window")])
-        for w in sorted({*(str(x) for x in wins if x), str(long_res["stat_steps"])}, key=int):
+        seeds, pairs = _pairs(long_res)
+        for w in _windows(long_res):
             L.append(f"### Statistics over {w} steps at dt {long_res['dt']} (after {sum(long_res['spinup'])} "
                      f"spin-up steps)\n")
             L.append("| pair | mean U max (L2) | u'u' | v'v' | w'w' | u'w' | p_rms | Re_tau |")
             L.append("|---|---|---|---|---|---|---|---:|")
-            pairs = [(f"mixed_seed{s}", f"fp64_seed{s}") for s in seeds]
-            if len(seeds) > 1:
-                pairs += [(f"fp64_seed{seeds[1]}", f"fp64_seed{seeds[0]}"),
-                          (f"mixed_seed{seeds[1]}", f"mixed_seed{seeds[0]}")]
-            wstats = {n: r["windows"][w] for n, r in runs.items()}
-            if len(seeds) > 1 and all(f"{k}_seed{s}" in runs for k in ("fp64", "mixed") for s in seeds):
-                for k in ("fp64", "mixed"):  # the seeds' statistics averaged: half the sampling variance
-                    wstats[f"{k}_pooled"] = pooled([wstats[f"{k}_seed{s}"] for s in seeds])
-                pairs.append(("mixed_pooled", "fp64_pooled"))
+            wstats = _window_stats(long_res, w, seeds)
             for a, b in pairs:
                 if a not in wstats or b not in wstats:
                     continue
@@ -265,7 +323,8 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("mode", choices=["short", "long", "report"])
     ap.add_argument("files", nargs="*", help="report: the short and/or long JSON results")
-    ap.add_argument("--out", default="precision_study.json")
+    ap.add_argument("--out", default="precision_study.json",
+                    help="short/long: the results; report: also write the numbers as JSON here if given")
     ap.add_argument("--grid", type=int, nargs=3, default=list(GRID))
     ap.add_argument("--seed", type=int, default=12345)
     ap.add_argument("--seeds", type=int, nargs="+", default=[12345, 12346])
@@ -281,8 +340,12 @@ def main():
     args = ap.parse_args()
     if args.mode == "report":
         res = [json.load(open(f)) for f in args.files]
-        print(report(next((r for r in res if r["kind"] == "short"), None),
-                     next((r for r in res if r["kind"] == "long"), None)))
+        sr = next((r for r in res if r["kind"] == "short"), None)
+        lr = next((r for r in res if r["kind"] == "long"), None)
+        print(report(sr, lr))
+        if "--out" in sys.argv:
+            with open(args.out, "w") as f:
+                json.dump(_round(summary(sr, lr)), f, separators=(",", ":"))
         return
     res = short(args) if args.mode == "short" else long(args)
     with open(args.out, "w") as f:
