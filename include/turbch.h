@@ -163,6 +163,14 @@ int tc_diagnostics(tc_handle* h, int level, double tau, double integral[3], doub
  * The results agree to round-off (summation order). */
 int tc_set_diag_fusion(tc_handle* h, int mode);
 
+/* How the pressure solve's horizontal FFTs run (no counterpart in the reference, which
+ * calls its FFT library per direction).  mode 1 (default): where (NX, NY) has a plane
+ * kernel that fits the device, the x- and y-FFTs of each z-plane run in one launch, a
+ * thread-block cluster holding the plane's half spectrum in its shared memory; 0: the
+ * separate x- and y-FFT kernels.  The arithmetic is the same (round-off may differ by
+ * FMA contraction). */
+int tc_set_fft_fusion(tc_handle* h, int mode);
+
 /* Segregated IMEX Runge-Kutta step of the collocated scheme (collocated_SRK:
  * data::Step, func_global.h:317-408; method tables as collocated_SRK/imex.h:10-41).
  * The handle must be collocated with cross viscosity and no turbulence model; the

@@ -251,105 +251,12 @@ static void xfft_reg_launch(const DivFftArgs<T>& a, const T* src, int rows, cuda
 }
 
 // ---------------------------------------------------------------------------
-// forward x-FFT, persistent and double-buffered
+// inverse x-FFT, persistent and double-buffered (float)
 // ---------------------------------------------------------------------------
-// The same transform as k_xfft_reg, but each CTA walks tiles of XP_RB rows (one z-plane's
-// rows y0 .. y0+RB-1, a contiguous block of the real field) and copies the next tile into
-// its second buffer with cp.async while it transforms the current one, so every CTA keeps
-// a tile of loads in flight across its transform and store phases.  Rows are stored with a
-// stride of N + pad (bank spread for the first pass's strided reads); the transformed
-// lines reuse the current tile's buffer, dead after the first pass.
 constexpr int XP_NT = 256;
-template <typename T, int N>
-struct XPipe {
-    static constexpr int RB = sizeof(T) == 4 ? 16 : 8, NL = RB / 2, ZS = N + 1;
-    static constexpr int RS = N + (sizeof(T) == 4 ? 12 : 6);  // row stride of a tile (16-byte rows)
-    static constexpr size_t in_bytes = (size_t)RB * RS * sizeof(T), zs_bytes = (size_t)NL * ZS * sizeof(cplx<T>);
-    static constexpr size_t buf = ((in_bytes > zs_bytes ? in_bytes : zs_bytes) + 15) / 16 * 16;
-    static constexpr size_t smem = 2 * buf + (size_t)NL * FftSplit<N>::YL * sizeof(cplx<T>);
-    static constexpr int CH = 16 / sizeof(T), CPR = N / CH;  // 16-byte chunks per row
-};
-
-template <typename T, int N>
-__global__ void __launch_bounds__(XP_NT) k_xfft_pipe(DivFftArgs<T> a, const T* __restrict__ src) {
-    using P = XPipe<T, N>;
-    constexpr int RB = P::RB, NL = P::NL, ZS = P::ZS, RS = P::RS, CH = P::CH, CPR = P::CPR;
-    constexpr int N1 = FftSplit<N>::N1, N2 = FftSplit<N>::N2, YL = FftSplit<N>::YL, NXH = N / 2 + 1;
-    extern __shared__ __align__(16) unsigned char smraw[];
-    cplx<T>* Y = reinterpret_cast<cplx<T>*>(smraw + 2 * P::buf);
-    const Geom& g = a.g;
-    const int NY = g.NY, YB = NY / RB;
-    const long long ntile = (long long)YB * g.NZ;
-    auto fetch = [&](long long t, int b) {
-        const int z = (int)(t / YB), y0 = (int)(t - (long long)z * YB) * RB;
-        const T* base = src + ((size_t)z * NY + y0) * N;
-        T* in = reinterpret_cast<T*>(smraw + b * P::buf);
-        for (int e = threadIdx.x; e < RB * CPR; e += XP_NT) {
-            const int r = e / CPR, c = e - r * CPR;
-            cp_async<16>(in + r * RS + c * CH, base + (size_t)r * N + c * CH);
-        }
-    };
-    long long t = blockIdx.x;
-    if (t < ntile) fetch(t, 0);
-    cp_async_commit();
-    for (int b = 0; t < ntile; t += gridDim.x, b ^= 1) {
-        if (t + gridDim.x < ntile) fetch(t + gridDim.x, b ^ 1);
-        cp_async_commit();
-        cp_async_wait<1>();
-        __syncthreads();  // tile t is in buffer b
-        const int z = (int)(t / YB), y0 = (int)(t - (long long)z * YB) * RB;
-        const T* in = reinterpret_cast<const T*>(smraw + b * P::buf);
-        cplx<T>* Zs = reinterpret_cast<cplx<T>*>(smraw + b * P::buf);  // over the tile, dead after pass A
-        for (int it = threadIdx.x; it < NL * N2; it += XP_NT) {
-            const int l = it / N2, n2 = it - l * N2;
-            const T* d0 = in + (2 * l) * RS + n2;
-            cplx<T> v[N1];
-#pragma unroll
-            for (int n1 = 0; n1 < N1; n1++) v[n1] = {d0[n1 * N2], d0[RS + n1 * N2]};
-            fft_pass_a<T, N, -1>(v, n2, a.twx, Y + l * YL);
-        }
-        __syncthreads();
-        for (int it = threadIdx.x; it < NL * N1; it += XP_NT) {
-            const int l = it / N1, k1 = it - l * N1;
-            cplx<T> v[N2];
-            fft_pass_b<T, N, -1>(v, k1, Y + l * YL);
-            cplx<T>* zl = Zs + l * ZS + k1;
-#pragma unroll
-            for (int k2 = 0; k2 < N2; k2++) zl[k2 * N1] = v[k2];
-        }
-        __syncthreads();
-        // unpack the two real rows of each line (as k_xfft_reg)
-        for (int e = threadIdx.x; e < NXH * RB; e += XP_NT) {
-            const int kx = e / RB, r = e % RB, l = r >> 1;
-            const cplx<T> Zk = Zs[l * ZS + kx], Zm = Zs[l * ZS + (kx == 0 ? 0 : N - kx)];
-            cplx<T> val;
-            if ((r & 1) == 0) val = {T(0.5) * (Zk.x + Zm.x), T(0.5) * (Zk.y - Zm.y)};
-            else val = {T(0.5) * (Zk.y + Zm.y), -T(0.5) * (Zk.x - Zm.x)};
-            a.spec[((size_t)z * NXH + kx) * NY + y0 + r] = val;
-        }
-        __syncthreads();  // buffer b and Y are refilled by the next iterations
-    }
-}
-
-template <typename T, int N>
-static bool xfft_pipe_launch(const DivFftArgs<T>& a, const T* src, cudaStream_t s) {
-    using P = XPipe<T, N>;
-    if (a.g.NY % P::RB != 0 || N % P::CH != 0) return false;
-    auto k = k_xfft_pipe<T, N>;
-    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P::smem);
-    int dev = 0, sms = 148, occ = 1;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, XP_NT, P::smem);
-    const long long ntile = (long long)(a.g.NY / P::RB) * a.g.NZ;
-    const int grid = (int)std::min<long long>(ntile, (long long)sms * std::max(1, occ));
-    k<<<grid, XP_NT, P::smem, s>>>(a, src);
-    return true;
-}
-
-// Inverse x-FFT, persistent and double-buffered: as k_ixfft_reg (the Hermitian-extended
+// As k_ixfft_reg (the Hermitian-extended
 // half spectrum of two rows per complex line, inverse transform, scaled rows into p), with
-// each CTA walking tiles of IP_RB y-values of one plane and copying the next tile's half
+// each CTA walking tiles of RB (16) y-values of one plane and copying the next tile's half
 // spectrum (NX/2+1 rows of RB contiguous values) into its second buffer while it
 // transforms the current one.
 template <typename T, int N>
@@ -429,18 +336,31 @@ __global__ void __launch_bounds__(XP_NT) k_ixfft_pipe(IxFftArgs<T> a) {
 
 template <typename T, int N>
 static bool ixfft_pipe_launch(const IxFftArgs<T>& a, cudaStream_t s) {
-    using P = IPipe<T, N>;
-    if (a.g.NY % P::RB != 0) return false;
-    auto k = k_ixfft_pipe<T, N>;
-    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P::smem);
-    int dev = 0, sms = 148, occ = 1;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, XP_NT, P::smem);
-    const long long ntile = (long long)(a.g.NY / P::RB) * a.g.NZ;
-    const int grid = (int)std::min<long long>(ntile, (long long)sms * std::max(1, occ));
-    k<<<grid, XP_NT, P::smem, s>>>(a);
-    return true;
+    // float only: in double the tiles halve and the k_ixfft_reg form measured faster
+    if constexpr (sizeof(T) != 4) {
+        return false;
+    } else {
+        using P = IPipe<T, N>;
+        if (a.g.NY % P::RB != 0) return false;
+        auto k = k_ixfft_pipe<T, N>;
+        static int sms = 0, occ = -1;  // per size, resolved at the first launch
+        if (occ < 0) {
+            int dev = 0, optin = 0, o = 0;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+            if (P::smem <= (size_t)optin) {
+                cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P::smem);
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k, XP_NT, P::smem);
+            }
+            occ = o;
+        }
+        if (occ < 1) return false;
+        const long long ntile = (long long)(a.g.NY / P::RB) * a.g.NZ;
+        const int grid = (int)std::min<long long>(ntile, (long long)sms * occ);
+        k<<<grid, XP_NT, P::smem, s>>>(a);
+        return true;
+    }
 }
 
 constexpr int DIV_ZC = 4;  // planes per thread of k_div_quad_z
@@ -604,8 +524,7 @@ int launch_div_xfft_reg(const DivFftArgs<T>& a, cudaStream_t s) {
         const int rows = xfft_reg_rows<T, n>(a.g.NY, false); \
         if (!rows) return 0;                                 \
         if (vec) div_quad_launch<T>(a, a.dtmp, s);           \
-        if (!xfft_pipe_launch<T, n>(a, vec ? a.dtmp : a.src_scalar, s)) \
-            xfft_reg_launch<T, n>(a, vec ? a.dtmp : a.src_scalar, rows, s); \
+        xfft_reg_launch<T, n>(a, vec ? a.dtmp : a.src_scalar, rows, s); \
         return vec ? 2 : 1;                                  \
     }
         TC_FFT_SIZES(TC_CASE)
@@ -630,6 +549,17 @@ bool launch_ixfft_reg(const IxFftArgs<T>& a, cudaStream_t s) {
     }
 }
 
+// The divergence pass alone (for the plane transforms of k_fft_plane.cu): false when the
+// vector RHS has no scratch or NX % 4 != 0.
+template <typename T>
+bool launch_div_quad(const DivFftArgs<T>& a, cudaStream_t s) {
+    if (a.dtmp == nullptr || a.g.NX % 4 != 0) return false;
+    div_quad_launch<T>(a, a.dtmp, s);
+    return true;
+}
+
+template bool launch_div_quad<double>(const DivFftArgs<double>&, cudaStream_t);
+template bool launch_div_quad<float>(const DivFftArgs<float>&, cudaStream_t);
 template bool launch_yfft_reg<double>(const YFftArgs<double>&, cudaStream_t);
 template bool launch_yfft_reg<float>(const YFftArgs<float>&, cudaStream_t);
 template int launch_div_xfft_reg<double>(const DivFftArgs<double>&, cudaStream_t);

@@ -190,6 +190,13 @@ template <typename T> void launch_ixfft(const IxFftArgs<T>& a, cudaStream_t s);
 template <typename T> int launch_div_xfft_reg(const DivFftArgs<T>& a, cudaStream_t s);  // 0: no such path
 template <typename T> bool launch_yfft_reg(const YFftArgs<T>& a, cudaStream_t s);
 template <typename T> bool launch_ixfft_reg(const IxFftArgs<T>& a, cudaStream_t s);
+template <typename T> bool launch_div_quad(const DivFftArgs<T>& a, cudaStream_t s);  // divergence into a.dtmp
+// Plane transforms (k_fft_plane.cu): the x- and y-FFTs of each z-plane in one kernel, one
+// thread-block cluster per plane.  plane_fft_ok: whether (NX, NY) has a compiled plane
+// kernel that fits this device; the launchers return 0 / false when it has none.
+template <typename T> bool plane_fft_ok(const Geom& g);
+template <typename T> int launch_div_xyfft_plane(const DivFftArgs<T>& a, const cplx<T>* twy, cudaStream_t s);
+template <typename T> bool launch_ixyfft_plane(const IxFftArgs<T>& a, const cplx<T>* twy, cudaStream_t s);
 template <typename T> void launch_correct(const CorrArgs<T>& a, cudaStream_t s);
 template <typename T> void launch_turb(const TurbArgs<T>& a, cudaStream_t s);
 template <typename T> void launch_divergence(const DivArgs<T>& a, cudaStream_t s);

@@ -235,6 +235,7 @@ struct tc_handle {
     // diagnostics fused into the step's correction (tc_set_diag_fusion)
     int diag_fuse = 0;             // 0 off (default), 1 always, 2 when the caller reads every step's diagnostics
     int mlp_fuse = 0;              // TC_TURB_MLP: 1 = closure evaluated inside the flux kernel (k_flux_mlp)
+    int fft_plane = 1;             // 1 = x- and y-FFTs of a plane in one cluster kernel where the grid has one
     bool diag_follow = false;      // mode 2: the last step's output level was read
     bool fused_valid = false, fused_used = false;
     int fused_level = -1, last_out = -1;
@@ -804,21 +805,26 @@ static void poisson(tc_handle* h, const void* rhs_vec, const void* rhs_scalar, v
     da.px = h->px;
     da.twx = twx<T>(h);
     da.dtmp = (T*)p_out;
-    const int ndx = launch_div_xfft<T>(da, h->st);
+    // plane kernels (x- and y-FFT of a plane in one launch) where the grid has them: the
+    // forward pair is timed as the x-FFT phase, the inverse pair as the inverse x-FFT phase
+    const bool plane = h->fft_plane && plane_fft_ok<T>(g);
+    int ndx = plane ? launch_div_xyfft_plane<T>(da, twy<T>(h), h->st) : 0;
+    const bool pf = ndx > 0;
+    if (!pf) ndx = launch_div_xfft<T>(da, h->st);
     if (mk) mark(h, 3, eb);
     YFftArgs<T> ya{g, (cplx<T>*)h->spec, h->py, twy<T>(h), -1};
-    launch_yfft<T>(ya, h->st);
+    if (!pf) launch_yfft<T>(ya, h->st);
     if (mk) mark(h, 4, eb);
     ZSolveArgs<T> za{g, mesh_dev<T>(h), mode_tabs(h), (cplx<T>*)h->spec, nullptr, h->err_flag, h->zfac, h->zfac_low};
     launch_zsolve_fac<T>(za, h->st, h->side, h->ev_fork, h->ev_join);
     if (mk) mark(h, 5, eb);
     ya.sign = +1;
-    launch_yfft<T>(ya, h->st);
+    if (!plane) launch_yfft<T>(ya, h->st);
     if (mk) mark(h, 6, eb);
     IxFftArgs<T> ia{g, (const cplx<T>*)h->spec, (T*)p_out, h->px, twx<T>(h), (T)(1.0 / ((double)g.NX * g.NY))};
-    launch_ixfft<T>(ia, h->st);
+    if (!(plane && launch_ixyfft_plane<T>(ia, twy<T>(h), h->st))) launch_ixfft<T>(ia, h->st);
     if (mk) mark(h, 7, eb);
-    h->launches += ndx + 5;
+    h->launches += ndx + (pf ? 0 : 1) + 2 + (plane ? 1 : 2);
 }
 
 template <typename T>
@@ -1892,6 +1898,12 @@ extern "C" int tc_mlp_forward(tc_mlp* m, const float* features, long long n, flo
 extern "C" int tc_set_mlp_fusion(tc_handle* h, int mode) {
     if (!h || mode < 0 || mode > 1) return fail(TC_E_ARG, "tc_set_mlp_fusion: bad handle or mode");
     h->mlp_fuse = mode;
+    return TC_OK;
+}
+
+extern "C" int tc_set_fft_fusion(tc_handle* h, int mode) {
+    if (!h || mode < 0 || mode > 1) return fail(TC_E_ARG, "tc_set_fft_fusion: bad handle or mode");
+    h->fft_plane = mode;
     return TC_OK;
 }
 
