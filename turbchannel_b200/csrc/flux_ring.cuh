@@ -11,12 +11,12 @@ namespace tc {
 constexpr int STX = 32, STY = 8;  // threads per CTA: 32 x 8
 constexpr int SG = 4;              // x-halo of the shared tile (a whole 16-byte chunk for float and double)
 
-// CY: cells per thread along y (the tile is 32 x 8*CY cells).
+// CY: cells per thread along y, TY: threads along y (the tile is 32 x TY*CY cells).
 // The offsets of the 2H+1 planes around the current one are computed once per plane,
 // so every stencil access is one of them plus a compile-time displacement.
-template <typename T, int H, int CY>
+template <typename T, int H, int CY, int TY = STY>
 struct RingAcc {
-    static constexpr int PW = STX + 2 * SG, PH = STY * CY + 2 * H, PL = PW * PH, RS = 2 * H + 2;
+    static constexpr int PW = STX + 2 * SG, PH = TY * CY + 2 * H, PL = PW * PH, RS = 2 * H + 2;
     const T* p[2 * H + 1];  // (slot of plane z+dz, component 0, this cell)
     __device__ __forceinline__ void set(const T* r, int zs, int tx, int ty) {  // ty: cell row inside the tile
         const T* c = r + (ty + H) * PW + tx + SG;
@@ -36,17 +36,18 @@ struct RingAcc {
 // shared-memory offset inside a ring slot and the global element offset without
 // the z term.  VEC: 16-byte chunks (the x-halo is chunk aligned, so the periodic
 // wrap moves whole chunks); otherwise single elements.
-template <typename T, int H, int CY, bool VEC>
+template <typename T, int H, int CY, bool VEC, int TY = STY>
 struct TileCopy {
-    using ACC = RingAcc<T, H, CY>;
+    using ACC = RingAcc<T, H, CY, TY>;
+    static constexpr int NT = STX * TY;  // threads of the CTA
     static constexpr int CH = VEC ? 16 / sizeof(T) : 1, NCH = ACC::PW / CH, PER = ACC::PH * NCH;
-    static constexpr int TOTAL = 3 * PER, NK = (TOTAL + STX * STY - 1) / (STX * STY);
+    static constexpr int TOTAL = 3 * PER, NK = (TOTAL + NT - 1) / NT;
     int sofs[NK];
     unsigned gofs[NK];  // < 2^32: checked on the host (3 N elements)
     __device__ __forceinline__ void init(int x0, int y0, int NX, int NY, long long N) {
 #pragma unroll
         for (int k = 0; k < NK; k++) {
-            const int e = threadIdx.x + k * STX * STY;
+            const int e = threadIdx.x + k * NT;
             if (e < TOTAL) {
                 const int c = e / PER, r = e - c * PER, py = r / NCH, ch = r - py * NCH;
                 const int gy = wrapi(y0 - H + py, NY), gx = wrapi(x0 - SG + ch * CH, NX);

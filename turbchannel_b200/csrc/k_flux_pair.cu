@@ -19,6 +19,7 @@
 
 #include "kernels.cuh"
 #include "stencil_stag.cuh"
+#include "stencil_vv4_int.cuh"
 
 namespace tc {
 
@@ -96,130 +97,8 @@ __device__ __forceinline__ F2 ld2(const float* p) { return F2(__ldg(reinterpret_
 __device__ __forceinline__ void st2(float* p, F2 v) { *reinterpret_cast<float2*>(p) = v.v; }
 __device__ __forceinline__ F2 fma2(F2 a, F2 b, F2 c) { return F2(__ffma2_rn(a.v, b.v, c.v)); }
 
-// ---------------------------------------------------------------------------------
-// Interior planes of VV4 with the CROSS viscosity (3 <= z <= NZ-4): the arithmetic of
-// conv_vv4 / visc_cross (INT = true) regrouped for packed FMAs, with the plane
-// constants K of MeshDev::FK (host-computed in double, see fill_flux_pair_consts):
-// every fourth-order interpolant 9 s - t is formed negated, t - 9 s (one FFMA2, no
-// negation needed), a face pair's fluxes Ir pr - Il pl as nl pl - nr pr, and each
-// direction's narrow and wide pairs are accumulated with their scale factors (the
-// reference's dz hy, C27 dzw hy, ... times the plane's momentum or w scale) folded
-// into K.  Same stencils and face fluxes as the reference (staggered/func_global.h:
-// 374-529 and 533-562); only the rounding order differs.
-
-// t - 9 s
-__device__ __forceinline__ F2 ni(F2 s, F2 t) { return fma2(F2(-9.f), s, t); }
-// nl pl - nr pr
-__device__ __forceinline__ F2 pd(F2 nl, F2 pl, F2 nr, F2 pr) { return nl * pl - nr * pr; }
-
-#define U(a, b, c) A(0, a, b, c)
-#define V(a, b, c) A(1, a, b, c)
-#define W(a, b, c) A(2, a, b, c)
-template <class ACC>
-__device__ __forceinline__ void visc_cross_int(const ACC& A, const F2* K, F2 s[3]) {
-#pragma unroll
-    for (int c = 0; c < 3; c++) {
-        const F2 v0 = A(c, 0, 0, 0);
-        const F2 tx = fma2(F2(-2.f), v0, A(c, 1, 0, 0) + A(c, -1, 0, 0));
-        const F2 ty = fma2(F2(-2.f), v0, A(c, 0, 1, 0) + A(c, 0, -1, 0));
-        F2 r = fma2(K[22], tx, s[c]);
-        r = fma2(K[23], ty, r);
-        r = fma2(K[c < 2 ? 18 : 20], A(c, 0, 0, 1) - v0, r);
-        s[c] = fma2(K[c < 2 ? 19 : 21], A(c, 0, 0, -1) - v0, r);
-    }
-}
-
-template <class ACC>
-__device__ __forceinline__ void conv_vv4_int(const ACC& A, const F2* K, F2 s[3]) {
-    {  // u: x-faces
-        const F2 U0 = U(0, 0, 0), Um1 = U(-1, 0, 0), Up1 = U(1, 0, 0), Um2 = U(-2, 0, 0), Up2 = U(2, 0, 0);
-        const F2 a = U0 + Up1, c = Um1 + U0;
-        const F2 dn = pd(ni(c, Um2 + Up1), c, ni(a, Um1 + Up2), a);
-        const F2 ppr = U0 + U(3, 0, 0), ppl = U(-3, 0, 0) + U0;
-        const F2 dw = pd(ni(Um2 + Um1, ppl), ppl, ni(Up1 + Up2, ppr), ppr);
-        s[0] = fma2(K[0], dn, s[0]);
-        s[0] = fma2(K[1], dw, s[0]);
-    }
-    {  // u: y-faces, v interpolated in x to the rows -1..2
-        const F2 U0 = U(0, 0, 0);
-        auto J = [&](int r) { return ni(V(0, r, 0) + V(-1, r, 0), V(-2, r, 0) + V(1, r, 0)); };
-        const F2 dn = pd(J(0), U(0, -1, 0) + U0, J(1), U0 + U(0, 1, 0));
-        const F2 dw = pd(J(-1), U(0, -3, 0) + U0, J(2), U0 + U(0, 3, 0));
-        s[0] = fma2(K[2], dn, s[0]);
-        s[0] = fma2(K[3], dw, s[0]);
-    }
-    {  // u: z-faces, w interpolated in x to the planes -1..2
-        const F2 U0 = U(0, 0, 0);
-        auto Kx = [&](int p) { return ni(W(0, 0, p) + W(-1, 0, p), W(-2, 0, p) + W(1, 0, p)); };
-        const F2 dn = pd(Kx(0), U(0, 0, -1) + U0, Kx(1), U0 + U(0, 0, 1));
-        const F2 dw = pd(Kx(-1), U0 + U(0, 0, -3), Kx(2), U0 + U(0, 0, 3));
-        s[0] = fma2(K[4], dn, s[0]);
-        s[0] = fma2(K[5], dw, s[0]);
-    }
-    {  // v: x-faces, u interpolated in y to the columns -1..2
-        const F2 V0 = V(0, 0, 0);
-        auto L = [&](int c) { return ni(U(c, 0, 0) + U(c, -1, 0), U(c, -2, 0) + U(c, 1, 0)); };
-        const F2 dn = pd(L(0), V(-1, 0, 0) + V0, L(1), V0 + V(1, 0, 0));
-        const F2 dw = pd(L(-1), V(-3, 0, 0) + V0, L(2), V0 + V(3, 0, 0));
-        s[1] = fma2(K[0], dn, s[1]);
-        s[1] = fma2(K[1], dw, s[1]);
-    }
-    {  // v: y-faces
-        const F2 V0 = V(0, 0, 0), Vm1 = V(0, -1, 0), Vp1 = V(0, 1, 0), Vm2 = V(0, -2, 0), Vp2 = V(0, 2, 0);
-        const F2 a = V0 + Vp1, c = Vm1 + V0;
-        const F2 dn = pd(ni(c, Vm2 + Vp1), c, ni(a, Vm1 + Vp2), a);
-        const F2 ppr = V0 + V(0, 3, 0), ppl = V(0, -3, 0) + V0;
-        const F2 dw = pd(ni(Vm2 + Vm1, ppl), ppl, ni(Vp1 + Vp2, ppr), ppr);
-        s[1] = fma2(K[2], dn, s[1]);
-        s[1] = fma2(K[3], dw, s[1]);
-    }
-    {  // v: z-faces, w interpolated in y to the planes -1..2
-        const F2 V0 = V(0, 0, 0);
-        auto Ky = [&](int p) { return ni(W(0, 0, p) + W(0, -1, p), W(0, -2, p) + W(0, 1, p)); };
-        const F2 dn = pd(Ky(0), V(0, 0, -1) + V0, Ky(1), V0 + V(0, 0, 1));
-        const F2 dw = pd(Ky(-1), V0 + V(0, 0, -3), Ky(2), V0 + V(0, 0, 3));
-        s[1] = fma2(K[4], dn, s[1]);
-        s[1] = fma2(K[5], dw, s[1]);
-    }
-    {  // w: x-faces, u interpolated in z (cell-height weights) to the w-face, columns -1..2
-        const F2 W0 = W(0, 0, 0);
-        auto M = [&](int c) {
-            return fma2(K[11], U(c, 0, -1), fma2(K[10], U(c, 0, 0), fma2(K[13], U(c, 0, 1), K[12] * U(c, 0, -2))));
-        };
-        auto MW = [&](int c) {
-            return fma2(K[15], U(c, 0, -1), fma2(K[14], U(c, 0, 0), fma2(K[17], U(c, 0, 1), K[16] * U(c, 0, -2))));
-        };
-        const F2 dn = pd(M(0), W(-1, 0, 0) + W0, M(1), W0 + W(1, 0, 0));
-        const F2 dw = pd(MW(-1), W(-3, 0, 0) + W0, MW(2), W0 + W(3, 0, 0));
-        s[2] = fma2(K[6], dn, s[2]);
-        s[2] = fma2(K[7], dw, s[2]);
-    }
-    {  // w: y-faces, v interpolated in z to the w-face, rows -1..2
-        const F2 W0 = W(0, 0, 0);
-        auto M = [&](int r) {
-            return fma2(K[11], V(0, r, -1), fma2(K[10], V(0, r, 0), fma2(K[13], V(0, r, 1), K[12] * V(0, r, -2))));
-        };
-        auto MW = [&](int r) {
-            return fma2(K[15], V(0, r, -1), fma2(K[14], V(0, r, 0), fma2(K[17], V(0, r, 1), K[16] * V(0, r, -2))));
-        };
-        const F2 dn = pd(M(0), W(0, -1, 0) + W0, M(1), W0 + W(0, 1, 0));
-        const F2 dw = pd(MW(-1), W(0, -3, 0) + W0, MW(2), W0 + W(0, 3, 0));
-        s[2] = fma2(K[6], dn, s[2]);
-        s[2] = fma2(K[7], dw, s[2]);
-    }
-    {  // w: z-faces
-        const F2 W0 = W(0, 0, 0), Wm1 = W(0, 0, -1), Wp1 = W(0, 0, 1), Wm2 = W(0, 0, -2), Wp2 = W(0, 0, 2);
-        const F2 pr = W0 + Wp1, pl = Wm1 + W0;
-        const F2 dn = pd(ni(pl, Wm2 + Wp1), pl, ni(pr, Wm1 + Wp2), pr);
-        const F2 ppr = W0 + W(0, 0, 3), ppl = W(0, 0, -3) + W0;
-        const F2 dw = pd(ni(Wm2 + Wm1, ppl), ppl, ni(Wp1 + Wp2, ppr), ppr);
-        s[2] = fma2(K[8], dn, s[2]);
-        s[2] = fma2(K[9], dw, s[2]);
-    }
-}
-#undef U
-#undef V
-#undef W
+// the interior-plane stencils of the fast path (the packed pair's vfma below)
+__device__ __forceinline__ F2 vfma(F2 a, F2 b, F2 c) { return fma2(a, b, c); }
 
 // RY: tile rows per thread (1: 256 threads; 2: 128 threads whose two rows share the
 // loads of their y-stencils, which the compiler merges as equal shared addresses).

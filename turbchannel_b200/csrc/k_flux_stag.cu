@@ -14,14 +14,15 @@
 #include "flux_ring.cuh"
 #include "kernels.cuh"
 #include "stencil_stag.cuh"
+#include "stencil_vv4_int.cuh"
 
 namespace tc {
 
-template <typename T, int SCHEME, int VISC, bool LES, bool INT, int CY>
-__device__ __forceinline__ void flux_cell(const RingAcc<T, SCHEME == TC_SCHEME_VV4 ? 3 : 1, CY>& A, const StagZ<T>& mz,
+template <typename T, int SCHEME, int VISC, bool LES, bool INT, int CY, int TY>
+__device__ __forceinline__ void flux_cell(const RingAcc<T, SCHEME == TC_SCHEME_VV4 ? 3 : 1, CY, TY>& A, const StagZ<T>& mz,
                                           T gcz, const FluxArgs<T>& a, int ix, int iy, int xm, int xp, int ym,
                                           int yp, size_t NXY, T f[3]) {
-    using ACC = RingAcc<T, SCHEME == TC_SCHEME_VV4 ? 3 : 1, CY>;
+    using ACC = RingAcc<T, SCHEME == TC_SCHEME_VV4 ? 3 : 1, CY, TY>;
     T cf[3], vf[3];
     if constexpr (SCHEME == TC_SCHEME_VV4) conv_vv4<T, ACC, INT>(A, mz, gcz, cf);
     else conv_hw2<T, ACC, INT>(A, mz, cf);
@@ -44,29 +45,35 @@ __device__ __forceinline__ void flux_cell(const RingAcc<T, SCHEME == TC_SCHEME_V
     f[2] = (T(0) + cf[2]) + vf[2];
 }
 
-template <typename T, int SCHEME, int VISC, bool LES, int ORDER, bool VEC, int CY>
-__global__ void __launch_bounds__(STX* STY, 2) k_flux_stag(FluxArgs<T> a, int tz) {
+template <typename T, int SCHEME, int VISC, bool LES, int ORDER, bool VEC, int CY, int TY>
+__global__ void __launch_bounds__(STX* TY, 2) k_flux_stag(FluxArgs<T> a, int tz) {
     constexpr int H = SCHEME == TC_SCHEME_VV4 ? 3 : 1;
-    using ACC = RingAcc<T, H, CY>;
+    using ACC = RingAcc<T, H, CY, TY>;
     constexpr int RS = ACC::RS;
     extern __shared__ __align__(16) unsigned char smraw[];
     T* ring = reinterpret_cast<T*>(smraw);
     __shared__ double sbuf[32];
+    // FP64 VV4 DNS: interior planes take the regrouped stencils of stencil_vv4_int.cuh with
+    // the plane constants FK64 of z and z+1 staged here
+    constexpr bool FAST = sizeof(T) == 8 && SCHEME == TC_SCHEME_VV4 && VISC == TC_VISC_CROSS && !LES;
+    __shared__ __align__(16) double fks[FAST ? 2 : 1][TC_FK64];
 
     const Geom& g = a.g;
     const int NX = g.NX, NY = g.NY, NZ = g.NZ;
     const size_t NXY = (size_t)NX * NY;
     const int tx = threadIdx.x % STX, tyt = threadIdx.x / STX;
-    const int x0 = blockIdx.x * STX, y0 = blockIdx.y * (STY * CY);
+    const int x0 = blockIdx.x * STX, y0 = blockIdx.y * (TY * CY);
     const int zb = blockIdx.z * tz, ze = min(NZ, zb + tz);
     const int ix = x0 + tx;
     // interior planes: no wall special case of the scheme applies
     const int zlo = SCHEME == TC_SCHEME_VV4 ? 3 : 1, zhi = SCHEME == TC_SCHEME_VV4 ? NZ - 4 : NZ - 2;
 
-    TileCopy<T, H, CY, VEC> cp;
+    TileCopy<T, H, CY, VEC, TY> cp;
     cp.init(x0, y0, NX, NY, g.N);
     const T* vbase = a.vel.c[0];  // the three components are consecutive blocks of N
     for (int z = max(0, zb - H); z <= min(NZ - 1, zb + H); z++) cp.load(ring, vbase, z, NXY);
+    if (FAST && threadIdx.x < TC_FK64 / 2 && zb < NZ)
+        cp_async<16>(&fks[zb & 1][2 * threadIdx.x], a.m.FK64 + (size_t)TC_FK64 * zb + 2 * threadIdx.x);
     cp_async_commit();
 
     StagZ<T> mz;
@@ -84,6 +91,8 @@ __global__ void __launch_bounds__(STX* STY, 2) k_flux_stag(FluxArgs<T> a, int tz
 
     for (int z = zb; z < ze; z++) {
         if (z + 1 < ze && z + H + 1 < NZ) cp.load(ring, vbase, z + H + 1, NXY);
+        if (FAST && z + 1 < ze && threadIdx.x < TC_FK64 / 2)
+            cp_async<16>(&fks[(z + 1) & 1][2 * threadIdx.x], a.m.FK64 + (size_t)TC_FK64 * (z + 1) + 2 * threadIdx.x);
         cp_async_commit();
         // history of this thread's cells, issued before the stencil so its latency overlaps it
         T hp[CY][3], hq[CY][3], vq[CY][3];
@@ -123,11 +132,21 @@ __global__ void __launch_bounds__(STX* STY, 2) k_flux_stag(FluxArgs<T> a, int tz
             ACC A = A0;
             A.shift_rows(q);
             T f[3];
-            if (inner) flux_cell<T, SCHEME, VISC, LES, true, CY>(A, mz, gcz, a, ix, iy, xm, xp, ym, yp, NXY, f);
-            else flux_cell<T, SCHEME, VISC, LES, false, CY>(A, mz, gcz, a, ix, iy, xm, xp, ym, yp, NXY, f);
+            bool done = false;
+            if constexpr (FAST) {
+                if (inner) {
+                    f[0] = (T)a.g.sour_dpdx;
+                    f[1] = f[2] = T(0);
+                    visc_cross_int(A, fks[z & 1], f);
+                    conv_vv4_int(A, fks[z & 1], f);
+                    done = true;
+                }
+            }
+            if (done) {
+            } else if (inner) flux_cell<T, SCHEME, VISC, LES, true, CY, TY>(A, mz, gcz, a, ix, iy, xm, xp, ym, yp, NXY, f);
+            else flux_cell<T, SCHEME, VISC, LES, false, CY, TY>(A, mz, gcz, a, ix, iy, xm, xp, ym, yp, NXY, f);
             if (z == 0) f[2] = 0;
             const size_t id = (size_t)z * NXY + (size_t)iy * NX + ix;
-#pragma unroll
             if (ORDER == 0) {
 #pragma unroll
                 for (int c = 0; c < 3; c++) a.fout.c[c][id] = f[c];
@@ -156,9 +175,12 @@ __global__ void __launch_bounds__(STX* STY, 2) k_flux_stag(FluxArgs<T> a, int tz
 // one for double (register budget of 2 CTAs/SM)
 template <typename T>
 constexpr int flux_cy() { return sizeof(T) == 4 ? 2 : 1; }
+// threads along y: 8 (256 threads per CTA)
+template <typename T>
+constexpr int flux_ty() { return STY; }
 
-static void flux_stag_shape(const Geom& g, int cy, dim3& grid, int& tz) {
-    const int ty = STY * cy;
+static void flux_stag_shape(const Geom& g, int tile_rows, dim3& grid, int& tz) {
+    const int ty = tile_rows;
     const int tiles = ((g.NX + STX - 1) / STX) * ((g.NY + ty - 1) / ty);
     int nch = std::max(1, (148 * 8 + tiles - 1) / tiles);
     tz = std::max(4, (g.NZ + nch - 1) / nch);
@@ -169,23 +191,23 @@ static void flux_stag_shape(const Geom& g, int cy, dim3& grid, int& tz) {
 int flux_grid_blocks(const Geom& g) {
     dim3 gr;
     int tz;
-    flux_stag_shape(g, 1, gr, tz);
+    flux_stag_shape(g, STY, gr, tz);  // the smallest tile of the kernels
     return (int)(gr.x * gr.y * gr.z);
 }
 
 template <typename T, int SCHEME, int VISC, bool LES, int ORDER>
 static void run(const FluxArgs<T>& a, cudaStream_t s) {
     constexpr int H = SCHEME == TC_SCHEME_VV4 ? 3 : 1;
-    constexpr int CY = flux_cy<T>();
-    constexpr size_t smem = sizeof(T) * (2 * H + 2) * 3 * RingAcc<T, H, CY>::PL;
+    constexpr int CY = flux_cy<T>(), TY = flux_ty<T>();
+    constexpr size_t smem = sizeof(T) * (2 * H + 2) * 3 * RingAcc<T, H, CY, TY>::PL;
     const bool vec = a.g.NX % (16 / (int)sizeof(T)) == 0;
-    auto kern = vec ? k_flux_stag<T, SCHEME, VISC, LES, ORDER, true, CY>
-                    : k_flux_stag<T, SCHEME, VISC, LES, ORDER, false, CY>;
+    auto kern = vec ? k_flux_stag<T, SCHEME, VISC, LES, ORDER, true, CY, TY>
+                    : k_flux_stag<T, SCHEME, VISC, LES, ORDER, false, CY, TY>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     dim3 grid;
     int tz;
-    flux_stag_shape(a.g, CY, grid, tz);
-    kern<<<grid, STX * STY, smem, s>>>(a, tz);
+    flux_stag_shape(a.g, TY * CY, grid, tz);
+    kern<<<grid, STX * TY, smem, s>>>(a, tz);
 }
 
 template <typename T, int SCHEME, int VISC, bool LES>

@@ -204,7 +204,7 @@ struct tc_handle {
     void* zfac = nullptr;  // time-independent factors of the z-matrices (k_zfactor)
     void* zfac_low = nullptr;  // double factors of the low modes
     void* mesh_t = nullptr;     // mesh arrays in T
-    void* fk = nullptr;         // float flux kernel plane constants (mixed precision)
+    void* fk = nullptr;         // flux kernels' interior-plane constants (float pairs mixed, doubles FP64 VV4)
     double* mesh_d = nullptr;   // mesh arrays in double
     double* tabs = nullptr;     // cos/sin tables
     void* tw = nullptr;         // twiddles (x then y), T complex
@@ -290,7 +290,8 @@ static MeshDev<T> mesh_dev(const tc_handle* h) {
     MeshDev<T> m;
     m.ZZ = t + 0 * L; m.DZ = t + 1 * L; m.DZW = t + 2 * L; m.GC1 = t + 3 * L; m.GC2 = t + 4 * L;
     m.GCZ = t + 5 * L; m.KERG = t + 6 * L; m.cellh = t + 7 * L; m.MAT_A = t + 8 * L; m.PC = t + 11 * L;
-    m.FK = (const float*)h->fk;
+    m.FK = h->fp64 ? nullptr : (const float*)h->fk;
+    m.FK64 = h->fp64 ? (const double*)h->fk : nullptr;
     m.dZZ = d + 0 * L; m.dDZ = d + 1 * L; m.dDZW = d + 2 * L; m.dKERG = d + 6 * L; m.dcellh = d + 7 * L;
     m.dMAT_A = d + 8 * L;
     for (int i = 0; i < 6; i++) m.MAT_D[i] = h->hm.MAT_D[i];
@@ -383,9 +384,9 @@ static void fill_plane_consts(const Geom& g, const HostMesh& hm, const T* t, T* 
 //            visc (2/(DZ[z]+DZ[z-1])) / DZ[z], visc (2/(DZ[z]+DZ[z-1])) / DZ[z-1]
 //   [22..23] visc / hx^2, visc / hy^2
 // (0 where an index leaves the mesh; those planes use the generic stencils).
-static void fill_flux_pair_consts(const Geom& g, const HostMesh& hm, std::vector<float>& fk) {
+static void fill_flux_plane_consts(const Geom& g, const HostMesh& hm, std::vector<double>& fk) {
     const int NZ = g.NZ;
-    fk.assign((size_t)TC_FK * NZ, 0.f);
+    fk.assign((size_t)TC_FK64 * NZ, 0.0);
     const double hx = g.hx, hy = g.hy, nu = g.visc, C27 = 1.0 / 27.0;
     const std::vector<double>&DZ = hm.DZ, &DZW = hm.DZW, &GCZ = hm.GCZ;
     for (int z = 0; z < NZ; z++) {
@@ -406,7 +407,7 @@ static void fill_flux_pair_consts(const Geom& g, const HostMesh& hm, std::vector
             k[20] = nu * dn / DZ[z]; k[21] = nu * dn / DZ[z - 1];
         }
         k[22] = nu / (hx * hx); k[23] = nu / (hy * hy);
-        for (int i = 0; i < 24; i++) fk[(size_t)TC_FK * z + 2 * i] = fk[(size_t)TC_FK * z + 2 * i + 1] = (float)k[i];
+        for (int i = 0; i < TC_FK64; i++) fk[(size_t)TC_FK64 * z + i] = k[i];
     }
 }
 
@@ -523,12 +524,20 @@ extern "C" int tc_create(const tc_params* prm, const double* zz, tc_handle** out
             for (size_t i = 0; i < mlen; i++) mf[i] = (float)md[i];
             fill_plane_consts<float>(g, hm, mf.data(), mf.data() + pc0);
             cudaMemcpy(h->mesh_t, mf.data(), mlen * sizeof(float), cudaMemcpyHostToDevice);
-            if (p.scheme != TC_SCHEME_COLLOC) {
-                std::vector<float> fk;
-                fill_flux_pair_consts(g, hm, fk);
+            if (p.scheme != TC_SCHEME_COLLOC) {  // each constant twice: a float2 for the packed arithmetic
+                std::vector<double> k;
+                fill_flux_plane_consts(g, hm, k);
+                std::vector<float> fk((size_t)TC_FK * g.NZ);
+                for (size_t i = 0; i < k.size(); i++) fk[2 * i] = fk[2 * i + 1] = (float)k[i];
                 TC_ALLOC(h->fk, fk.size() * sizeof(float));
                 cudaMemcpy(h->fk, fk.data(), fk.size() * sizeof(float), cudaMemcpyHostToDevice);
             }
+        }
+        if (h->fp64 && p.scheme == TC_SCHEME_VV4) {
+            std::vector<double> k;
+            fill_flux_plane_consts(g, hm, k);
+            TC_ALLOC(h->fk, k.size() * sizeof(double));
+            cudaMemcpy(h->fk, k.data(), k.size() * sizeof(double), cudaMemcpyHostToDevice);
         }
     }
     // mode tables (staggered/func_global.h:208-211 cos tables; VV4 sin(pi k / N))

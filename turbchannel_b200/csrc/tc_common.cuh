@@ -32,14 +32,15 @@ struct Geom {
 // (DZ[-1] = 0), [2] 2/(DZ[z]+DZ[z+1]) (DZ[NZ] = 0), [3] 1/DZ[z-1] (0 at z = 0),
 // [4] VV4 convective scale -1/(32 (DZ-DZW/9) hx hy), [5] VV4 w scale -GCZ/(32 hx hy).
 constexpr int TC_PC = 8;
-// FK (mixed precision only): per plane the 24 constants of the float flux kernel's
-// interior-plane stencils, each stored twice (a float2 for the packed arithmetic):
-// TC_FK floats per plane, layout in k_flux_pair.cu.
-constexpr int TC_FK = 48;
+// FK (mixed precision): per plane the 24 constants of the flux kernels' interior-plane
+// stencils (stencil_vv4_int.cuh), each stored twice (a float2 for the packed arithmetic):
+// TC_FK floats per plane.  FK64 (FP64, VV4): the same constants once, TC_FK64 doubles.
+constexpr int TC_FK = 48, TC_FK64 = 24;
 template <typename T>
 struct MeshDev {
     const T *ZZ, *DZ, *DZW, *GC1, *GC2, *GCZ, *KERG, *MAT_A, *cellh, *PC;
     const float* FK = nullptr;
+    const double* FK64 = nullptr;
     const double *dZZ, *dDZ, *dDZW, *dKERG, *dMAT_A, *dcellh;
     double MAT_D[6];
     double KERG_norm2;
