@@ -67,6 +67,7 @@ def peaks():
 
 
 GRID = None  # (NX, NY, NZ) override for profiling runs (--grid); not a bench number
+FLUX_STAGING = None  # --flux-staging: the float flux kernel's ring fill, None = the library default
 
 
 def workload_params(precision: int, device: int, small: bool = False):
@@ -134,6 +135,8 @@ def time_arm(precision: int, steps: int, warmup: int, device: int, dist_ctx, sma
 
     p, zz, w = workload_params(precision, device, small)
     S = tb.Solver(p, zz)
+    if FLUX_STAGING is not None:
+        S.set_flux_staging(FLUX_STAGING)
     S.init_channel(0, seed=12345, amp=0.1, project=True)
     S.set_forcing(1, 1.0)
     tau = w["tau"]
@@ -398,10 +401,13 @@ def main():
     ap.add_argument("--only", choices=["mixed", "fp64"], help="time one precision only (profiling)")
     ap.add_argument("--grid", type=int, nargs=3, metavar=("NX", "NY", "NZ"),
                     help="override the grid (profiling runs; not a bench number)")
+    ap.add_argument("--flux-staging", type=int, choices=[0, 1], default=None,
+                    help="float flux kernel ring fill: 0 cp.async, 1 TMA tensor boxes (tc_set_flux_staging)")
     args = ap.parse_args()
-    global GRID
+    global GRID, FLUX_STAGING
     if args.grid:
         GRID = tuple(args.grid)
+    FLUX_STAGING = args.flux_staging
     if args.only == "mixed":
         args.no_fp64 = True
     args.warmup = max(3, args.warmup)

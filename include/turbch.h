@@ -171,6 +171,14 @@ int tc_set_diag_fusion(tc_handle* h, int mode);
  * FMA contraction). */
 int tc_set_fft_fusion(tc_handle* h, int mode);
 
+/* How the float flux kernel (mixed precision, staggered CROSS) fills its shared-memory
+ * ring of velocity planes (no counterpart in the reference).  mode 0 (default): every
+ * thread copies 16-byte chunks (cp.async); 1: tiles whose halo does not wrap (NX % 64 ==
+ * 0, NY % 8 == 0) are filled by TMA tensor-map boxes, one per component and plane,
+ * completed on an mbarrier (bounded waits: a load that never completes makes tc_sync
+ * return TC_E_CUDA), the border tiles by cp.async in a second launch.  Same results. */
+int tc_set_flux_staging(tc_handle* h, int mode);
+
 /* Segregated IMEX Runge-Kutta step of the collocated scheme (collocated_SRK:
  * data::Step, func_global.h:317-408; method tables as collocated_SRK/imex.h:10-41).
  * The handle must be collocated with cross viscosity and no turbulence model; the

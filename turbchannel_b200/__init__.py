@@ -42,7 +42,7 @@ EXPORTS = [
     "tc_diagnostics", "tc_op_explicit_term", "tc_op_apply_gradient", "tc_op_apply_divergence",
     "tc_op_unapply_gradient", "tc_op_pressure_solve", "tc_op_turb_visc", "tc_set_nu_t", "tc_get_nu_t",
     "tc_init_channel", "tc_mesh_tanh", "tc_phase_timing", "tc_phase_times", "tc_launch_count",
-    "tc_op_pressure_solve_static", "tc_set_diag_fusion", "tc_set_fft_fusion", "tc_checkpoint_save", "tc_checkpoint_load",
+    "tc_op_pressure_solve_static", "tc_set_diag_fusion", "tc_set_fft_fusion", "tc_set_flux_staging", "tc_checkpoint_save", "tc_checkpoint_load",
     "tc_stats_accumulate", "tc_stats_read", "tc_stats_reset", "tc_run_graph", "tc_pressure_solve_device",
     "tc_srk_init", "tc_srk_step",
 ]
@@ -110,6 +110,7 @@ def load_library(path: str = LIB_PATH):
     L.tc_launch_count.argtypes = [vp, C.POINTER(C.c_ulonglong)]
     L.tc_set_diag_fusion.argtypes = [vp, ip]
     L.tc_set_fft_fusion.argtypes = [vp, ip]
+    L.tc_set_flux_staging.argtypes = [vp, ip]
     L.tc_set_mlp_fusion.argtypes = [vp, ip]
     L.tc_srk_init.argtypes = [vp, ip, ip, vp, vp, ip, C.c_double]
     L.tc_srk_step.argtypes = [vp, C.c_double, C.c_double]
@@ -350,6 +351,10 @@ class Solver:
     def set_fft_fusion(self, mode: int):
         """1 (default): the x- and y-FFTs of a plane in one cluster kernel where the grid has one, 0: separate kernels."""
         self._check(self.L.tc_set_fft_fusion(self.h, mode))
+
+    def set_flux_staging(self, mode: int):
+        """Float flux kernel ring fill: 0 (default) cp.async chunks, 1 TMA tensor boxes on tiles whose halo does not wrap."""
+        self._check(self.L.tc_set_flux_staging(self.h, mode))
 
     def srk_init(self, method, stab_type: int = 1, alpha_tau: float = None):
         """Set up the segregated IMEX Runge-Kutta step (collocated_SRK data::Step) with a

@@ -36,6 +36,8 @@ struct FluxArgs {
     double* ub_partial;
     unsigned* ticket;
     double* ub_out;
+    int* err_flag = nullptr;  // set to 2 when a bounded wait of the TMA staging gives up
+    int staging = 0;          // float pair kernel: 0 cp.async ring fill, 1 TMA tensor tiles (interior tiles)
 };
 
 // SBDF right-hand side (staggered/func_global.h:910-932) with the flux history kept as

@@ -236,6 +236,7 @@ struct tc_handle {
     int diag_fuse = 0;             // 0 off (default), 1 always, 2 when the caller reads every step's diagnostics
     int mlp_fuse = 0;              // TC_TURB_MLP: 1 = closure evaluated inside the flux kernel (k_flux_mlp)
     int fft_plane = 1;             // 1 = x- and y-FFTs of a plane in one cluster kernel where the grid has one
+    int flux_staging = 0;          // float pair flux kernel: 0 cp.async ring fill, 1 TMA tensor boxes
     bool diag_follow = false;      // mode 2: the last step's output level was read
     bool fused_valid = false, fused_used = false;
     int fused_level = -1, last_out = -1;
@@ -775,6 +776,7 @@ extern "C" int tc_sync(tc_handle* h) {
     TC_CUDA(cudaMemcpy(&flag, h->err_flag, sizeof(int), cudaMemcpyDeviceToHost));
     if (flag) {
         cudaMemset(h->err_flag, 0, sizeof(int));
+        if (flag == 2) return fail(TC_E_CUDA, "flux kernel: a TMA tile load did not complete (bounded wait gave up)");
         return fail(TC_E_NUMERIC, "banded pressure solve met a vanishing pivot");
     }
     return TC_OK;
@@ -880,6 +882,8 @@ static int step_impl(tc_handle* h, double tau, int cur, int order) {
     fa.ub_partial = h->red + 2;
     fa.ticket = h->ticket;
     fa.ub_out = cfr ? h->red : nullptr;
+    fa.err_flag = h->err_flag;
+    fa.staging = h->flux_staging;
     const double itd = (double)inv_tau;
     if (order >= 2) rebase_hist<T>(h, prv, itd);
     if (order == 3) rebase_hist<T>(h, pr2, itd);
@@ -1907,6 +1911,12 @@ extern "C" int tc_mlp_forward(tc_mlp* m, const float* features, long long n, flo
 extern "C" int tc_set_mlp_fusion(tc_handle* h, int mode) {
     if (!h || mode < 0 || mode > 1) return fail(TC_E_ARG, "tc_set_mlp_fusion: bad handle or mode");
     h->mlp_fuse = mode;
+    return TC_OK;
+}
+
+extern "C" int tc_set_flux_staging(tc_handle* h, int mode) {
+    if (!h || mode < 0 || mode > 1) return fail(TC_E_ARG, "tc_set_flux_staging: bad handle or mode");
+    h->flux_staging = mode;
     return TC_OK;
 }
 

@@ -104,6 +104,47 @@ __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
+// ---------------------------------------------------------------------------
+// mbarrier and TMA tiled tensor loads into this CTA's shared memory (no cluster
+// multicast; the tensor map covers this GPU's memory only).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Wait for the phase of `bar` with the given parity; false after `limit` polls (the
+// caller records an error instead of waiting for ever).
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity, int limit = 1 << 22) {
+    for (int it = 0; it < limit; it++)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+// Order this thread's earlier generic-proxy shared-memory accesses before later
+// async-proxy (TMA) writes to the same memory.
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+// One box of a 3-D tiled tensor map into shared memory at `dst` (128-byte aligned),
+// complete_tx on `bar`.  x * element size must be a multiple of 16 bytes.
+__device__ __forceinline__ void tma_load_3d(void* dst, const void* tmap, int x, int y, int z, unsigned long long* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];\n" ::"r"(
+            smem_u32(dst)),
+        "l"(tmap), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+        : "memory");
+}
+
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -133,10 +174,10 @@ __device__ __forceinline__ double block_sum(double v, double* sbuf) {
 // Deterministic grid reduction: every block stores its partial, the last block to
 // arrive sums all partials in index order and stores the total (then re-arms the
 // ticket for the next launch).  Thread 0 of each block passes its partial.
-__device__ __forceinline__ void grid_sum_finish(double partial, double* partials, unsigned* ticket, double* out,
-                                                double* sbuf) {
-    const unsigned nb = gridDim.x * gridDim.y * gridDim.z;
-    const unsigned bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+// grid_sum_finish_at: the same over several launches of one stream that share the
+// ticket: block `bid` of `nb` in all (the last launch's last block finishes).
+__device__ __forceinline__ void grid_sum_finish_at(double partial, double* partials, unsigned* ticket, double* out,
+                                                   double* sbuf, unsigned bid, unsigned nb) {
     __shared__ unsigned s_last;
     if (threadIdx.x == 0) {
         partials[bid] = partial;
@@ -154,6 +195,11 @@ __device__ __forceinline__ void grid_sum_finish(double partial, double* partials
         *out = s;
         *ticket = 0u;
     }
+}
+__device__ __forceinline__ void grid_sum_finish(double partial, double* partials, unsigned* ticket, double* out,
+                                                double* sbuf) {
+    grid_sum_finish_at(partial, partials, ticket, out, sbuf, blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z),
+                       gridDim.x * gridDim.y * gridDim.z);
 }
 
 __device__ __forceinline__ int wrapi(int i, int n) {
