@@ -4,7 +4,7 @@ Forall kernels, cuFFT D2Z/Z2D, Thrust reductions; staggered/func_cuda.cpp,
 collocated_AB3/main.cpp:114-178), compiled from the reference's sources by
 ``make -C oracle ref`` into oracle/_ref/libref_<variant>.so.
 
-BASELINE INFRASTRUCTURE ONLY (like the oracle): the product never loads these
+Timing infrastructure for the comparison only (like the oracle): the product never loads these
 libraries; bench.py runs this script in a child process for its ``reference_gpu``
 figures, so the reference's CUDA context, allocations and exit-on-error handling
 (staggered/func_cuda.cpp:23-35) stay out of the benchmark process.
