@@ -373,9 +373,10 @@ static void run_pair(const FluxArgs<float>& a, cudaStream_t s) {
     constexpr int H = SCHEME == TC_SCHEME_VV4 ? 3 : 1;
     constexpr size_t smem = sizeof(float) * (2 * H + 2) * 3 * RingX2<H>::PLP + 128;  // + alignment slack
     const int ntx = (a.g.NX + PCX - 1) / PCX, nty = (a.g.NY + PTR - 1) / PTR, tiles = ntx * nty;
-    // z-chunks: about one CTA per resident slot (2 per SM; measured at 384x384x256:
-    // 0.699 ms against 0.710 ms with 8 slots per SM, shorter chunks)
-    const int nch = std::max(1, (148 * 2 + tiles - 1) / tiles);
+    // z-chunks: as many as still fit the 2 resident CTAs per SM in one wave (measured at
+    // 384x384x256, 288 tiles: one chunk 0.703 ms, two chunks (two waves) 0.708, chunks for
+    // 8 slots per SM 0.710)
+    const int nch = std::max(1, (148 * 2) / tiles);
     const int tz = std::max(4, (a.g.NZ + nch - 1) / nch);
     const int nzc = (a.g.NZ + tz - 1) / tz;
     auto plain = k_flux_pair<SCHEME, ORDER, PAIR_RY, false>;

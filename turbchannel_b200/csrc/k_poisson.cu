@@ -641,7 +641,12 @@ void launch_zfactor(const ZSolveArgs<T>& a, cudaStream_t s) {
 template <typename T, int SCHEME>
 __global__ void __launch_bounds__(128) k_zsolve_fac(ZSolveArgs<T> a) {
     constexpr bool VV = SCHEME == TC_SCHEME_VV4;
-    constexpr int R = sizeof(T) == 4 ? 8 : 4;
+    // rows per register batch: as deep as keeps the kernel at 4 (float, 120 registers) or 5
+    // (double, 96) CTAs of 128 threads per SM, so that the ~74 k mode threads of a
+    // 384 x 384 plane run as one wave (measured at 384x256x384: float 8 rows, 152 registers,
+    // 1.3 waves: 0.176 ms; 6 rows 0.152; 5 rows 0.158; double 4 rows 0.318, 3 rows 0.296,
+    // 2 rows 0.292)
+    constexpr int R = sizeof(T) == 4 ? 6 : 2;
     using FQ = typename std::conditional<VV, Q4<T>, Q2<T>>::type;
     using BQ = typename std::conditional<VV, Q4<T>, T>::type;
     const Geom& g = a.g;
