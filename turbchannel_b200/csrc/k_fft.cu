@@ -79,8 +79,11 @@ static void yfft_reg_launch(const YFftArgs<T>& a, cudaStream_t s) {
 // stencils stay in registers from one plane to the next (one new w load per plane
 // instead of four; measured at 384x384x256, float: 0.188 ms with the x-FFT against 0.223
 // ms for one plane per thread).
+// Bounded for four CTAs per SM in float (64 registers) and three in double (80 registers;
+// 0.351 against 0.359 ms with the x-FFT at 384x256x384; float with one CTA as the bound
+// takes 79 registers and 0.193 against 0.184 ms)
 template <typename T, int SCHEME, int ZC>
-__global__ void __launch_bounds__(256) k_div_quad_z(DivFftArgs<T> a, T* __restrict__ out) {
+__global__ void __launch_bounds__(256, sizeof(T) == 8 ? 3 : 4) k_div_quad_z(DivFftArgs<T> a, T* __restrict__ out) {
     const Geom& g = a.g;
     const int NX = g.NX, NY = g.NY, NZ = g.NZ, NQ = NX >> 2, NZB = (NZ + ZC - 1) / ZC;
     const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -180,8 +183,9 @@ __host__ __device__ constexpr bool xfft_alias(int rows) {
     return (rows / 2) * FftSplit<N>::N1 <= 256;
 }
 
+// Three CTAs per SM in float (79 registers at N = 384, no spill), two in double.
 template <typename T, int N>
-__global__ void __launch_bounds__(256, 2) k_xfft_reg(DivFftArgs<T> a, const T* __restrict__ src, int rows, int lrows) {
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xfft_reg(DivFftArgs<T> a, const T* __restrict__ src, int rows, int lrows) {
     constexpr int N1 = FftSplit<N>::N1, N2 = FftSplit<N>::N2, YL = FftSplit<N>::YL, ZS = N + 1;
     extern __shared__ __align__(16) unsigned char smraw[];
     const Geom& g = a.g;
