@@ -37,7 +37,12 @@ __global__ void __launch_bounds__(256) k_yfft_reg(cplx<T>* spec, long long nline
     constexpr int LINES = yfft_reg_lines<T, N>();
     extern __shared__ __align__(16) unsigned char smraw[];
     cplx<T>* Y = reinterpret_cast<cplx<T>*>(smraw);
-    const long long L0 = (long long)blockIdx.x * LINES;
+    // the forward transform takes the lines in descending z, the reverse of the x-FFT that
+    // wrote them (its last planes are still in L2), and leaves the low planes, which the
+    // z-solve's forward sweep reads first, written last (384x256x384 float: y-FFT 0.052
+    // against 0.059 ms, z-solve 0.144 against 0.152; double 0.097 / 0.283 against 0.101 / 0.292)
+    const long long blk = SIGN < 0 ? (long long)gridDim.x - 1 - blockIdx.x : (long long)blockIdx.x;
+    const long long L0 = blk * LINES;
     const int nl = (int)min((long long)LINES, nlines - L0);
     cplx<T>* base = spec + L0 * N;
     for (int it = threadIdx.x; it < nl * N2; it += blockDim.x) {
@@ -89,7 +94,11 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 3 : 4) k_div_quad_z(DivF
     const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= (long long)NQ * NY * NZB) return;
     const int row = (int)(q / NQ), x = (int)(q - (long long)row * NQ) * 4;
-    const int y = row % NY, z0 = (row / NY) * ZC;
+    // float: plane chunks in descending z, the float flux kernel's last-written planes (high
+    // z) being the ones still in L2 (divergence + x-FFT 0.177 against 0.179 ms at
+    // 384x256x384); double keeps ascending chunks (the FP64 flux kernel writes in z-chunks,
+    // and descending took 0.377 against 0.353 ms)
+    const int y = row % NY, z0 = (sizeof(T) == 4 ? NZB - 1 - row / NY : row / NY) * ZC;
     const size_t NXY = (size_t)NX * NY, col = (size_t)y * NX + x;
     const T *u = a.v.c[0], *v = a.v.c[1], *w = a.v.c[2];
     const T ihx = (T)g.inv_hx, ihy = (T)g.inv_hy;
@@ -281,7 +290,10 @@ __global__ void __launch_bounds__(XP_NT) k_ixfft_pipe(IxFftArgs<T> a) {
     const Geom& g = a.g;
     const int NY = g.NY, YB = NY / RB;
     const long long ntile = (long long)YB * g.NZ;
+    // tiles in descending z, the reverse of the inverse y-FFT that wrote them (its last
+    // planes are still in L2)
     auto fetch = [&](long long t, int b) {
+        t = ntile - 1 - t;
         const int z = (int)(t / YB), y0 = (int)(t - (long long)z * YB) * RB;
         cplx<T>* tile = reinterpret_cast<cplx<T>*>(smraw + b * P::buf);
         for (int e = threadIdx.x; e < NXH * CPK; e += XP_NT) {
@@ -298,7 +310,8 @@ __global__ void __launch_bounds__(XP_NT) k_ixfft_pipe(IxFftArgs<T> a) {
         cp_async_commit();
         cp_async_wait<1>();
         __syncthreads();  // tile t is in buffer b
-        const int z = (int)(t / YB), y0 = (int)(t - (long long)z * YB) * RB;
+        const long long tr = ntile - 1 - t;
+        const int z = (int)(tr / YB), y0 = (int)(tr - (long long)z * YB) * RB;
         const cplx<T>* tile = reinterpret_cast<const cplx<T>*>(smraw + b * P::buf);
         for (int it = threadIdx.x; it < NL * N2; it += XP_NT) {
             const int l = it / N2, n2 = it - l * N2;
@@ -391,7 +404,8 @@ __global__ void __launch_bounds__(512) k_ixfft_reg(IxFftArgs<T> a, int rows, int
     // alias: the first pass's output over the tile itself, every thread holding at most
     // one line segment (gather all, barrier, transform and write); else after the tile
     cplx<T>* Y = alias ? tile : tile + NXH * TS;
-    const int z = blockIdx.y, y0 = blockIdx.x * rows;
+    // planes in descending z, the reverse of the inverse y-FFT that wrote them
+    const int z = gridDim.y - 1 - blockIdx.y, y0 = blockIdx.x * rows;
     {
         const int cpr = rows / PC, lc = lrows - (PC == 2 ? 1 : 0);
         for (int e = threadIdx.x; e < NXH * cpr; e += blockDim.x) {
