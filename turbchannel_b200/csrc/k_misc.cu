@@ -145,7 +145,10 @@ __global__ void __launch_bounds__(QX* QY, 3) k_correct_quad(CorrArgs<T> a) {
     const size_t NXY = (size_t)NX * NY;
     const int xq = blockIdx.x * QX + threadIdx.x % QX, iy = blockIdx.y * QY + threadIdx.x / QX;
     if (xq >= NQ || iy >= NY) return;
-    const int x = 4 * xq, zb = blockIdx.z * ZN;
+    // float: planes in descending z, so that the next step's flux kernel (marching up from
+    // z = 0) finds the last-written low planes in L2; double keeps ascending planes, the
+    // reverse of its descending inverse x-FFT
+    const int x = 4 * xq, zb = (sizeof(T) == 4 ? (int)(gridDim.z - 1 - blockIdx.z) : (int)blockIdx.z) * ZN;
     const int xl = x == 0 ? NX - 4 : x - 4, xr = x + 4 == NX ? 0 : x + 4;
     const int ym = wrapi(iy - 1, NY), ymm = wrapi(iy - 2, NY), yp = wrapi(iy + 1, NY);
     const T* __restrict__ p = a.p;
