@@ -360,18 +360,24 @@ static bool ixfft_pipe_launch(const IxFftArgs<T>& a, cudaStream_t s) {
         using P = IPipe<T, N>;
         if (a.g.NY % P::RB != 0) return false;
         auto k = k_ixfft_pipe<T, N>;
-        static int sms = 0, occ = -1;  // per size, resolved at the first launch
-        if (occ < 0) {
-            int dev = 0, optin = 0, o = 0;
-            cudaGetDevice(&dev);
-            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        // per size and device (function attributes are per device), resolved at the first launch
+        constexpr int MAXDEV = 64;
+        static int sms_of[MAXDEV] = {}, occ_of[MAXDEV] = {};  // occ 0: not resolved yet, -1: does not fit
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (dev < 0 || dev >= MAXDEV) return false;
+        if (occ_of[dev] == 0) {
+            int optin = 0, o = 0, n = 0;
+            cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
             cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
             if (P::smem <= (size_t)optin) {
                 cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P::smem);
                 cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k, XP_NT, P::smem);
             }
-            occ = o;
+            sms_of[dev] = n;
+            occ_of[dev] = o > 0 ? o : -1;
         }
+        const int occ = occ_of[dev], sms = sms_of[dev];
         if (occ < 1) return false;
         const long long ntile = (long long)(a.g.NY / P::RB) * a.g.NZ;
         const int grid = (int)std::min<long long>(ntile, (long long)sms * occ);

@@ -273,13 +273,19 @@ static bool plane_fits() {
     if constexpr (!P::ok) {
         return false;
     } else {
-        static int state = -1;  // resolved at the first call
-        if (state < 0)
-            state = cluster_fits(reinterpret_cast<const void*>(k_xyfft_plane<T, NX, NY>), P::smem) &&
-                            cluster_fits(reinterpret_cast<const void*>(k_ixyfft_plane<T, NX, NY>), P::smem)
-                        ? 1
-                        : 0;
-        return state == 1;
+        // per device (function attributes are per device), resolved at the first call:
+        // 0 not resolved, 1 fits, -1 does not
+        constexpr int MAXDEV = 64;
+        static int state[MAXDEV] = {};
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (dev < 0 || dev >= MAXDEV) return false;
+        if (state[dev] == 0)
+            state[dev] = cluster_fits(reinterpret_cast<const void*>(k_xyfft_plane<T, NX, NY>), P::smem) &&
+                                 cluster_fits(reinterpret_cast<const void*>(k_ixyfft_plane<T, NX, NY>), P::smem)
+                             ? 1
+                             : -1;
+        return state[dev] == 1;
     }
 }
 
