@@ -11,7 +11,7 @@ namespace tc {
 // conv_vv4 / visc_cross (INT = true) regrouped for FMAs, with the 24 plane constants K
 // (host-computed in double, see fill_flux_plane_consts in tc_api.cu; float2 pairs in the
 // float pair kernel, doubles in the FP64 kernel):
-// every fourth-order interpolant 9 s - t is formed negated, t - 9 s (one FFMA2, no
+// every fourth-order interpolant 9 s - t is formed negated, t - 9 s (one FMA, no
 // negation needed), a face pair's fluxes Ir pr - Il pl as nl pl - nr pr, and each
 // direction's narrow and wide pairs are accumulated with their scale factors (the
 // reference's dz hy, C27 dzw hy, ... times the plane's momentum or w scale) folded

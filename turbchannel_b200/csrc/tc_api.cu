@@ -375,9 +375,10 @@ static void fill_plane_consts(const Geom& g, const HostMesh& hm, const T* t, T* 
     }
 }
 
-// Constants of the float flux kernel's interior planes (k_flux_pair), from the double
-// mesh, each written twice: per plane z, with miv and w5 the VV4 momentum and w scales
-// of PC[4], PC[5] and C27 = 1/27,
+// Constants of the flux kernels' interior VV4 planes (stencil_vv4_int.cuh: the float
+// pair kernel stores each twice as a float2, the FP64 kernel once), from the double mesh:
+// per plane z, with miv and w5 the VV4 momentum and w scales of PC[4], PC[5] and
+// C27 = 1/27,
 //   [0..5]   miv dz hy, -miv C27 dzw hy, miv dz hx, -miv C27 dzw hx, miv hx hy, -miv C27 hx hy
 //   [6..9]   w5 hy, -w5 C27 hy, w5 hx hy, -w5 C27 hx hy
 //   [10..13] -9 DZ[z], -9 DZ[z-1], DZ[z-2], DZ[z+1]; [14..17] the same of DZW
